@@ -1,0 +1,123 @@
+/*
+ * spires_ext.h -- additive entry points of the B200 spires library.
+ *
+ * Nothing here exists in the reference header; these calls carry what
+ * spires.h cannot express (device-resident series, recorded state matrices,
+ * spike rasters, mixed-precision ridge options, washout, host-only model
+ * inspection) and the tuning hooks of the GPU implementation. All use plain C
+ * types; device pointers are passed as `const double *` / `double *` and are
+ * documented as such.
+ */
+#ifndef SPIRES_EXT_H
+#define SPIRES_EXT_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "spires.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- host-only model (no GPU needed) -------------------------------------
+ * Runs the construction of spires_reservoir_create (same rand() draws, same
+ * spectral-radius rescale) on the host and exposes the result. Used to check
+ * construction against the reference on machines without a GPU. */
+typedef struct spires_ext_model spires_ext_model;
+
+typedef struct {
+    size_t num_neurons, num_inputs, num_outputs, nnz;
+    int    ring_len;          /* FLIF_GL history length L (Caputo: mem_len - 2) */
+    int    micro_steps;       /* 1/dt */
+    int    syn_ring_len;      /* FRACTIONAL synapse history length */
+    int    syn_components;    /* FRACTIONAL_MULTIEXP component count */
+    double spectral_radius_before_rescale;
+} spires_ext_model_info;
+
+spires_status spires_ext_model_build(const spires_reservoir_config *cfg,
+                                     spires_ext_model **out);
+void          spires_ext_model_free(spires_ext_model *m);
+spires_status spires_ext_model_info_get(const spires_ext_model *m,
+                                        spires_ext_model_info *info);
+/* CSR of W (ascending columns); any pointer may be NULL */
+spires_status spires_ext_model_csr(const spires_ext_model *m, int64_t *row_ptr,
+                                   int32_t *col, double *val);
+spires_status spires_ext_model_w_in(const spires_ext_model *m, double *w_in);
+spires_status spires_ext_model_w_out(const spires_ext_model *m, double *w_out);
+/* PSC_HETEROGENEOUS per-edge tau in CSR order */
+spires_status spires_ext_model_edge_tau(const spires_ext_model *m, double *tau);
+/* FLIF_GL / FLIF_CAPUTO coefficient table [ring_len] */
+spires_status spires_ext_model_coef(const spires_ext_model *m, double *coef);
+
+/* ---- recorded runs -------------------------------------------------------
+ * Advance `T` macro steps from the current state with inputs u[T x num_inputs]
+ * (host memory; NULL = zeros) and record, after every macro step, the state
+ * (phi [T x N], may be NULL), the spike bits (raster [T x ceil(N/32)] words,
+ * bit i%32 of word i/32 = neuron i, may be NULL) and the readout
+ * (y [T x num_outputs], may be NULL). */
+spires_status spires_ext_run_record(spires_reservoir *r, const double *u, size_t T,
+                                    double *phi, uint32_t *raster, double *y);
+
+/* Same, with every pointer in device memory (u may be NULL); asynchronous on
+ * the handle's stream; completion and errors via spires_ext_sync. */
+spires_status spires_ext_run_device(spires_reservoir *r, const double *d_u, size_t T,
+                                    double *d_phi, uint32_t *d_raster, double *d_y);
+spires_status spires_ext_sync(spires_reservoir *r);
+void         *spires_ext_stream(spires_reservoir *r);    /* cudaStream_t */
+size_t        spires_ext_spike_words(const spires_reservoir *r);
+long long     spires_ext_kernel_launches(const spires_reservoir *r);
+
+/* Input weights W_in [N x num_inputs] of a reservoir (host copy). */
+spires_status spires_ext_read_w_in(const spires_reservoir *r, double *w_in);
+
+/* ---- launch shape of the persistent step kernel --------------------------- */
+typedef struct {
+    int ctas;         /* CTAs of the cooperative grid; 1 = single CTA */
+    int warps_max;    /* warps per CTA */
+    int variant;      /* 0 = generic, 1 = bulk-copy ring pipeline (FLIF_GL) */
+    int stages;       /* pipeline stages (variant 1) */
+    int rows;         /* ring rows per stage (variant 1) */
+} spires_ext_launch;
+
+spires_status spires_ext_get_launch(const spires_reservoir *r, spires_ext_launch *l);
+spires_status spires_ext_set_launch(spires_reservoir *r, const spires_ext_launch *l);
+/* Time candidate launch shapes on this reservoir (state is saved and restored)
+ * and keep the fastest. `steps` macro steps per candidate. */
+spires_status spires_ext_autotune(spires_reservoir *r, size_t steps);
+
+/* FLIF_DIFFUSIVE refractory sampler seed (per reservoir; neuron i gets a
+ * stream derived from seed and i). Takes effect at the next reset. */
+spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed);
+
+/* ---- ridge readout with options ------------------------------------------ */
+typedef enum {
+    SPIRES_EXT_GRAM_FP64 = 0,      /* FP64 Gram (CUDA cores) */
+    SPIRES_EXT_GRAM_BF16X3 = 1     /* BF16 hi/lo split on tensor cores, FP32
+                                      accumulate, FP64 refinement */
+} spires_ext_gram_mode;
+
+typedef struct {
+    int    gram_mode;        /* spires_ext_gram_mode */
+    int    max_refine;       /* iterative-refinement sweeps (BF16X3) */
+    double refine_tol;       /* relative residual target */
+    size_t washout;          /* leading rows excluded from the fit */
+} spires_ext_ridge_opts;
+
+typedef struct {
+    int    gram_mode_used;
+    int    refine_iters;
+    double rel_residual;     /* ||Phi^T Y - (Phi^T Phi + lambda I) W|| / ||Phi^T Y|| */
+    double collect_ms, gram_ms, factor_ms, refine_ms;
+    int    factor_failed;
+    int    lu_fallback;
+} spires_ext_ridge_report;
+
+spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_series,
+                                     const double *target_series, size_t series_length,
+                                     double lambda, const spires_ext_ridge_opts *opts,
+                                     spires_ext_ridge_report *report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

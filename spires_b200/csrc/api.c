@@ -1,0 +1,548 @@
+/*
+ * api.c -- every entry point of include/spires.h (and the host side of
+ * include/spires_ext.h) for the B200 library.
+ *
+ * Mirrors src/spires_api.c of the reference: argument checks and status codes
+ * are the same (NULL handle or buffer -> SPIRES_ERR_INVALID_ARG, dt must be in
+ * (0, 1] with 1/dt an integer within 1e-12, src/spires_api.c:22-75). Behind the
+ * checks, construction runs on the host (construct.c) and everything that
+ * advances or reads the reservoir runs on the device (dev_*.cu).
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "../../include/spires.h"
+#include "../../include/spires_ext.h"
+#include "sp_model.h"
+#include "sp_dev.h"
+#include "sp_api_internal.h"
+
+#define SPIRES_EXPORT __attribute__((visibility("default")))
+
+static spires_status to_status(int rc)
+{
+    switch (rc) {
+    case SP_OK: return SPIRES_OK;
+    case SP_EINVAL: return SPIRES_ERR_INVALID_ARG;
+    case SP_EALLOC: return SPIRES_ERR_ALLOC;
+    default: return SPIRES_ERR_INTERNAL;
+    }
+}
+
+/* dt check of src/spires_api.c:28-38 */
+static int dt_ok(double dt)
+{
+    if (dt <= 0.0 || dt > 1.0)
+        return 0;
+    double steps_d = 1.0 / dt;
+    int steps = (int)llround(steps_d);
+    if (steps < 1 || fabs(steps_d - (double)steps) > 1e-12)
+        return 0;
+    return 1;
+}
+
+static int model_from_config(const spires_reservoir_config *cfg, sp_host_model *m)
+{
+    memset(m, 0, sizeof(*m));
+    if (!dt_ok(cfg->dt))
+        return SP_EINVAL;
+    int rc = sp_validate_config(cfg->num_neurons, cfg->num_inputs, cfg->num_outputs, cfg->dt,
+                                (int)cfg->connectivity_type, (int)cfg->neuron_type,
+                                cfg->neuron_params, (int)cfg->synapse_type,
+                                (int)cfg->synapse_backend);
+    if (rc)
+        return rc;
+    m->n = cfg->num_neurons;
+    m->din = cfg->num_inputs;
+    m->dout = cfg->num_outputs;
+    m->spectral_radius = cfg->spectral_radius;
+    m->ei_ratio = cfg->ei_ratio;
+    m->input_strength = cfg->input_strength;
+    m->connectivity = cfg->connectivity;
+    m->dt = cfg->dt;
+    m->conn_type = (int)cfg->connectivity_type;
+    m->neuron_type = (int)cfg->neuron_type;
+    m->syn_type = (int)cfg->synapse_type;
+    m->syn_backend = (int)cfg->synapse_backend;
+    m->neuron_params = cfg->neuron_params;
+    m->synapse_params = cfg->synapse_params;
+    return SP_OK;
+}
+
+/* Wrap an already built host model into a handle with device state. */
+int sp_handle_from_model(sp_host_model *m, spires_reservoir **out_r)
+{
+    spires_reservoir *r = calloc(1, sizeof(*r));
+    if (!r)
+        return SP_EALLOC;
+    int rc = sp_dev_create(m, &r->dev);
+    if (rc) {
+        free(r);
+        return rc;
+    }
+    r->m = *m;
+    memset(m, 0, sizeof(*m)); /* ownership moved */
+    *out_r = r;
+    return SP_OK;
+}
+
+/* ----------------------------------------------------------- lifecycle -- */
+
+SPIRES_EXPORT spires_status spires_reservoir_create(const spires_reservoir_config *cfg,
+                                                    spires_reservoir **out_r)
+{
+    if (!cfg || !out_r)
+        return SPIRES_ERR_INVALID_ARG;
+    if (!dt_ok(cfg->dt)) {
+        fprintf(stderr, "dt must be in (0, 1.0] and divide 1.0 evenly\n");
+        return SPIRES_ERR_INVALID_ARG;
+    }
+    sp_host_model m;
+    int rc = model_from_config(cfg, &m);
+    if (rc)
+        return to_status(rc);
+    rc = sp_model_build(&m);
+    if (rc) {
+        sp_model_free(&m);
+        return rc == SP_EINVAL ? SPIRES_ERR_INVALID_ARG : SPIRES_ERR_INTERNAL;
+    }
+    rc = sp_handle_from_model(&m, out_r);
+    if (rc) {
+        sp_model_free(&m);
+        return to_status(rc);
+    }
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT void spires_reservoir_destroy(spires_reservoir *r)
+{
+    if (!r)
+        return;
+    sp_dev_destroy(r->dev);
+    sp_model_free(&r->m);
+    free(r);
+}
+
+SPIRES_EXPORT spires_status spires_reservoir_reset(spires_reservoir *r)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    /* neuron parameters are re-read through the caller's pointer, as
+     * reset_reservoir re-runs init_neuron (src/reservoir.c:770-780) */
+    int rc = sp_model_derive_neuron(&r->m);
+    if (rc)
+        return to_status(rc);
+    return to_status(sp_dev_reset_neurons(r->dev, &r->m));
+}
+
+/* ------------------------------------------------------------ stepping -- */
+
+SPIRES_EXPORT spires_status spires_step(spires_reservoir *r, const double *u_t)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_run_args a;
+    memset(&a, 0, sizeof(a));
+    a.u = u_t; /* NULL = zero input vector */
+    a.T = 1;
+    return to_status(sp_dev_run(r->dev, &a));
+}
+
+SPIRES_EXPORT double *spires_run(spires_reservoir *r, const double *input_series,
+                                 size_t series_length)
+{
+    if (!r || !r->dev || !input_series)
+        return NULL;
+    size_t count = r->m.dout * series_length;
+    double *out = malloc((count ? count : 1) * sizeof(double));
+    if (!out)
+        return NULL;
+    sp_run_args a;
+    memset(&a, 0, sizeof(a));
+    a.u = input_series;
+    a.T = series_length;
+    a.h_y = r->m.dout ? out : NULL;
+    a.sync = 1;
+    if (sp_dev_run(r->dev, &a) != SP_OK) {
+        free(out);
+        return NULL;
+    }
+    return out;
+}
+
+/* ------------------------------------------------------------ training -- */
+
+SPIRES_EXPORT spires_status spires_train_online(spires_reservoir *r, const double *target_vec,
+                                                double lr)
+{
+    if (!r || !r->dev || !target_vec)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_train_online(r->dev, target_vec, lr, r->m.W_out));
+}
+
+SPIRES_EXPORT spires_status spires_train_ridge(spires_reservoir *r, const double *input_series,
+                                               const double *target_series,
+                                               size_t series_length, double lambda)
+{
+    if (!r || !r->dev || !input_series || !target_series)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_opts o;
+    memset(&o, 0, sizeof(o));
+    o.gram_mode = sp_default_gram_mode();
+    o.max_refine = 30;
+    o.refine_tol = 1e-13;
+    sp_ridge_report rep;
+    int rc = sp_model_derive_neuron(&r->m); /* train_ridge starts with a reset */
+    if (rc)
+        return to_status(rc);
+    rc = sp_dev_train_ridge(r->dev, &r->m, input_series, target_series, series_length, lambda,
+                            &o, &rep, r->m.W_out);
+    return to_status(rc);
+}
+
+SPIRES_EXPORT spires_status spires_train_rls(spires_reservoir *r, const double *input_series,
+                                             const double *target_series, size_t series_length,
+                                             double delta, double lambda)
+{
+    if (!r || !r->dev || !input_series || !target_series)
+        return SPIRES_ERR_INVALID_ARG;
+    int rc = sp_model_derive_neuron(&r->m);
+    if (rc)
+        return to_status(rc);
+    return to_status(sp_dev_train_rls(r->dev, &r->m, input_series, target_series, series_length,
+                                      delta, lambda, r->m.W_out));
+}
+
+/* --------------------------------------------------------------- state -- */
+
+SPIRES_EXPORT double *spires_copy_reservoir_state(spires_reservoir *r)
+{
+    if (!r || !r->dev)
+        return NULL;
+    double *s = malloc(r->m.n * sizeof(double));
+    if (!s)
+        return NULL;
+    if (sp_dev_read_state(r->dev, s) != SP_OK) {
+        free(s);
+        return NULL;
+    }
+    return s;
+}
+
+SPIRES_EXPORT spires_status spires_read_reservoir_state(spires_reservoir *r, double *buffer)
+{
+    if (!r || !r->dev || !buffer) {
+        fprintf(stderr, "Error reading reservoir state, buffer not initialized!\n");
+        return SPIRES_ERR_INVALID_ARG;
+    }
+    return to_status(sp_dev_read_state(r->dev, buffer));
+}
+
+SPIRES_EXPORT spires_status spires_read_spike_state(spires_reservoir *r, double *buffer)
+{
+    if (!r || !r->dev || !buffer)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_read_spikes(r->dev, buffer));
+}
+
+static void dense_from_csr(const sp_host_model *m, double *buf)
+{
+    size_t n = m->n;
+    memset(buf, 0, n * n * sizeof(double));
+    for (size_t i = 0; i < n; i++)
+        for (int64_t k = m->row_ptr[i]; k < m->row_ptr[i + 1]; k++)
+            buf[i * n + (size_t)m->col[k]] = m->w[k];
+}
+
+SPIRES_EXPORT double *spires_copy_weights(const spires_reservoir *r)
+{
+    if (!r || !r->m.n)
+        return NULL;
+    double *buf = malloc(r->m.n * r->m.n * sizeof(double));
+    if (!buf)
+        return NULL;
+    dense_from_csr(&r->m, buf);
+    return buf;
+}
+
+SPIRES_EXPORT spires_status spires_read_weights(const spires_reservoir *r, double *buffer)
+{
+    if (!r || !buffer)
+        return SPIRES_ERR_INVALID_ARG;
+    if (r->m.n)
+        dense_from_csr(&r->m, buffer);
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT double *spires_copy_readout(const spires_reservoir *r)
+{
+    if (!r)
+        return NULL;
+    size_t cnt = r->m.dout * r->m.n;
+    double *buf = malloc((cnt ? cnt : 1) * sizeof(double));
+    if (!buf)
+        return NULL;
+    memcpy(buf, r->m.W_out, cnt * sizeof(double));
+    return buf;
+}
+
+SPIRES_EXPORT spires_status spires_read_readout(const spires_reservoir *r, double *buffer)
+{
+    if (!r || !buffer)
+        return SPIRES_ERR_INVALID_ARG;
+    memcpy(buffer, r->m.W_out, r->m.dout * r->m.n * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_compute_output(spires_reservoir *r, double *out)
+{
+    if (!r || !r->dev || !out)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_compute_output(r->dev, out));
+}
+
+SPIRES_EXPORT size_t spires_num_neurons(const spires_reservoir *r) { return r ? r->m.n : 0; }
+SPIRES_EXPORT size_t spires_num_inputs(const spires_reservoir *r) { return r ? r->m.din : 0; }
+SPIRES_EXPORT size_t spires_num_outputs(const spires_reservoir *r) { return r ? r->m.dout : 0; }
+
+/* -------------------------------------------------------- extensions -- */
+
+struct spires_ext_model {
+    sp_host_model m;
+};
+
+SPIRES_EXPORT spires_status spires_ext_model_build(const spires_reservoir_config *cfg,
+                                                   spires_ext_model **out)
+{
+    if (!cfg || !out)
+        return SPIRES_ERR_INVALID_ARG;
+    spires_ext_model *h = calloc(1, sizeof(*h));
+    if (!h)
+        return SPIRES_ERR_ALLOC;
+    int rc = model_from_config(cfg, &h->m);
+    if (!rc)
+        rc = sp_model_build(&h->m);
+    if (rc) {
+        sp_model_free(&h->m);
+        free(h);
+        return to_status(rc);
+    }
+    *out = h;
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT void spires_ext_model_free(spires_ext_model *h)
+{
+    if (!h)
+        return;
+    sp_model_free(&h->m);
+    free(h);
+}
+
+static void fill_info(const sp_host_model *m, spires_ext_model_info *info)
+{
+    memset(info, 0, sizeof(*info));
+    info->num_neurons = m->n;
+    info->num_inputs = m->din;
+    info->num_outputs = m->dout;
+    info->nnz = m->nnz;
+    info->ring_len = m->nc.L;
+    info->micro_steps = m->micro_steps;
+    info->syn_ring_len = m->sc.frac_L;
+    info->syn_components = m->sc.mexp_N;
+    info->spectral_radius_before_rescale = m->spectral_radius_before;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_info_get(const spires_ext_model *h,
+                                                      spires_ext_model_info *info)
+{
+    if (!h || !info)
+        return SPIRES_ERR_INVALID_ARG;
+    fill_info(&h->m, info);
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_csr(const spires_ext_model *h, int64_t *row_ptr,
+                                                 int32_t *col, double *val)
+{
+    if (!h)
+        return SPIRES_ERR_INVALID_ARG;
+    const sp_host_model *m = &h->m;
+    if (row_ptr)
+        memcpy(row_ptr, m->row_ptr, (m->n + 1) * sizeof(int64_t));
+    if (col)
+        memcpy(col, m->col, m->nnz * sizeof(int32_t));
+    if (val)
+        memcpy(val, m->w, m->nnz * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_w_in(const spires_ext_model *h, double *w_in)
+{
+    if (!h || !w_in)
+        return SPIRES_ERR_INVALID_ARG;
+    memcpy(w_in, h->m.W_in, h->m.n * h->m.din * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_w_out(const spires_ext_model *h, double *w_out)
+{
+    if (!h || !w_out)
+        return SPIRES_ERR_INVALID_ARG;
+    memcpy(w_out, h->m.W_out, h->m.n * h->m.dout * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_edge_tau(const spires_ext_model *h, double *tau)
+{
+    if (!h || !tau || !h->m.edge_tau)
+        return SPIRES_ERR_INVALID_ARG;
+    memcpy(tau, h->m.edge_tau, h->m.nnz * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_coef(const spires_ext_model *h, double *coef)
+{
+    if (!h || !coef || !h->m.coef)
+        return SPIRES_ERR_INVALID_ARG;
+    memcpy(coef, h->m.coef, (size_t)h->m.nc.L * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_run_record(spires_reservoir *r, const double *u, size_t T,
+                                                  double *phi, uint32_t *raster, double *y)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_run_args a;
+    memset(&a, 0, sizeof(a));
+    a.u = u;
+    a.T = T;
+    a.h_phi = phi;
+    a.h_raster = raster;
+    a.h_y = (y && r->m.dout) ? y : NULL;
+    a.sync = 1;
+    return to_status(sp_dev_run(r->dev, &a));
+}
+
+SPIRES_EXPORT spires_status spires_ext_run_device(spires_reservoir *r, const double *d_u,
+                                                  size_t T, double *d_phi, uint32_t *d_raster,
+                                                  double *d_y)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_run_args a;
+    memset(&a, 0, sizeof(a));
+    a.u = d_u;
+    a.u_on_device = 1;
+    a.T = T;
+    a.d_phi = d_phi;
+    a.d_raster = d_raster;
+    a.d_y = (d_y && r->m.dout) ? d_y : NULL;
+    return to_status(sp_dev_run(r->dev, &a));
+}
+
+SPIRES_EXPORT spires_status spires_ext_sync(spires_reservoir *r)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_sync(r->dev));
+}
+
+SPIRES_EXPORT void *spires_ext_stream(spires_reservoir *r)
+{
+    return (r && r->dev) ? sp_dev_stream(r->dev) : NULL;
+}
+
+SPIRES_EXPORT size_t spires_ext_spike_words(const spires_reservoir *r)
+{
+    return r ? (r->m.n + 31) / 32 : 0;
+}
+
+SPIRES_EXPORT long long spires_ext_kernel_launches(const spires_reservoir *r)
+{
+    return (r && r->dev) ? sp_dev_kernel_launches(r->dev) : 0;
+}
+
+SPIRES_EXPORT spires_status spires_ext_read_w_in(const spires_reservoir *r, double *w_in)
+{
+    if (!r || !w_in)
+        return SPIRES_ERR_INVALID_ARG;
+    memcpy(w_in, r->m.W_in, r->m.n * r->m.din * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_get_launch(const spires_reservoir *r,
+                                                  spires_ext_launch *l)
+{
+    if (!r || !r->dev || !l)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_launch s;
+    sp_dev_get_launch(r->dev, &s);
+    l->ctas = s.ctas;
+    l->warps_max = s.warps_max;
+    l->variant = s.variant;
+    l->stages = s.stages;
+    l->rows = s.rows;
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_set_launch(spires_reservoir *r,
+                                                  const spires_ext_launch *l)
+{
+    if (!r || !r->dev || !l)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_launch s = {l->ctas, l->warps_max, l->variant, l->stages, l->rows};
+    return to_status(sp_dev_set_launch(r->dev, &s));
+}
+
+SPIRES_EXPORT spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_set_seed(r->dev, seed));
+}
+
+SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
+                                                   const double *input_series,
+                                                   const double *target_series,
+                                                   size_t series_length, double lambda,
+                                                   const spires_ext_ridge_opts *opts,
+                                                   spires_ext_ridge_report *report)
+{
+    if (!r || !r->dev || !input_series || !target_series)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_opts o;
+    memset(&o, 0, sizeof(o));
+    o.gram_mode = sp_default_gram_mode();
+    o.max_refine = 30;
+    o.refine_tol = 1e-13;
+    if (opts) {
+        o.gram_mode = opts->gram_mode;
+        o.max_refine = opts->max_refine;
+        o.refine_tol = opts->refine_tol;
+        o.washout = opts->washout;
+    }
+    if (o.washout >= series_length)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_report rep;
+    memset(&rep, 0, sizeof(rep));
+    int rc = sp_model_derive_neuron(&r->m);
+    if (rc)
+        return to_status(rc);
+    rc = sp_dev_train_ridge(r->dev, &r->m, input_series, target_series, series_length, lambda,
+                            &o, &rep, r->m.W_out);
+    if (report) {
+        report->gram_mode_used = rep.gram_mode_used;
+        report->refine_iters = rep.refine_iters;
+        report->rel_residual = rep.rel_residual;
+        report->collect_ms = rep.collect_ms;
+        report->gram_ms = rep.gram_ms;
+        report->factor_ms = rep.factor_ms;
+        report->refine_ms = rep.refine_ms;
+        report->factor_failed = rep.factor_failed;
+        report->lu_fallback = rep.lu_fallback;
+    }
+    return to_status(rc);
+}

@@ -1,0 +1,889 @@
+/*
+ * construct.c -- host construction of a reservoir model.
+ *
+ * Weights are drawn with the C library's rand() in exactly the order the
+ * reference draws them, so a caller that seeds srand() gets the same W, W_in
+ * and W_out from this library as from the reference:
+ *
+ *   1. W_in, n*din draws of generate_weight          src/reservoir.c:378-383
+ *   2. recurrent topology                           src/reservoir.c:385-537
+ *   3. PSC_HETEROGENEOUS per-edge tau               src/synapses/psc_heterogeneous.c:60-89
+ *   4. spectral-radius rescale (no draws)           src/reservoir.c:548-557
+ *   5. W_out, n*dout draws of generate_weight(0.5)  src/reservoir.c:559-571
+ *
+ * The reference materialises a dense n x n scratch (3.2 GB at n = 20000) and an
+ * n x n byte adjacency for scale-free graphs; here rows are produced directly
+ * in CSR order and the Barabasi-Albert roulette runs on a Fenwick tree. Both
+ * choices give the same picks: the roulette totals are sums of small integers,
+ * which double arithmetic holds exactly, so "first u with r <= prefix(u)" is
+ * the same integer search either way.
+ *
+ * All libm-derived constants used by the dynamics (pow, exp, log, tgamma, sin,
+ * cos) are computed here with the same expressions the reference evaluates, so
+ * the device only ever sees their bits.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "sp_model.h"
+
+/* ---------------------------------------------------------------- draws -- */
+
+/* (double)rand()/RAND_MAX, src/reservoir.c:330-333 */
+static double urand01(void) { return (double)rand() / (double)RAND_MAX; }
+
+/* magnitude first, then the sign draw; src/reservoir.c:308-317 */
+static double draw_weight(double ei_ratio)
+{
+    double magnitude = (double)rand() / RAND_MAX;
+    if (((double)rand() / RAND_MAX) < ei_ratio)
+        return magnitude;
+    return -magnitude;
+}
+
+/* ------------------------------------------------------- triplet buffer -- */
+
+typedef struct {
+    int32_t r, c;
+    double v;
+} trip;
+
+typedef struct {
+    trip *t;
+    size_t n, cap;
+} tripbuf;
+
+static int tb_push(tripbuf *b, int32_t r, int32_t c, double v)
+{
+    if (b->n == b->cap) {
+        size_t nc = b->cap ? b->cap * 2 : 1024;
+        trip *nt = realloc(b->t, nc * sizeof(trip));
+        if (!nt)
+            return -1;
+        b->t = nt;
+        b->cap = nc;
+    }
+    b->t[b->n].r = r;
+    b->t[b->n].c = c;
+    b->t[b->n].v = v;
+    b->n++;
+    return 0;
+}
+
+static int trip_cmp(const void *a, const void *b)
+{
+    const trip *x = a, *y = b;
+    if (x->r != y->r)
+        return x->r < y->r ? -1 : 1;
+    if (x->c != y->c)
+        return x->c < y->c ? -1 : 1;
+    return 0;
+}
+
+/* Triplets (unique (r,c), any order) -> CSR with ascending columns, dropping
+ * entries equal to zero exactly as csr_build_from_dense does
+ * (src/sparse.c:7-42: `dense[k] != 0.0`). */
+static int csr_from_trips(sp_host_model *m, tripbuf *b, int sorted)
+{
+    size_t n = m->n;
+    if (!sorted)
+        qsort(b->t, b->n, sizeof(trip), trip_cmp);
+    size_t nnz = 0;
+    for (size_t k = 0; k < b->n; k++)
+        if (b->t[k].v != 0.0)
+            nnz++;
+    m->row_ptr = calloc(n + 1, sizeof(int64_t));
+    m->col = malloc((nnz ? nnz : 1) * sizeof(int32_t));
+    m->w = malloc((nnz ? nnz : 1) * sizeof(double));
+    if (!m->row_ptr || !m->col || !m->w)
+        return SP_EALLOC;
+    size_t idx = 0;
+    for (size_t k = 0; k < b->n; k++) {
+        if (b->t[k].v == 0.0)
+            continue;
+        m->row_ptr[b->t[k].r + 1]++;
+        m->col[idx] = b->t[k].c;
+        m->w[idx] = b->t[k].v;
+        idx++;
+    }
+    for (size_t i = 0; i < n; i++)
+        m->row_ptr[i + 1] += m->row_ptr[i];
+    m->nnz = nnz;
+    return SP_OK;
+}
+
+/* ------------------------------------------------------------ topologies -- */
+
+/* Erdos-Renyi directed, no self loops; src/reservoir.c:386-397 */
+static int topo_random(sp_host_model *m, tripbuf *b)
+{
+    size_t n = m->n;
+    for (size_t i = 0; i < n; i++)
+        for (size_t j = 0; j < n; j++) {
+            if (i == j)
+                continue;
+            if (urand01() < m->connectivity)
+                if (tb_push(b, (int32_t)i, (int32_t)j, draw_weight(m->ei_ratio)))
+                    return SP_EALLOC;
+        }
+    return SP_OK;
+}
+
+/* Watts-Strogatz on a directed ring; src/reservoir.c:399-443. The ring pass
+ * draws every ring weight before any rewiring draw, so ring weights are kept
+ * per row and each row is then rewired against its own dense scratch row. */
+static int topo_small_world(sp_host_model *m, tripbuf *b)
+{
+    size_t n = m->n;
+    if (n < 3)
+        return SP_OK;
+    int K = (int)((m->connectivity) * (double)(n - 1) + 0.5);
+    if (K < 2)
+        K = 2;
+    if (K % 2)
+        K++;
+    if (K >= (int)n)
+        K = (int)n - 1;
+    const double p = 0.1;
+    int half = K / 2;
+
+    double *ring = malloc((size_t)n * (size_t)(half > 0 ? half : 1) * sizeof(double));
+    double *row = calloc(n, sizeof(double));
+    int32_t *touched = malloc(((size_t)2 * half + 2) * sizeof(int32_t));
+    if (!ring || !row || !touched) {
+        free(ring);
+        free(row);
+        free(touched);
+        return SP_EALLOC;
+    }
+    for (size_t i = 0; i < n; i++)
+        for (int s = 1; s <= half; s++)
+            ring[i * half + (s - 1)] = draw_weight(m->ei_ratio);
+
+    for (size_t i = 0; i < n; i++) {
+        int nt = 0;
+        for (int s = 1; s <= half; s++) {
+            size_t j = (i + (size_t)s) % n;
+            row[j] = ring[i * half + (s - 1)];
+            touched[nt++] = (int32_t)j;
+        }
+        for (int s = 1; s <= half; s++) {
+            size_t j_old = (i + (size_t)s) % n;
+            if (urand01() < p) {
+                row[j_old] = 0.0;
+                size_t j_new;
+                int attempts = 0;
+                do {
+                    j_new = (size_t)(urand01() * (double)n);
+                    if (j_new >= n)
+                        j_new = n - 1;
+                    if (++attempts > 10 * (int)n)
+                        break;
+                } while (j_new == i || row[j_new] != 0.0);
+                if (j_new != i) {
+                    row[j_new] = draw_weight(m->ei_ratio);
+                    touched[nt++] = (int32_t)j_new;
+                }
+            }
+        }
+        /* emit the row in ascending column order, each column once */
+        for (int a = 1; a < nt; a++) { /* insertion sort: nt <= 2*half */
+            int32_t v = touched[a];
+            int c = a - 1;
+            while (c >= 0 && touched[c] > v) {
+                touched[c + 1] = touched[c];
+                c--;
+            }
+            touched[c + 1] = v;
+        }
+        for (int a = 0; a < nt; a++) {
+            if (a > 0 && touched[a] == touched[a - 1])
+                continue;
+            if (tb_push(b, (int32_t)i, touched[a], row[touched[a]])) {
+                free(ring);
+                free(row);
+                free(touched);
+                return SP_EALLOC;
+            }
+        }
+        for (int a = 0; a < nt; a++)
+            row[touched[a]] = 0.0;
+    }
+    free(ring);
+    free(row);
+    free(touched);
+    return SP_OK;
+}
+
+/* Fenwick tree over int64 weights (deg[u] + 1 per node). */
+typedef struct {
+    int64_t *t;
+    size_t n;
+} fenwick;
+
+static void fw_add(fenwick *f, size_t i, int64_t v)
+{
+    for (size_t k = i + 1; k <= f->n; k += k & (~k + 1))
+        f->t[k] += v;
+}
+
+/* smallest index u (0-based) with prefix(u) >= target, target >= 1;
+ * returns n if the total is below target */
+static size_t fw_lower_bound(const fenwick *f, int64_t target)
+{
+    size_t pos = 0;
+    size_t step = 1;
+    while (step * 2 <= f->n)
+        step *= 2;
+    for (; step; step >>= 1) {
+        if (pos + step <= f->n && f->t[pos + step] < target) {
+            pos += step;
+            target -= f->t[pos];
+        }
+    }
+    return pos; /* 0-based index of the element reaching target */
+}
+
+static int cmp_i32(const void *a, const void *b)
+{
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* Barabasi-Albert with initial attractiveness A = 1 and random orientation;
+ * src/reservoir.c:445-536 */
+static int topo_scale_free(sp_host_model *m, tripbuf *b)
+{
+    size_t n = m->n;
+    if (n < 2)
+        return SP_OK;
+    int mm = (int)((m->connectivity) * (double)(n - 1) + 0.5);
+    if (mm < 1)
+        mm = 1;
+    if (mm >= (int)n)
+        mm = (int)n - 1;
+    int m0 = mm > 2 ? mm : 2;
+    if (m0 >= (int)n)
+        m0 = (int)n - 1;
+
+    int rc = SP_EALLOC;
+    int64_t *deg = calloc(n, sizeof(int64_t));
+    fenwick fw = {calloc(n + 1, sizeof(int64_t)), n};
+    size_t max_edges = (size_t)m0 * (size_t)(m0 - 1) / 2 + (n - (size_t)m0) * (size_t)mm;
+    int32_t *eu = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
+    int32_t *ev = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
+    int32_t *picks = malloc((size_t)mm * sizeof(int32_t));
+    int64_t *adj_off = NULL;
+    int32_t *adj = NULL;
+    size_t ne = 0;
+    if (!deg || !fw.t || !eu || !ev || !picks)
+        goto done;
+
+    /* seed clique on m0 nodes */
+    for (int u = 0; u < m0; u++)
+        for (int v = u + 1; v < m0; v++) {
+            eu[ne] = u;
+            ev[ne] = v;
+            ne++;
+            deg[u]++;
+            deg[v]++;
+        }
+    for (size_t u = 0; u < n; u++)
+        fw_add(&fw, u, (u < (size_t)m0) ? deg[u] + 1 : 0);
+    int64_t degsum = 0;
+    for (int u = 0; u < m0; u++)
+        degsum += deg[u];
+
+    for (size_t v = (size_t)m0; v < n; v++) {
+        int added = 0, guard = 0;
+        while (added < mm && guard < 50 * mm) {
+            /* total = sum_{u<v} (deg[u] + A): an exact integer in double */
+            double total = (double)(degsum + (int64_t)v);
+            if (total <= 0.0)
+                total = (double)v;
+            double r = urand01() * total;
+            /* first u with r <= acc(u); acc(u) integral, so acc >= ceil(r) */
+            double cr = ceil(r);
+            size_t pick = 0;
+            if (cr <= 0.0) {
+                pick = 0;
+            } else {
+                size_t u = fw_lower_bound(&fw, (int64_t)cr);
+                pick = (u < v) ? u : 0; /* no u satisfies: pick stays 0 */
+            }
+            int dup = 0;
+            for (int a = 0; a < added; a++)
+                if (picks[a] == (int32_t)pick)
+                    dup = 1;
+            if (pick != v && !dup) {
+                picks[added++] = (int32_t)pick;
+                deg[v]++;
+                deg[pick]++;
+                degsum += 1; /* only deg[pick] counts in totals for u < v */
+                fw_add(&fw, pick, 1);
+            }
+            guard++;
+        }
+        while (added < mm) {
+            size_t pick = (size_t)(urand01() * (double)v);
+            if (pick >= v)
+                pick = v - 1;
+            int dup = 0;
+            for (int a = 0; a < added; a++)
+                if (picks[a] == (int32_t)pick)
+                    dup = 1;
+            if (pick != v && !dup) {
+                picks[added++] = (int32_t)pick;
+                deg[v]++;
+                deg[pick]++;
+                degsum += 1;
+                fw_add(&fw, pick, 1);
+            }
+        }
+        for (int a = 0; a < added; a++) {
+            eu[ne] = picks[a];
+            ev[ne] = (int32_t)v;
+            ne++;
+        }
+        /* node v joins the roulette for later nodes with weight deg[v] + A */
+        fw_add(&fw, v, deg[v] + 1);
+        degsum += deg[v];
+    }
+
+    /* undirected adjacency lists, sorted */
+    adj_off = calloc(n + 1, sizeof(int64_t));
+    adj = malloc(((2) * (ne) > 0 ? (2) * (ne) : 1) * sizeof(int32_t));
+    if (!adj_off || !adj)
+        goto done;
+    for (size_t e = 0; e < ne; e++) {
+        adj_off[eu[e] + 1]++;
+        adj_off[ev[e] + 1]++;
+    }
+    for (size_t u = 0; u < n; u++)
+        adj_off[u + 1] += adj_off[u];
+    {
+        int64_t *fill = malloc(n * sizeof(int64_t));
+        if (!fill)
+            goto done;
+        memcpy(fill, adj_off, n * sizeof(int64_t));
+        for (size_t e = 0; e < ne; e++) {
+            adj[fill[eu[e]]++] = ev[e];
+            adj[fill[ev[e]]++] = eu[e];
+        }
+        free(fill);
+    }
+    for (size_t u = 0; u < n; u++)
+        qsort(adj + adj_off[u], (size_t)(adj_off[u + 1] - adj_off[u]), sizeof(int32_t), cmp_i32);
+
+    /* orientation pass in row-major order over i < j */
+    for (size_t i = 0; i < n; i++)
+        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++) {
+            size_t j = (size_t)adj[k];
+            if (j <= i)
+                continue;
+            int fail;
+            if (urand01() < 0.5)
+                fail = tb_push(b, (int32_t)i, (int32_t)j, draw_weight(m->ei_ratio));
+            else
+                fail = tb_push(b, (int32_t)j, (int32_t)i, draw_weight(m->ei_ratio));
+            if (fail)
+                goto done;
+        }
+    rc = SP_OK;
+done:
+    free(deg);
+    free(fw.t);
+    free(eu);
+    free(ev);
+    free(picks);
+    free(adj_off);
+    free(adj);
+    return rc;
+}
+
+/* -------------------------------------------------------- power iteration -- */
+
+/* csr_spectral_radius, src/sparse.c:93-127 (max-abs normalised power
+ * iteration, tol 1e-6, at most 1000 iterations, x0 = 1). */
+double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
+                              const double *w)
+{
+    const unsigned int max_iter = 1000;
+    const double tol = 1e-6;
+    double *x = malloc((n ? n : 1) * sizeof(double));
+    double *y = malloc((n ? n : 1) * sizeof(double));
+    if (!x || !y) {
+        free(x);
+        free(y);
+        return NAN;
+    }
+    for (size_t i = 0; i < n; i++)
+        x[i] = 1.0;
+    double lambda_old = 0.0, lambda_new = 0.0;
+    for (unsigned int it = 0; it < max_iter; it++) {
+        for (size_t i = 0; i < n; i++) {
+            double s = 0.0;
+            for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++)
+                s += w[k] * x[col[k]];
+            y[i] = s;
+        }
+        lambda_new = 0.0;
+        for (size_t i = 0; i < n; i++) {
+            double a = fabs(y[i]);
+            if (a > lambda_new)
+                lambda_new = a;
+        }
+        for (size_t i = 0; i < n; i++)
+            x[i] = y[i] / lambda_new;
+        if (fabs(lambda_new - lambda_old) < tol)
+            break;
+        lambda_old = lambda_new;
+    }
+    free(x);
+    free(y);
+    return lambda_new;
+}
+
+/* ---------------------------------------------------------- validation -- */
+
+int sp_validate_config(size_t n, size_t din, size_t dout, double dt, int conn_type,
+                       int neuron_type, const double *neuron_params, int syn_type,
+                       int syn_backend)
+{
+    (void)din;
+    (void)dout;
+    if (n == 0 || n > (size_t)INT32_MAX)
+        return SP_EINVAL;
+    if (conn_type < SP_CONN_RANDOM || conn_type > SP_CONN_SCALE_FREE)
+        return SP_EINVAL;
+    if (neuron_type < SP_LIF_DISCRETE || neuron_type > SP_FLIF_DIFFUSIVE)
+        return SP_EINVAL;
+    if (syn_type < SP_SYN_SIMPLE || syn_type > SP_SYN_FRAC_MEXP)
+        return SP_EINVAL;
+    if (syn_backend != 0 && syn_backend != 1)
+        return SP_EINVAL;
+    if (!neuron_params)
+        return SP_EINVAL;
+    if (!(dt > 0.0))
+        return SP_EINVAL;
+    return SP_OK;
+}
+
+/* ------------------------------------------------------ neuron constants -- */
+
+/* GL coefficients, src/neuron.c:14-21: note the (float) cast of k. */
+static void gl_coeffs_float_k(double *c, double alpha, int L)
+{
+    c[0] = 1.0;
+    for (int k = 1; k < L; k++)
+        c[k] = c[k - 1] * (1.0 - (alpha + 1.0) / (float)k);
+}
+
+int sp_model_derive_neuron(sp_host_model *m)
+{
+    const double *p = m->neuron_params;
+    const double dt = m->dt;
+    sp_neuron_consts nc;
+    memset(&nc, 0, sizeof(nc));
+    if (!p)
+        return SP_EINVAL;
+    switch (m->neuron_type) {
+    case SP_LIF_DISCRETE: /* src/neurons/lif_discrete.c:12-41 */
+        nc.a = p[0];
+        nc.b = p[1];
+        nc.c = 1.0 - p[2];
+        nc.d = p[3];
+        nc.v_init = p[0];
+        break;
+    case SP_LIF_BIO: /* src/neurons/lif_bio.c:4-29 */
+        nc.a = p[0];
+        nc.b = p[1];
+        nc.c = p[2];
+        nc.d = p[3];
+        nc.v_init = p[0];
+        break;
+    case SP_FLIF_GL: { /* src/neurons/flif_gl.c:7-49, src/neuron.c:36-54 */
+        double T_mem = p[5];
+        int L = (T_mem > 0 && dt > 0) ? (int)(T_mem / dt) : 2000;
+        if (L > SP_MAX_MEM_LEN)
+            L = SP_MAX_MEM_LEN;
+        if (L < 1)
+            return SP_EINVAL; /* the reference divides by zero (step % 0) */
+        if (m->coef && m->nc.L != L)
+            return SP_EINVAL; /* ring length is fixed at creation */
+        nc.a = p[0];
+        nc.b = p[1];
+        nc.c = p[2];
+        nc.d = p[3];
+        nc.e = p[6];
+        nc.f = p[7];
+        nc.g = pow(dt, p[4]);
+        nc.v_init = p[2];
+        nc.tprev_init = p[7] + dt;
+        nc.L = L;
+        if (!m->coef) { /* computed once, with the creation-time alpha */
+            m->coef = malloc((size_t)L * sizeof(double));
+            if (!m->coef)
+                return SP_EALLOC;
+            gl_coeffs_float_k(m->coef, p[4], L);
+        }
+        break;
+    }
+    case SP_FLIF_CAPUTO: { /* src/neurons/flif_caputo.c:5-40 */
+        double T_mem = p[8];
+        int mem_len = (T_mem > 0) ? (int)(T_mem / dt) : SP_MAX_MEM_LEN;
+        if (mem_len > SP_MAX_MEM_LEN)
+            mem_len = SP_MAX_MEM_LEN;
+        int D = mem_len - 2;
+        if (D < 1)
+            return SP_EINVAL; /* the reference writes past a zero-length array */
+        if (m->coef && m->nc.L != D)
+            return SP_EINVAL;
+        double alpha = p[6];
+        nc.a = p[3];
+        nc.b = p[4];
+        nc.c = p[1];
+        nc.d = p[2];
+        nc.e = p[0];
+        nc.f = p[7];
+        nc.g = pow(dt, alpha) * tgamma(2.0 - alpha);
+        nc.v_init = p[4];
+        nc.tprev_init = 2 * p[7];
+        nc.L = D;
+        if (!m->coef) {
+            m->coef = malloc((size_t)D * sizeof(double));
+            if (!m->coef)
+                return SP_EALLOC;
+        }
+        /* every neuron recomputes its weights at init, so reset re-reads alpha */
+        for (int i = 0; i < D; i++) {
+            double x = i + 2;
+            m->coef[i] = pow(x, 1.0 - alpha) - pow(x - 1.0, 1.0 - alpha);
+        }
+        break;
+    }
+    case SP_FLIF_DIFFUSIVE: { /* src/neurons/flif_diffusive.c:67-136 */
+        double tau_m = p[3], alpha = p[4], P6 = p[5], ddt = dt;
+        if (tau_m <= 0.0)
+            tau_m = 1.0;
+        if (ddt <= 0.0)
+            ddt = 1e-3;
+        if (alpha < 0.0)
+            alpha = 0.0;
+        if (alpha > 1.0)
+            alpha = 1.0;
+        nc.a = p[0];
+        nc.b = p[1];
+        nc.c = p[2];
+        nc.d = p[6];
+        nc.e = ddt / tau_m;
+        nc.v_init = p[2];
+        if (alpha < 1.0) {
+            double t_min = 1.0 * ddt;
+            double t_max = (P6 > 0.0) ? P6 : 100.0 * tau_m;
+            if (t_max <= t_min)
+                t_max = t_min * 2.0;
+            nc.f = t_min;
+            nc.g = t_max;
+            nc.h = ddt;
+            nc.i = pow(alpha, 2.0);
+            nc.j = 6.0 * alpha;
+            nc.k = pow(t_min, 1.0 - nc.j);
+            nc.l = pow(t_max, 1.0 - nc.j);
+            nc.diff_stochastic = 1;
+        } else {
+            double t_ref = (P6 > 0.0) ? P6 : 0.0;
+            long s = 0;
+            if (t_ref > 0.0) {
+                s = (long)ceil(t_ref / ddt);
+                if (s < 0)
+                    s = 0;
+            }
+            nc.h = t_ref;
+            nc.det_refr_steps = (int)s;
+            nc.diff_stochastic = 0;
+        }
+        break;
+    }
+    default:
+        return SP_EINVAL;
+    }
+    m->nc = nc;
+    return SP_OK;
+}
+
+/* ----------------------------------------------------- synapse constants -- */
+
+/* GL derivative coefficients of the fractional synapse (double k),
+ * src/synapses/fractional.c:95-101 */
+static void gl_coeffs_double_k(double *c, double alpha, int L)
+{
+    c[0] = 1.0;
+    for (int k = 1; k < L; k++)
+        c[k] = c[k - 1] * (1.0 - (alpha + 1.0) / (double)k);
+}
+
+static double log_uniform_tau(double tau_min, double tau_max)
+{
+    double log_min = log(tau_min);
+    double log_max = log(tau_max);
+    return exp(log_min + urand01() * (log_max - log_min));
+}
+
+/* Per-type constants and draws of synapse_build_from_dense (src/synapse.c:3-30). */
+int sp_model_build_synapse(sp_host_model *m, const double *unused)
+{
+    (void)unused;
+    const double *sp = m->synapse_params;
+    const double dt = m->dt;
+    sp_synapse_consts sc;
+    memset(&sc, 0, sizeof(sc));
+    switch (m->syn_type) {
+    case SP_SYN_SIMPLE:
+        break;
+    case SP_SYN_PSC_HOM: { /* src/synapses/psc_homogeneous.c:25-84 */
+        double tau = sp ? sp[0] : 1.0;
+        double decay = exp(-dt / tau);
+        sc.decay = decay;
+        sc.omd = 1.0 - decay;
+        break;
+    }
+    case SP_SYN_PSC_HET: { /* src/synapses/psc_heterogeneous.c:34-89,206-229 */
+        double tmin = sp ? sp[0] : 1.0, tmax = sp ? sp[1] : 1.0;
+        size_t nnz = m->nnz, n = m->n;
+        m->edge_tau = malloc((nnz ? nnz : 1) * sizeof(double));
+        m->edge_decay = malloc((nnz ? nnz : 1) * sizeof(double));
+        m->edge_omd = malloc((nnz ? nnz : 1) * sizeof(double));
+        if (!m->edge_tau || !m->edge_decay || !m->edge_omd)
+            return SP_EALLOC;
+        if (m->syn_backend == 0) {
+            for (size_t k = 0; k < nnz; k++)
+                m->edge_tau[k] = log_uniform_tau(tmin, tmax);
+        } else {
+            /* dense storage draws a tau for every one of the n*n entries */
+            for (size_t i = 0; i < n; i++) {
+                int64_t k = m->row_ptr[i], kend = m->row_ptr[i + 1];
+                for (size_t j = 0; j < n; j++) {
+                    double t = log_uniform_tau(tmin, tmax);
+                    if (k < kend && (size_t)m->col[k] == j)
+                        m->edge_tau[k++] = t;
+                }
+            }
+        }
+        for (size_t k = 0; k < nnz; k++) {
+            double decay = exp(-dt / m->edge_tau[k]);
+            m->edge_decay[k] = decay;
+            m->edge_omd[k] = 1.0 - decay;
+        }
+        break;
+    }
+    case SP_SYN_FRAC: { /* src/synapses/fractional.c:40-61,103-142 */
+        double alpha = sp ? sp[0] : 1.0;
+        double tau = sp ? sp[1] : 1.0;
+        double T_mem = sp ? sp[2] : 10.0;
+        int L = (T_mem > 0 && dt > 0) ? (int)(T_mem / dt) : 2000;
+        if (L > SP_MAX_MEM_LEN)
+            L = SP_MAX_MEM_LEN;
+        if (L < 1)
+            L = 1;
+        m->syn_coef = malloc((size_t)L * sizeof(double));
+        if (!m->syn_coef)
+            return SP_EALLOC;
+        gl_coeffs_double_k(m->syn_coef, alpha, L);
+        sc.frac_L = L;
+        sc.frac_dta = pow(dt, alpha);
+        sc.frac_tau = tau;
+        break;
+    }
+    case SP_SYN_FRAC_MEXP: { /* src/synapses/fractional_multiexp.c:21-90,136-157 */
+        const double PI_ = 3.14159265358979323846;
+        double alpha = sp ? sp[0] : 0.5;
+        double tau_syn = sp ? sp[1] : 1.0;
+        double tau_min = sp ? sp[2] : 1.0;
+        double tau_max = sp ? sp[3] : 20.0;
+        int N = sp ? (int)(sp[4] + 0.5) : 8;
+        if (N < 1)
+            N = 1;
+        double sin_apia = sin(alpha * PI_);
+        int degenerate = fabs(sin_apia) < 1e-9;
+        int Nc = degenerate ? 1 : N;
+        m->mexp_tau = malloc((size_t)Nc * sizeof(double));
+        m->mexp_c = malloc((size_t)Nc * sizeof(double));
+        m->mexp_decay = malloc((size_t)Nc * sizeof(double));
+        m->mexp_omd = malloc((size_t)Nc * sizeof(double));
+        double *raw = malloc((size_t)Nc * sizeof(double));
+        if (!m->mexp_tau || !m->mexp_c || !m->mexp_decay || !m->mexp_omd || !raw) {
+            free(raw);
+            return SP_EALLOC;
+        }
+        if (degenerate) {
+            m->mexp_tau[0] = tau_syn;
+            m->mexp_c[0] = 1.0;
+        } else {
+            double log_tau_min = log(tau_min);
+            double log_tau_max = log(tau_max);
+            double d_log_tau = (N > 1) ? (log_tau_max - log_tau_min) / (N - 1) : 0.0;
+            double cos_apia = cos(alpha * PI_);
+            double sum_raw = 0.0;
+            for (int i = 0; i < N; i++) {
+                double log_tau_i = log_tau_min + i * d_log_tau;
+                double tau_i = exp(log_tau_i);
+                double x = tau_syn / tau_i;
+                double K = (1.0 / PI_) * pow(x, alpha - 1.0) * sin_apia /
+                           (pow(x, 2.0 * alpha) + 2.0 * pow(x, alpha) * cos_apia + 1.0);
+                double wq = K * x * d_log_tau;
+                if (wq < 0.0)
+                    wq = 0.0;
+                raw[i] = wq * tau_i;
+                m->mexp_tau[i] = tau_i;
+                sum_raw += raw[i];
+            }
+            for (int i = 0; i < N; i++)
+                m->mexp_c[i] = (sum_raw > 0.0) ? raw[i] / sum_raw : 1.0 / N;
+        }
+        free(raw);
+        for (int c = 0; c < Nc; c++) {
+            double decay = exp(-dt / m->mexp_tau[c]);
+            m->mexp_decay[c] = decay;
+            m->mexp_omd[c] = 1.0 - decay;
+        }
+        sc.mexp_N = Nc;
+        break;
+    }
+    default:
+        return SP_EINVAL;
+    }
+    m->sc = sc;
+    return SP_OK;
+}
+
+/* ------------------------------------------------------------- top level -- */
+
+int sp_model_build(sp_host_model *m)
+{
+    int rc;
+    size_t n = m->n;
+    m->micro_steps = (int)llround(1.0 / m->dt);
+
+    /* the reference initialises neurons before drawing weights; neuron init
+     * draws nothing, so the order does not matter for rand() */
+    rc = sp_model_derive_neuron(m);
+    if (rc)
+        return rc;
+
+    m->W_in = malloc(((n) * (m->din) > 0 ? (n) * (m->din) : 1) * sizeof(double));
+    m->W_out = malloc(((n) * (m->dout) > 0 ? (n) * (m->dout) : 1) * sizeof(double));
+    if (!m->W_in || !m->W_out)
+        return SP_EALLOC;
+
+    for (size_t k = 0; k < n * m->din; k++)
+        m->W_in[k] = draw_weight(m->ei_ratio);
+
+    tripbuf b = {0};
+    switch (m->conn_type) {
+    case SP_CONN_RANDOM:
+        rc = topo_random(m, &b);
+        if (!rc)
+            rc = csr_from_trips(m, &b, 1);
+        break;
+    case SP_CONN_SMALL_WORLD:
+        rc = topo_small_world(m, &b);
+        if (!rc)
+            rc = csr_from_trips(m, &b, 1);
+        break;
+    case SP_CONN_SCALE_FREE:
+        rc = topo_scale_free(m, &b);
+        if (!rc)
+            rc = csr_from_trips(m, &b, 0);
+        break;
+    default:
+        rc = SP_EINVAL;
+    }
+    free(b.t);
+    if (rc)
+        return rc;
+
+    rc = sp_model_build_synapse(m, NULL);
+    if (rc)
+        return rc;
+
+    /* rescale_weights, src/reservoir.c:548-557 */
+    double sr = sp_csr_spectral_radius(n, m->row_ptr, m->col, m->w);
+    m->spectral_radius_before = sr;
+    if (sr > 1e-9) {
+        double f = m->spectral_radius / sr;
+        for (size_t k = 0; k < m->nnz; k++)
+            m->w[k] = f * m->w[k];
+    }
+
+    /* randomize_output_layer, src/reservoir.c:559-571 */
+    for (size_t k = 0; k < n * m->dout; k++)
+        m->W_out[k] = draw_weight(0.5);
+
+    /* FLIF_DIFFUSIVE seeds: the reference hashes the heap address of each
+     * neuron (flif_diffusive.c:119-126), which no caller can reproduce; this
+     * library hashes the parameter bits and the neuron index instead. */
+    {
+        uint64_t s = 0x9E3779B97F4A7C15ULL;
+        for (int i = 0; i < 7 && m->neuron_type == SP_FLIF_DIFFUSIVE; i++) {
+            uint64_t bits;
+            memcpy(&bits, &m->neuron_params[i], sizeof(bits));
+            s ^= bits + 0x9E3779B97F4A7C15ULL + (s << 6) + (s >> 2);
+        }
+        m->diffusive_seed = s;
+    }
+    return SP_OK;
+}
+
+void sp_model_free(sp_host_model *m)
+{
+    if (!m)
+        return;
+    free(m->W_in);
+    free(m->W_out);
+    free(m->row_ptr);
+    free(m->col);
+    free(m->w);
+    free(m->coef);
+    free(m->edge_decay);
+    free(m->edge_omd);
+    free(m->edge_tau);
+    free(m->syn_coef);
+    free(m->mexp_decay);
+    free(m->mexp_omd);
+    free(m->mexp_c);
+    free(m->mexp_tau);
+    memset(m, 0, sizeof(*m));
+}
+
+/* Recurrent weights from a dense row-major matrix, then the synapse build
+ * (synapse_build_from_dense, src/synapse.c:3-30; PSC_HETEROGENEOUS draws its
+ * per-edge tau here). Used by coarse-graining, which builds its merged matrix
+ * densely (src/reservoir.c:951). */
+int sp_model_set_dense_weights(sp_host_model *m, const double *dense)
+{
+    size_t n = m->n, nnz = 0;
+    for (size_t k = 0; k < n * n; k++)
+        if (dense[k] != 0.0)
+            nnz++;
+    m->row_ptr = calloc(n + 1, sizeof(int64_t));
+    m->col = malloc((nnz ? nnz : 1) * sizeof(int32_t));
+    m->w = malloc((nnz ? nnz : 1) * sizeof(double));
+    if (!m->row_ptr || !m->col || !m->w)
+        return SP_EALLOC;
+    size_t idx = 0;
+    for (size_t i = 0; i < n; i++) {
+        m->row_ptr[i] = (int64_t)idx;
+        for (size_t j = 0; j < n; j++) {
+            double v = dense[i * n + j];
+            if (v != 0.0) {
+                m->col[idx] = (int32_t)j;
+                m->w[idx] = v;
+                idx++;
+            }
+        }
+    }
+    m->row_ptr[n] = (int64_t)idx;
+    m->nnz = nnz;
+    return sp_model_build_synapse(m, NULL);
+}

@@ -1,0 +1,860 @@
+// dev_readout.cu -- readout training on the device.
+//
+//   ridge  (src/reservoir.c:573-679): reset, record Phi[T][N] (no washout unless
+//          asked), A = Phi^T Phi + lambda I, B = Phi^T Y, solve A W = B.
+//          The reference forms A with dgemm and solves one LU (dgesv) per
+//          output; here A is factored once by a blocked Cholesky in FP64 and
+//          all outputs are solved together, followed by iterative refinement
+//          whose residual R = Phi^T (Y - Phi W) - lambda W is formed from the
+//          FP64 Phi itself. A non-positive pivot falls back to LU with partial
+//          pivoting, which is what dgesv does.
+//   RLS    (src/reservoir.c:681-767) and the online delta rule
+//          (src/reservoir.c:244-280), with W_out and P resident on the device.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <chrono>
+#include "sp_dev.h"
+#include "sp_kernels.cuh"
+#include "sp_dev_internal.h"
+#include "sp_gram.h"
+
+using namespace sp;
+
+#define RK(x)                                                                      \
+    do {                                                                           \
+        cudaError_t e_ = (x);                                                      \
+        if (e_ != cudaSuccess) {                                                   \
+            sp_dev_note_error(#x, e_);                                             \
+            rc = (e_ == cudaErrorMemoryAllocation) ? SP_EALLOC : SP_EINTERNAL;     \
+            goto out;                                                              \
+        }                                                                          \
+    } while (0)
+
+namespace {
+
+constexpr int NB = 64;  // Cholesky panel width
+
+// ---------------------------------------------------------------- Gram (FP64)
+// C = X^T X over rows [t0, t1) of X (T x n, row-major); lower tiles computed,
+// the upper triangle mirrored. 64x64 tile per CTA, 4x4 per thread.
+__global__ void __launch_bounds__(256) k_syrk_f64(const double *__restrict__ X, int n, size_t t0,
+                                                  size_t t1, double *__restrict__ C, int ldc)
+{
+    // tile index -> (bi, bj) with bi >= bj
+    int b = blockIdx.x;
+    int bi = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+    while (bi * (bi + 1) / 2 > b) --bi;
+    int bj = b - bi * (bi + 1) / 2;
+    const int i0 = bi * 64, j0 = bj * 64;
+    __shared__ double si[16][64 + 1];
+    __shared__ double sj[16][64 + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4] = {};
+    for (size_t t = t0; t < t1; t += 16) {
+        for (int q = threadIdx.x; q < 16 * 64; q += 256) {
+            int r = q >> 6, c = q & 63;
+            size_t tt = t + r;
+            si[r][c] = (tt < t1 && i0 + c < n) ? X[tt * n + i0 + c] : 0.0;
+            sj[r][c] = (tt < t1 && j0 + c < n) ? X[tt * n + j0 + c] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            double a[4], bb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u] = si[r][ty * 4 + u];
+                bb[u] = sj[r][tx * 4 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v)
+                    acc[u][v] = fma(a[u], bb[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+            if (i < n && j < n && j <= i) {
+                C[(size_t)i * ldc + j] = acc[u][v];
+                C[(size_t)j * ldc + i] = acc[u][v];
+            }
+        }
+}
+
+// R[i][o] = sum_{t in [t0,t1)} X[t][i] E[t][o] (- lam * W[i][o] when W != 0),
+// split over `parts` contiguous t ranges reduced in a fixed order.
+__global__ void k_xt_e_part(const double *__restrict__ X, int n, size_t t0, size_t t1,
+                            const double *__restrict__ E, int dout, int parts,
+                            double *__restrict__ part)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int pidx = blockIdx.y;
+    const size_t len = t1 - t0;
+    const size_t a = t0 + len * pidx / parts, b = t0 + len * (pidx + 1) / parts;
+    if (i >= n)
+        return;
+    double acc[16];
+    for (int o = 0; o < dout; ++o)
+        acc[o] = 0.0;
+    for (size_t t = a; t < b; ++t) {
+        double x = X[t * n + i];
+        for (int o = 0; o < dout; ++o)
+            acc[o] = fma(x, E[t * dout + o], acc[o]);
+    }
+    for (int o = 0; o < dout; ++o)
+        part[((size_t)pidx * n + i) * dout + o] = acc[o];
+}
+
+__global__ void k_reduce_parts(const double *__restrict__ part, int parts, int n, int dout,
+                               const double *__restrict__ W, double lam, double *__restrict__ R)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)n * dout;
+    if (k >= total)
+        return;
+    double s = 0.0;
+    for (int p = 0; p < parts; ++p)
+        s += part[(size_t)p * total + k];
+    if (W)
+        s -= lam * W[k];
+    R[k] = s;
+}
+
+// E[t][o] = Y[t][o] - sum_i X[t][i] W[i][o], one warp per row t.
+__global__ void k_resid_rows(const double *__restrict__ X, int n, size_t t0, size_t t1,
+                             const double *__restrict__ Y, const double *__restrict__ W,
+                             int dout, double *__restrict__ E)
+{
+    const size_t t = t0 + (size_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= t1)
+        return;
+    double acc[16];
+    for (int o = 0; o < dout; ++o)
+        acc[o] = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        double x = X[t * n + i];
+        for (int o = 0; o < dout; ++o)
+            acc[o] = fma(x, W[(size_t)i * dout + o], acc[o]);
+    }
+    for (int o = 0; o < dout; ++o) {
+        double s = acc[o];
+        for (int off = 16; off; off >>= 1)
+            s += __shfl_xor_sync(kFull, s, off);
+        if (lane == 0)
+            E[t * dout + o] = Y[t * dout + o] - s;
+    }
+}
+
+__global__ void k_add_diag(double *A, int n, int lda, double lam)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        A[(size_t)i * lda + i] += lam;
+}
+
+// ------------------------------------------------------- blocked Cholesky
+// A (n x n, row-major, lower triangle used) -> L in place.
+__global__ void k_potrf_diag(double *A, int n, int lda, int k0, int kb, int *info)
+{
+    __shared__ double s[NB][NB + 1];
+    if (*info)
+        return;
+    for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+        int r = q / kb, c = q % kb;
+        s[r][c] = A[(size_t)(k0 + r) * lda + k0 + c];
+    }
+    __syncthreads();
+    __shared__ int bad;
+    if (threadIdx.x == 0)
+        bad = 0;
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        if (threadIdx.x == 0) {
+            double d = s[j][j];
+            if (!(d > 0.0) || !isfinite(d)) {
+                bad = k0 + j + 1;
+                s[j][j] = 1.0;
+            } else {
+                s[j][j] = sqrt(d);
+            }
+        }
+        __syncthreads();
+        const double djj = s[j][j];
+        for (int r = j + 1 + threadIdx.x; r < kb; r += blockDim.x)
+            s[r][j] /= djj;
+        __syncthreads();
+        // trailing update of the diagonal block, lower part
+        for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+            int r = q / kb, c = q % kb;
+            if (r > j && c > j && c <= r)
+                s[r][c] -= s[r][j] * s[c][j];
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+        int r = q / kb, c = q % kb;
+        if (c <= r)
+            A[(size_t)(k0 + r) * lda + k0 + c] = s[r][c];
+    }
+    if (threadIdx.x == 0 && bad)
+        atomicCAS(info, 0, bad);
+}
+
+// rows r >= k0+kb: L[r][k0:k0+kb] = A[r][k0:k0+kb] * Lkk^{-T}
+__global__ void k_trsm_panel(double *A, int n, int lda, int k0, int kb, const int *info)
+{
+    __shared__ double L[NB][NB + 1];
+    if (*info)
+        return;
+    for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+        int r = q / kb, c = q % kb;
+        L[r][c] = (c <= r) ? A[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int r = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n)
+        return;
+    double x[NB];
+    double *row = A + (size_t)r * lda + k0;
+    for (int c = 0; c < kb; ++c) {
+        double v = row[c];
+        for (int q = 0; q < c; ++q)
+            v -= x[q] * L[c][q];
+        x[c] = v / L[c][c];
+    }
+    for (int c = 0; c < kb; ++c)
+        row[c] = x[c];
+}
+
+// trailing update A22 -= L21 L21^T on lower tiles of the trailing matrix
+__global__ void __launch_bounds__(256) k_syrk_update(double *A, int n, int lda, int k0, int kb,
+                                                     const int *info)
+{
+    if (*info)
+        return;
+    const int base = k0 + kb;
+    int b = blockIdx.x;
+    int bi = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+    while (bi * (bi + 1) / 2 > b) --bi;
+    int bj = b - bi * (bi + 1) / 2;
+    const int i0 = base + bi * 64, j0 = base + bj * 64;
+    __shared__ double si[64][33];
+    __shared__ double sj[64][33];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4] = {};
+    for (int c0 = 0; c0 < kb; c0 += 32) {
+        const int cw = (kb - c0 < 32) ? kb - c0 : 32;
+        for (int q = threadIdx.x; q < 64 * 32; q += 256) {
+            int r = q >> 5, c = q & 31;
+            si[r][c] = (c < cw && i0 + r < n) ? A[(size_t)(i0 + r) * lda + k0 + c0 + c] : 0.0;
+            sj[r][c] = (c < cw && j0 + r < n) ? A[(size_t)(j0 + r) * lda + k0 + c0 + c] : 0.0;
+        }
+        __syncthreads();
+        for (int c = 0; c < cw; ++c) {
+            double a[4], bb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u] = si[ty * 4 + u][c];
+                bb[u] = sj[tx * 4 + u][c];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v)
+                    acc[u][v] = fma(a[u], bb[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+            if (i < n && j < n && j <= i)
+                A[(size_t)i * lda + j] -= acc[u][v];
+        }
+}
+
+// ----------------------------------------------------- triangular solves
+// Forward L Z = B in place on Z (n x dout), panel by panel.
+__global__ void k_fwd_diag(const double *L, int lda, int k0, int kb, double *Z, int dout)
+{
+    const int o = threadIdx.x;
+    if (o >= dout)
+        return;
+    for (int r = 0; r < kb; ++r) {
+        double v = Z[(size_t)(k0 + r) * dout + o];
+        for (int c = 0; c < r; ++c)
+            v -= L[(size_t)(k0 + r) * lda + k0 + c] * Z[(size_t)(k0 + c) * dout + o];
+        Z[(size_t)(k0 + r) * dout + o] = v / L[(size_t)(k0 + r) * lda + k0 + r];
+    }
+}
+
+__global__ void k_fwd_update(const double *L, int n, int lda, int k0, int kb, double *Z, int dout)
+{
+    const int r = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n)
+        return;
+    for (int o = 0; o < dout; ++o) {
+        double v = 0.0;
+        for (int c = 0; c < kb; ++c)
+            v = fma(L[(size_t)r * lda + k0 + c], Z[(size_t)(k0 + c) * dout + o], v);
+        Z[(size_t)r * dout + o] -= v;
+    }
+}
+
+// Backward L^T X = Z, panels from the last one.
+__global__ void k_bwd_diag(const double *L, int lda, int k0, int kb, double *Z, int dout)
+{
+    const int o = threadIdx.x;
+    if (o >= dout)
+        return;
+    for (int r = kb - 1; r >= 0; --r) {
+        double v = Z[(size_t)(k0 + r) * dout + o];
+        for (int c = r + 1; c < kb; ++c)
+            v -= L[(size_t)(k0 + c) * lda + k0 + r] * Z[(size_t)(k0 + c) * dout + o];
+        Z[(size_t)(k0 + r) * dout + o] = v / L[(size_t)(k0 + r) * lda + k0 + r];
+    }
+}
+
+__global__ void k_bwd_update(const double *L, int lda, int k0, int kb, double *Z, int dout)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // rows i < k0
+    if (i >= k0)
+        return;
+    for (int o = 0; o < dout; ++o) {
+        double v = 0.0;
+        for (int c = 0; c < kb; ++c)
+            v = fma(L[(size_t)(k0 + c) * lda + i], Z[(size_t)(k0 + c) * dout + o], v);
+        Z[(size_t)i * dout + o] -= v;
+    }
+}
+
+// ------------------------------------------------ LU with partial pivoting
+// Unblocked right-looking LU, one column per step (fallback path only).
+__global__ void k_lu_pivot(double *A, int n, int lda, int j, int *piv, int *info)
+{
+    __shared__ double bv[256];
+    __shared__ int bi[256];
+    double best = -1.0;
+    int idx = j;
+    for (int r = j + threadIdx.x; r < n; r += blockDim.x) {
+        double v = fabs(A[(size_t)r * lda + j]);
+        if (v > best) {
+            best = v;
+            idx = r;
+        }
+    }
+    bv[threadIdx.x] = best;
+    bi[threadIdx.x] = idx;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            double o = bv[threadIdx.x + s];
+            int oi = bi[threadIdx.x + s];
+            if (o > bv[threadIdx.x] || (o == bv[threadIdx.x] && oi < bi[threadIdx.x])) {
+                bv[threadIdx.x] = o;
+                bi[threadIdx.x] = oi;
+            }
+        }
+        __syncthreads();
+    }
+    const int p = bi[0];
+    if (threadIdx.x == 0) {
+        piv[j] = p;
+        if (A[(size_t)p * lda + j] == 0.0 && *info == 0)
+            *info = j + 1;
+    }
+    if (p != j)
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            double t = A[(size_t)j * lda + c];
+            A[(size_t)j * lda + c] = A[(size_t)p * lda + c];
+            A[(size_t)p * lda + c] = t;
+        }
+}
+
+__global__ void k_lu_update(double *A, int n, int lda, int j)
+{
+    const double pv = A[(size_t)j * lda + j];
+    if (pv == 0.0)
+        return;
+    for (int r = j + 1 + blockIdx.x; r < n; r += gridDim.x) {
+        const double l = A[(size_t)r * lda + j] / pv;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            A[(size_t)r * lda + j] = l;
+        for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x)
+            A[(size_t)r * lda + c] -= l * A[(size_t)j * lda + c];
+    }
+}
+
+__global__ void k_lu_solve(const double *A, int n, int lda, const int *piv, double *Z, int dout)
+{
+    const int o = blockIdx.x;
+    if (o >= dout)
+        return;
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < n; ++j) {
+            int p = piv[j];
+            if (p != j) {
+                double t = Z[(size_t)j * dout + o];
+                Z[(size_t)j * dout + o] = Z[(size_t)p * dout + o];
+                Z[(size_t)p * dout + o] = t;
+            }
+        }
+        for (int r = 0; r < n; ++r) {
+            double v = Z[(size_t)r * dout + o];
+            for (int c = 0; c < r; ++c)
+                v -= A[(size_t)r * lda + c] * Z[(size_t)c * dout + o];
+            Z[(size_t)r * dout + o] = v;
+        }
+        for (int r = n - 1; r >= 0; --r) {
+            double v = Z[(size_t)r * dout + o];
+            for (int c = r + 1; c < n; ++c)
+                v -= A[(size_t)r * lda + c] * Z[(size_t)c * dout + o];
+            Z[(size_t)r * dout + o] = v / A[(size_t)r * lda + r];
+        }
+    }
+}
+
+__global__ void k_axpy(double *y, const double *x, size_t cnt)
+{
+    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < cnt)
+        y[k] += x[k];
+}
+
+// W (n x dout) -> W_out (dout x n)
+__global__ void k_transpose_w(const double *W, int n, int dout, double *W_out)
+{
+    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < (size_t)n * dout) {
+        int i = (int)(k / dout), o = (int)(k % dout);
+        W_out[(size_t)o * n + i] = W[k];
+    }
+}
+
+__global__ void k_sumsq(const double *x, size_t cnt, double *out)
+{
+    __shared__ double s[256];
+    double a = 0.0;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+         k += (size_t)gridDim.x * blockDim.x)
+        a = fma(x[k], x[k], a);
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int st = 128; st; st >>= 1) {
+        if (threadIdx.x < st)
+            s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        atomicAdd(out, s[0]);
+}
+
+// ------------------------------------------------------------------- RLS
+// Px = P x
+__global__ void k_gemv_rows(const double *__restrict__ P, int n, const double *__restrict__ x,
+                            double *__restrict__ y)
+{
+    const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n)
+        return;
+    double s = 0.0;
+    for (int c = lane; c < n; c += 32)
+        s = fma(P[(size_t)r * n + c], x[c], s);
+    for (int off = 16; off; off >>= 1)
+        s += __shfl_xor_sync(kFull, s, off);
+    if (lane == 0)
+        y[r] = s;
+}
+
+// scalars: denom = lambda + x.Px ; e = target - W_out x ; k = Px / denom
+__global__ void k_rls_scalars(const double *x, const double *Px, int n, double lambda,
+                              const double *W_out, int dout, const double *target,
+                              double *scal /* [0]=denom, [1..dout]=e */)
+{
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        s = fma(x[i], Px[i], s);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int st = 128; st; st >>= 1) {
+        if (threadIdx.x < st)
+            red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        scal[0] = lambda + red[0];
+    __syncthreads();
+    for (int o = 0; o < dout; ++o) {
+        double a = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            a = fma(W_out[(size_t)o * n + i], x[i], a);
+        red[threadIdx.x] = a;
+        __syncthreads();
+        for (int st = 128; st; st >>= 1) {
+            if (threadIdx.x < st)
+                red[threadIdx.x] += red[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            scal[1 + o] = target[o] - red[0];
+        __syncthreads();
+    }
+}
+
+// W_out += e k^T ; P = (P - denom k k^T) / lambda   with k = Px / denom
+__global__ void k_rls_update(double *P, int n, const double *Px, const double *scal, double lambda,
+                             double *W_out, int dout)
+{
+    const double denom = scal[0];
+    const double inv = 1.0 / denom;
+    const size_t total = (size_t)n * n;
+    const double sc = (lambda != 1.0) ? 1.0 / lambda : 1.0;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(q / n), c = (int)(q % n);
+        const double kr = inv * Px[r], kc = inv * Px[c];
+        double v = P[q] + kr * (-denom * kc);
+        P[q] = (lambda != 1.0) ? sc * v : v;
+    }
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < (size_t)dout * n;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int o = (int)(q / n), i = (int)(q % n);
+        W_out[q] += (inv * Px[i]) * scal[1 + o];
+    }
+}
+
+__global__ void k_diag_init(double *P, int n, double v)
+{
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < (size_t)n * n;
+         q += (size_t)gridDim.x * blockDim.x)
+        P[q] = ((q / n) == (q % n)) ? v : 0.0;
+}
+
+// online delta rule: W_out[o][i] += (lr * (target_o - y_o)) * x_i
+__global__ void k_online(double *W_out, int n, int dout, const double *x, const double *y,
+                         const double *target, double lr)
+{
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < (size_t)dout * n;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int o = (int)(q / n), i = (int)(q % n);
+        const double a = lr * (target[o] - y[o]);
+        W_out[q] = __dadd_rn(W_out[q], __dmul_rn(a, x[i]));
+    }
+}
+
+double ms_since(std::chrono::steady_clock::time_point t)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t)
+        .count();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ factor + solve
+// Factor A (n x n) in place; returns 0 or the 1-based failing pivot.
+static int cholesky_inplace(cudaStream_t s, double *A, int n, int *d_info)
+{
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int kb = (n - k0 < NB) ? n - k0 : NB;
+        k_potrf_diag<<<1, 256, 0, s>>>(A, n, n, k0, kb, d_info);
+        const int rest = n - k0 - kb;
+        if (rest > 0) {
+            k_trsm_panel<<<(rest + 63) / 64, 64, 0, s>>>(A, n, n, k0, kb, d_info);
+            const int nt = (rest + 63) / 64;
+            k_syrk_update<<<nt * (nt + 1) / 2, 256, 0, s>>>(A, n, n, k0, kb, d_info);
+        }
+    }
+    int h = 0;
+    cudaMemcpyAsync(&h, d_info, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h;
+}
+
+static void chol_solve(cudaStream_t s, const double *L, int n, double *Z, int dout)
+{
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int kb = (n - k0 < NB) ? n - k0 : NB;
+        k_fwd_diag<<<1, 32, 0, s>>>(L, n, k0, kb, Z, dout);
+        const int rest = n - k0 - kb;
+        if (rest > 0)
+            k_fwd_update<<<(rest + 127) / 128, 128, 0, s>>>(L, n, n, k0, kb, Z, dout);
+    }
+    const int last = ((n - 1) / NB) * NB;
+    for (int k0 = last; k0 >= 0; k0 -= NB) {
+        const int kb = (n - k0 < NB) ? n - k0 : NB;
+        k_bwd_diag<<<1, 32, 0, s>>>(L, n, k0, kb, Z, dout);
+        if (k0 > 0)
+            k_bwd_update<<<(k0 + 127) / 128, 128, 0, s>>>(L, n, k0, kb, Z, dout);
+    }
+}
+
+static int lu_factor_solve(cudaStream_t s, double *A, int n, int *d_piv, int *d_info, double *Z,
+                           int dout)
+{
+    for (int j = 0; j < n; ++j) {
+        k_lu_pivot<<<1, 256, 0, s>>>(A, n, n, j, d_piv, d_info);
+        int rows = n - j - 1;
+        if (rows > 0)
+            k_lu_update<<<rows < 1024 ? rows : 1024, 256, 0, s>>>(A, n, n, j);
+    }
+    int h = 0;
+    cudaMemcpyAsync(&h, d_info, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (h)
+        return h;
+    k_lu_solve<<<dout, 32, 0, s>>>(A, n, n, d_piv, Z, dout);
+    return 0;
+}
+
+// Residual R = Phi^T (Y - Phi W) - lambda W for rows [t0, t1).
+static void ridge_residual(cudaStream_t s, const double *Phi, int n, size_t t0, size_t t1,
+                           const double *Y, const double *W, int dout, double lambda, double *E,
+                           double *part, int parts, double *R)
+{
+    const size_t rows = t1 - t0;
+    k_resid_rows<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(Phi, n, t0, t1, Y, W, dout, E);
+    dim3 g((n + 127) / 128, parts);
+    k_xt_e_part<<<g, 128, 0, s>>>(Phi, n, t0, t1, E, dout, parts, part);
+    const size_t tot = (size_t)n * dout;
+    k_reduce_parts<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, parts, n, dout, W, lambda,
+                                                                 R);
+}
+
+static double device_norm(cudaStream_t s, const double *x, size_t cnt, double *d_tmp)
+{
+    cudaMemsetAsync(d_tmp, 0, sizeof(double), s);
+    k_sumsq<<<64, 256, 0, s>>>(x, cnt, d_tmp);
+    double h = 0.0;
+    cudaMemcpyAsync(&h, d_tmp, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return sqrt(h);
+}
+
+extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,
+                                  const double *h_y, size_t T, double lambda,
+                                  const sp_ridge_opts *o, sp_ridge_report *rep, double *h_W_out)
+{
+    int rc = SP_OK;
+    const int n = d->n, dout = d->dout;
+    cudaStream_t s = d->stream;
+    double *Phi = nullptr, *Y = nullptr, *A = nullptr, *Aw = nullptr, *B = nullptr, *W = nullptr,
+           *R = nullptr, *E = nullptr, *part = nullptr, *tmp = nullptr;
+    int *info = nullptr, *piv = nullptr;
+    const int parts = 64;
+    const size_t w0 = o->washout;
+    memset(rep, 0, sizeof(*rep));
+    if (dout == 0)
+        return SP_OK;
+    if (dout > 16)
+        return SP_EINVAL; /* per-thread accumulators below hold up to 16 outputs */
+    auto tstart = std::chrono::steady_clock::now();
+
+    rc = sp_dev_reset_neurons(d, m);
+    if (rc)
+        return rc;
+    RK(cudaMalloc(&Phi, (T ? T : 1) * (size_t)n * sizeof(double)));
+    RK(cudaMalloc(&Y, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(cudaMalloc(&A, (size_t)n * n * sizeof(double)));
+    RK(cudaMalloc(&B, (size_t)n * dout * sizeof(double)));
+    RK(cudaMalloc(&W, (size_t)n * dout * sizeof(double)));
+    RK(cudaMalloc(&R, (size_t)n * dout * sizeof(double)));
+    RK(cudaMalloc(&E, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(cudaMalloc(&part, (size_t)parts * n * dout * sizeof(double)));
+    RK(cudaMalloc(&tmp, 4 * sizeof(double)));
+    RK(cudaMalloc(&info, sizeof(int)));
+    RK(cudaMalloc(&piv, (size_t)n * sizeof(int)));
+    RK(cudaMemsetAsync(info, 0, sizeof(int), s));
+    RK(cudaMemcpyAsync(Y, h_y, T * dout * sizeof(double), cudaMemcpyHostToDevice, s));
+    {
+        sp_run_args a;
+        memset(&a, 0, sizeof(a));
+        a.u = h_u;
+        a.T = T;
+        a.d_phi = Phi;
+        a.sync = 1;
+        rc = sp_dev_run(d, &a);
+        if (rc)
+            goto out;
+    }
+    rep->collect_ms = ms_since(tstart);
+
+    {
+        auto tg = std::chrono::steady_clock::now();
+        int mode = o->gram_mode;
+        if (mode == 1 && sp_gram_bf16x3_available()) {
+            rc = sp_gram_bf16x3(s, Phi, n, w0, T, A, n);
+            if (rc)
+                goto out;
+        } else {
+            mode = 0;
+            const int nt = (n + 63) / 64;
+            k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(Phi, n, w0, T, A, n);
+        }
+        rep->gram_mode_used = mode;
+        dim3 g((n + 127) / 128, parts);
+        k_xt_e_part<<<g, 128, 0, s>>>(Phi, n, w0, T, Y, dout, parts, part);
+        const size_t tot = (size_t)n * dout;
+        k_reduce_parts<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, parts, n, dout, nullptr,
+                                                                     0.0, B);
+        k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, lambda);
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+        rep->gram_ms = ms_since(tg);
+    }
+
+    {
+        auto tf = std::chrono::steady_clock::now();
+        RK(cudaMemcpyAsync(W, B, (size_t)n * dout * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        int bad = cholesky_inplace(s, A, n, info);
+        if (bad) {
+            // dgesv semantics: LU with partial pivoting on the original matrix
+            rep->factor_failed = 1;
+            rep->lu_fallback = 1;
+            RK(cudaMemsetAsync(info, 0, sizeof(int), s));
+            if (rep->gram_mode_used == 1) {
+                rc = sp_gram_bf16x3(s, Phi, n, w0, T, A, n);
+                if (rc)
+                    goto out;
+            } else {
+                const int nt = (n + 63) / 64;
+                k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(Phi, n, w0, T, A, n);
+            }
+            k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, lambda);
+            int lbad = lu_factor_solve(s, A, n, piv, info, W, dout);
+            if (lbad) {
+                // singular: the reference leaves W_out unchanged and warns
+                fprintf(stderr, "Warning: Ridge regression failed (singular system).\n");
+                rc = SP_OK;
+                goto out;
+            }
+        } else {
+            chol_solve(s, A, n, W, dout);
+        }
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+        rep->factor_ms = ms_since(tf);
+    }
+
+    {
+        // iterative refinement with FP64 residuals from Phi itself
+        auto tr = std::chrono::steady_clock::now();
+        const double bnorm = device_norm(s, B, (size_t)n * dout, tmp);
+        int it = 0;
+        double rel = 0.0;
+        const int maxit = rep->lu_fallback ? 0 : o->max_refine;
+        for (;;) {
+            ridge_residual(s, Phi, n, w0, T, Y, W, dout, lambda, E, part, parts, R);
+            rel = device_norm(s, R, (size_t)n * dout, tmp) / (bnorm > 0 ? bnorm : 1.0);
+            if (rel <= o->refine_tol || it >= maxit)
+                break;
+            chol_solve(s, A, n, R, dout);
+            const size_t tot = (size_t)n * dout;
+            k_axpy<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, R, tot);
+            ++it;
+            if (rep->gram_mode_used == 0 && it >= 2)
+                ; /* FP64 Gram: refinement converges in one or two sweeps */
+        }
+        rep->refine_iters = it;
+        rep->rel_residual = rel;
+        rep->refine_ms = ms_since(tr);
+    }
+
+    {
+        const size_t tot = (size_t)n * dout;
+        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, d->W_out);
+        RK(cudaMemcpyAsync(h_W_out, d->W_out, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+    }
+out:
+    cudaStreamSynchronize(s);
+    void *bufs[] = {Phi, Y, A, Aw, B, W, R, E, part, tmp, info, piv};
+    for (void *b : bufs)
+        if (b)
+            cudaFree(b);
+    return rc;
+}
+
+extern "C" int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double *h_u,
+                                const double *h_y, size_t T, double delta, double lambda,
+                                double *h_W_out)
+{
+    int rc = SP_OK;
+    const int n = d->n, dout = d->dout;
+    cudaStream_t s = d->stream;
+    double *P = nullptr, *Px = nullptr, *scal = nullptr, *Yd = nullptr;
+    RK(cudaMalloc(&P, (size_t)n * n * sizeof(double)));
+    RK(cudaMalloc(&Px, (size_t)n * sizeof(double)));
+    RK(cudaMalloc(&scal, (size_t)(dout + 1) * sizeof(double)));
+    RK(cudaMalloc(&Yd, (T ? T : 1) * (size_t)(dout ? dout : 1) * sizeof(double)));
+    k_diag_init<<<1024, 256, 0, s>>>(P, n, 1.0 / delta);
+    RK(cudaMemsetAsync(d->W_out, 0, (size_t)n * dout * sizeof(double), s));
+    if (T && dout)
+        RK(cudaMemcpyAsync(Yd, h_y, T * dout * sizeof(double), cudaMemcpyHostToDevice, s));
+    rc = sp_dev_reset_neurons(d, m);
+    if (rc)
+        goto out;
+    for (size_t t = 0; t < T; ++t) {
+        sp_run_args a;
+        memset(&a, 0, sizeof(a));
+        a.u = h_u ? h_u + t * d->din : nullptr;
+        a.T = 1;
+        rc = sp_dev_run(d, &a);
+        if (rc)
+            goto out;
+        k_gemv_rows<<<(n + 7) / 8, 256, 0, s>>>(P, n, d->V, Px);
+        k_rls_scalars<<<1, 256, 0, s>>>(d->V, Px, n, lambda, d->W_out, dout, Yd + t * dout, scal);
+        k_rls_update<<<4 * d->num_sms, 256, 0, s>>>(P, n, Px, scal, lambda, d->W_out, dout);
+    }
+    RK(cudaMemcpyAsync(h_W_out, d->W_out, (size_t)n * dout * sizeof(double),
+                       cudaMemcpyDeviceToHost, s));
+    RK(cudaStreamSynchronize(s));
+    RK(cudaGetLastError());
+out:
+    cudaStreamSynchronize(s);
+    if (P) cudaFree(P);
+    if (Px) cudaFree(Px);
+    if (scal) cudaFree(scal);
+    if (Yd) cudaFree(Yd);
+    return rc;
+}
+
+extern "C" int sp_dev_train_online(sp_dev *d, const double *h_target, double lr, double *h_W_out)
+{
+    int rc = SP_OK;
+    const int n = d->n, dout = d->dout;
+    cudaStream_t s = d->stream;
+    if (dout == 0)
+        return SP_OK;
+    // prediction with the same readout kernel as spires_compute_output
+    rc = sp_dev_readout(d, d->V, 1, d->d_y);
+    if (rc)
+        return rc;
+    RK(cudaMemcpyAsync(d->d_y + dout, h_target, (size_t)dout * sizeof(double),
+                       cudaMemcpyHostToDevice, s));
+    k_online<<<(unsigned)(((size_t)n * dout + 255) / 256), 256, 0, s>>>(d->W_out, n, dout, d->V,
+                                                                       d->d_y, d->d_y + dout, lr);
+    RK(cudaMemcpyAsync(h_W_out, d->W_out, (size_t)n * dout * sizeof(double),
+                       cudaMemcpyDeviceToHost, s));
+    RK(cudaStreamSynchronize(s));
+    RK(cudaGetLastError());
+out:
+    return rc;
+}

@@ -1,0 +1,454 @@
+/*
+ * optimize.c -- spires_optimize: AGILE hyper-parameter search over the public
+ * API (src/spires_api.c:263-498, src/spires_opt_agile.c, src/agile.c).
+ *
+ * The search logic is the reference's, step for step, so that a caller gets
+ * the same sequence of candidate configurations for the same losses:
+ *   - PCG32 generator with the reference's increment (src/agile.c:10-23);
+ *   - two-point SPSA with Rademacher signs, clamped probes (src/agile.c:114-142);
+ *   - truncated power-law (Levy) step length on [eta_min, eta_max]
+ *     (src/agile.c:99-110), reflection at the bounds (src/agile.c:32-49);
+ *   - exploration with patience (x0.9 per improvement, floor 1), then SPSA
+ *     gradient-descent refinement from the best point (src/agile.c:217-335);
+ *   - one AGILE run per budget, warm-started from the previous best, 8-D theta
+ *     with the reference's bounds, start point and options
+ *     (src/spires_opt_agile.c:47-190).
+ * Every loss evaluation builds, trains and validates reservoirs through this
+ * library, so the simulation and ridge solves run on the GPU. The validation
+ * pass (src/spires_api.c:298-342) runs as one launch with the readout fused
+ * in; its per-step outputs are the same bits spires_step + spires_compute_output
+ * would produce.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "../../include/spires.h"
+#include "../../include/spires_ext.h"
+#include "sp_api_internal.h"
+
+#define SPIRES_EXPORT __attribute__((visibility("default")))
+
+static int verbose(void) { return getenv("SPIRES_VERBOSE") != NULL; }
+
+/* ------------------------------------------------------------ generator -- */
+
+static uint32_t pcg32_next(uint64_t *s)
+{
+    uint64_t old = *s;
+    *s = old * 6364136223846793005ULL + 0xda3e39cb94b95bdbULL;
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((-rot) & 31));
+}
+
+static double pcg_uniform(uint64_t *s) { return pcg32_next(s) * (1.0 / 4294967296.0); }
+
+/* -------------------------------------------------------------- AGILE core -- */
+
+typedef double (*loss_fn)(const double *theta, int dim, void *ctx);
+
+typedef struct {
+    double mu, eta_min, eta_max, patience0, patience_decay;
+    double refine_step;
+    int refine_max_iters, refine_no_improve;
+    double spsa_eps;
+    int reflect;
+    uint64_t seed;
+} agile_opts;
+
+typedef struct {
+    double best_loss;
+    int best_iter, total_evals, total_iters, refined;
+} agile_report;
+
+static double clampd(double x, double a, double b) { return x < a ? a : (x > b ? b : x); }
+
+static void project(double *x, const double *lo, const double *hi, int d, int reflect)
+{
+    for (int i = 0; i < d; i++) {
+        if (!reflect) {
+            x[i] = clampd(x[i], lo[i], hi[i]);
+        } else if (x[i] < lo[i]) {
+            double over = lo[i] - x[i], span = hi[i] - lo[i];
+            double k = floor(over / span);
+            x[i] = lo[i] + (over - k * span);
+        } else if (x[i] > hi[i]) {
+            double over = x[i] - hi[i], span = hi[i] - lo[i];
+            double k = floor(over / span);
+            x[i] = hi[i] - (over - k * span);
+        }
+    }
+}
+
+static void spsa(const double *th, const double *lo, const double *hi, int d, double eps,
+                 loss_fn f, void *ctx, uint64_t *rng, double *g)
+{
+    double delta[64], tp[64], tm[64];
+    for (int i = 0; i < d; i++) {
+        delta[i] = (pcg32_next(rng) & 1) ? 1.0 : -1.0;
+        tp[i] = clampd(th[i] + eps * delta[i], lo[i], hi[i]);
+        tm[i] = clampd(th[i] - eps * delta[i], lo[i], hi[i]);
+    }
+    double fp = f(tp, d, ctx);
+    double fm = f(tm, d, ctx);
+    double scale = (fp - fm) / (2.0 * eps);
+    for (int i = 0; i < d; i++)
+        g[i] = scale * delta[i];
+}
+
+static double levy_step(double mu, double a, double b, uint64_t *rng)
+{
+    if (mu <= 1.0)
+        mu = 1.000001;
+    double u = pcg_uniform(rng);
+    double c1 = pow(a, 1.0 - mu), c2 = pow(b, 1.0 - mu);
+    return pow(c1 + (c2 - c1) * u, 1.0 / (1.0 - mu));
+}
+
+static int agile_run(const double *theta0, const double *lo, const double *hi, int d, loss_fn f,
+                     void *ctx, const agile_opts *o, double *best_theta, agile_report *rep)
+{
+    if (d > 64)
+        return -1;
+    double th[64], cand[64], g[64], dir[64];
+    double refine_step = o->refine_step > 0.0 ? o->refine_step : o->eta_min;
+    uint64_t rng = o->seed ? o->seed : 0xA57B17E5ULL;
+
+    memcpy(th, theta0, (size_t)d * sizeof(double));
+    project(th, lo, hi, d, o->reflect);
+    double loss = f(th, d, ctx);
+    double best = loss;
+    memcpy(best_theta, th, (size_t)d * sizeof(double));
+    int evals = 1, iters = 0, best_iter = 0, refined = 0;
+    double patience = o->patience0;
+    int since = 0;
+
+    for (;;) {
+        iters++;
+        spsa(th, lo, hi, d, o->spsa_eps, f, ctx, &rng, g);
+        evals += 2;
+        double s = 0.0;
+        for (int i = 0; i < d; i++)
+            s += g[i] * g[i];
+        double gn = sqrt(s);
+        if (gn > 1e-18) {
+            for (int i = 0; i < d; i++)
+                dir[i] = (-1.0 / gn) * g[i];
+        } else {
+            double ss = 0.0;
+            for (int i = 0; i < d; i++) {
+                double z = pcg_uniform(&rng) * 2.0 - 1.0;
+                dir[i] = z;
+                ss += z * z;
+            }
+            double nn = sqrt(ss) + 1e-18;
+            for (int i = 0; i < d; i++)
+                dir[i] /= nn;
+        }
+        double eta = levy_step(o->mu, o->eta_min, o->eta_max, &rng);
+        for (int i = 0; i < d; i++)
+            cand[i] = th[i] + eta * dir[i];
+        project(cand, lo, hi, d, o->reflect);
+        double cl = f(cand, d, ctx);
+        evals++;
+        if (cl < loss) {
+            memcpy(th, cand, (size_t)d * sizeof(double));
+            loss = cl;
+            since = 0;
+            patience *= o->patience_decay;
+            if (patience < 1.0)
+                patience = 1.0;
+            if (loss < best) {
+                best = loss;
+                best_iter = iters;
+                memcpy(best_theta, th, (size_t)d * sizeof(double));
+            }
+            if (verbose())
+                printf("[AGILE] iter %d improved: loss=%.6g, patience=%.2f\n", iters, loss,
+                       patience);
+        } else {
+            since++;
+        }
+        if (since >= (int)ceil(patience)) {
+            refined = 1;
+            break;
+        }
+        if (iters > 1000000)
+            break;
+    }
+
+    if (refined) {
+        memcpy(th, best_theta, (size_t)d * sizeof(double));
+        loss = best;
+        int no_imp = 0;
+        for (int k = 0; k < o->refine_max_iters; ++k) {
+            iters++;
+            spsa(th, lo, hi, d, o->spsa_eps, f, ctx, &rng, g);
+            evals += 2;
+            for (int i = 0; i < d; i++)
+                th[i] += -refine_step * g[i];
+            project(th, lo, hi, d, o->reflect);
+            double nl = f(th, d, ctx);
+            evals++;
+            if (nl < loss - 1e-12) {
+                loss = nl;
+                if (loss < best) {
+                    best = loss;
+                    best_iter = iters;
+                    memcpy(best_theta, th, (size_t)d * sizeof(double));
+                }
+                no_imp = 0;
+            } else {
+                no_imp++;
+            }
+            if (no_imp >= o->refine_no_improve)
+                break;
+        }
+    }
+    if (rep) {
+        rep->best_loss = best;
+        rep->best_iter = best_iter;
+        rep->total_evals = evals;
+        rep->total_iters = iters;
+        rep->refined = refined;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------ spires objective -- */
+
+static size_t snap_n(double x)
+{
+    static const size_t choices[] = {200, 400, 800, 1200};
+    size_t best = choices[0];
+    double bd = fabs(x - (double)choices[0]);
+    for (size_t i = 1; i < 4; i++) {
+        double dd = fabs(x - (double)choices[i]);
+        if (dd < bd) {
+            bd = dd;
+            best = choices[i];
+        }
+    }
+    return best;
+}
+
+static int snap_topo(double t)
+{
+    int k = (int)llround(t);
+    if (k < 0)
+        k = 0;
+    if (k > 2)
+        k = 2;
+    return k;
+}
+
+typedef struct {
+    double alpha, rho, gain, conn, ei, log10_ridge, n_cont, topo_cont;
+} opt_params;
+
+typedef struct {
+    double data_fraction;
+    int num_seeds;
+} budget;
+
+typedef struct {
+    const spires_reservoir_config *base;
+    const double *x, *y;
+    size_t n;
+    int alpha_index;
+    const budget *bud;
+    double lambda_var, lambda_cost;
+} opt_ctx;
+
+/* mean squared error of one-step readouts over [off, off+len) */
+static double validation_mse(spires_reservoir *r, const double *x, const double *y, size_t off,
+                             size_t len, size_t din, size_t dout)
+{
+    if (len == 0 || dout == 0)
+        return INFINITY;
+    double *yhat = malloc(len * dout * sizeof(double));
+    if (!yhat)
+        return INFINITY;
+    if (spires_ext_run_record(r, x + off * din, len, NULL, NULL, yhat) != SPIRES_OK) {
+        free(yhat);
+        return INFINITY;
+    }
+    const double *yb = y + off * dout;
+    double se = 0.0;
+    for (size_t t = 0; t < len; t++)
+        for (size_t o = 0; o < dout; o++) {
+            double e = yb[t * dout + o] - yhat[t * dout + o];
+            se += e * e;
+        }
+    free(yhat);
+    return se / (double)(len * dout);
+}
+
+static int evaluate(const opt_params *pr, const budget *b, const opt_ctx *ctx, double *mean_out,
+                    double *std_out, double *cost_out, int *feasible)
+{
+    spires_reservoir_config cfg = *ctx->base;
+    cfg.num_neurons = snap_n(pr->n_cont);
+    cfg.spectral_radius = pr->rho;
+    cfg.input_strength = pr->gain;
+    cfg.connectivity = pr->conn;
+    cfg.ei_ratio = pr->ei;
+    cfg.connectivity_type = (spires_connectivity_type)snap_topo(pr->topo_cont);
+    double local_params[8] = {0};
+    if (!cfg.neuron_params)
+        cfg.neuron_params = local_params;
+    /* written through the caller's array, as src/spires_api.c:362-365 does */
+    cfg.neuron_params[ctx->alpha_index] = pr->alpha;
+
+    const size_t din = cfg.num_inputs ? cfg.num_inputs : 1;
+    const size_t dout = cfg.num_outputs ? cfg.num_outputs : 1;
+    size_t n_train = (size_t)((double)ctx->n * fmax(0.0, fmin(1.0, b->data_fraction)));
+    if (n_train < 8 || ctx->n <= n_train) {
+        *feasible = 0;
+        *mean_out = 0.0;
+        *std_out = 1.0;
+        *cost_out = 1.0;
+        return 0;
+    }
+    size_t n_valid = ctx->n - n_train;
+    const int seeds = b->num_seeds > 0 ? b->num_seeds : 1;
+    double sum = 0.0, sum2 = 0.0;
+    int ok = 0;
+    for (int s = 0; s < seeds; s++) {
+        spires_reservoir *r = NULL;
+        if (spires_reservoir_create(&cfg, &r) != SPIRES_OK || !r)
+            continue;
+        double lambda = pow(10.0, pr->log10_ridge);
+        if (spires_train_ridge(r, ctx->x, ctx->y, n_train, lambda) != SPIRES_OK) {
+            spires_reservoir_destroy(r);
+            continue;
+        }
+        if (spires_reservoir_reset(r) != SPIRES_OK) {
+            spires_reservoir_destroy(r);
+            continue;
+        }
+        double mse = validation_mse(r, ctx->x, ctx->y, n_train, n_valid, din, dout);
+        spires_reservoir_destroy(r);
+        if (!isfinite(mse) || mse < 0.0)
+            continue;
+        double metric = 1.0 / (1.0 + mse);
+        sum += metric;
+        sum2 += metric * metric;
+        ok++;
+    }
+    if (ok == 0) {
+        *feasible = 0;
+        *mean_out = 0.0;
+        *std_out = 1.0;
+        *cost_out = 1.0;
+        return 0;
+    }
+    double mean = sum / (double)ok;
+    double var = fmax(0.0, (sum2 / (double)ok) - mean * mean);
+    *mean_out = mean;
+    *std_out = sqrt(var);
+    double sparsity = cfg.connectivity > 1e-8 ? cfg.connectivity : 1e-8;
+    *cost_out = (double)cfg.num_neurons * (1.0 / sparsity) * 1e-6;
+    *feasible = 1;
+    return 0;
+}
+
+static void theta_to_params(const double *th, opt_params *p)
+{
+    p->alpha = th[0];
+    p->rho = th[1];
+    p->gain = th[2];
+    p->conn = th[3];
+    p->ei = th[4];
+    p->log10_ridge = th[5];
+    p->n_cont = th[6];
+    p->topo_cont = th[7];
+}
+
+static double objective(const double *theta, int dim, void *vctx)
+{
+    (void)dim;
+    const opt_ctx *ctx = (const opt_ctx *)vctx;
+    opt_params p;
+    theta_to_params(theta, &p);
+    p.n_cont = (double)snap_n(p.n_cont);
+    p.topo_cont = (double)snap_topo(p.topo_cont);
+    double mean = 0, sd = 0, cost = 0;
+    int feasible = 1;
+    int rc = evaluate(&p, ctx->bud, ctx, &mean, &sd, &cost, &feasible);
+    if (rc != 0 || !feasible)
+        return 1e6;
+    return -(mean - ctx->lambda_var * sd - ctx->lambda_cost * cost);
+}
+
+SPIRES_EXPORT int spires_optimize(const spires_reservoir_config *base_config,
+                                  const struct spires_opt_budget *budgets_pub, int num_budgets,
+                                  const struct spires_opt_score *score_pub,
+                                  struct spires_opt_result *out_pub, const double *input_series,
+                                  const double *target_series, size_t series_length)
+{
+    if (verbose())
+        printf("[SPIRES] spires_optimize entered\n");
+    if (!base_config || !budgets_pub || num_budgets <= 0 || !score_pub || !out_pub)
+        return -1;
+    budget *buds = calloc((size_t)num_budgets, sizeof(budget));
+    if (!buds)
+        return -2;
+    for (int i = 0; i < num_budgets; i++) {
+        buds[i].data_fraction = budgets_pub[i].data_fraction;
+        buds[i].num_seeds = budgets_pub[i].num_seeds;
+    }
+    opt_ctx ctx = {base_config, input_series, target_series, series_length, 4, NULL,
+                   score_pub->lambda_var, score_pub->lambda_cost};
+
+    enum { D = 8 };
+    const double lo[D] = {0.05, 0.75, 0.20, 0.08, 0.70, -5.0, 200.0, 0.0};
+    const double hi[D] = {1.0, 1.05, 1.50, 0.35, 1.10, -1.0, 1200.0, 2.0};
+    double th0[D] = {0.55, 0.90, 1.00, 0.20, 0.80, -2.0, 400.0, 0.0};
+    double thb[D];
+    agile_opts o = {1.3, 1e-3, 0.3, 100.0, 0.9, 1e-2, 600, 60, 1e-3, 1, 0xA91EULL};
+    for (int i = 0; i < num_budgets; i++) {
+        ctx.bud = &buds[i];
+        agile_report rep;
+        if (agile_run(th0, lo, hi, D, objective, &ctx, &o, thb, &rep) != 0) {
+            free(buds);
+            return -1;
+        }
+        if (verbose())
+            printf("[AGILE] budget %d: best loss %.6g after %d evaluations\n", i, rep.best_loss,
+                   rep.total_evals);
+        memcpy(th0, thb, sizeof(th0));
+    }
+
+    opt_params pb;
+    theta_to_params(thb, &pb);
+    pb.n_cont = (double)snap_n(pb.n_cont);
+    pb.topo_cont = (double)snap_topo(pb.topo_cont);
+    double mean = 0, sd = 0, cost = 0;
+    int feasible = 1;
+    (void)evaluate(&pb, &buds[num_budgets - 1], &ctx, &mean, &sd, &cost, &feasible);
+    free(buds);
+
+    out_pub->best_config = *base_config;
+    out_pub->best_config.num_neurons = snap_n(pb.n_cont);
+    out_pub->best_config.spectral_radius = pb.rho;
+    out_pub->best_config.input_strength = pb.gain;
+    out_pub->best_config.connectivity = pb.conn;
+    out_pub->best_config.ei_ratio = pb.ei;
+    out_pub->best_config.connectivity_type = (spires_connectivity_type)snap_topo(pb.topo_cont);
+    out_pub->best_log10_ridge = pb.log10_ridge;
+    out_pub->metric_mean = mean;
+    out_pub->metric_std = sd;
+    out_pub->best_score = mean - score_pub->lambda_var * sd - score_pub->lambda_cost * cost;
+    return 0;
+}
+
+int sp_default_gram_mode(void)
+{
+    const char *e = getenv("SPIRES_RIDGE_GRAM");
+    if (e && (!strcmp(e, "bf16x3") || !strcmp(e, "1")))
+        return 1;
+    return 0;
+}

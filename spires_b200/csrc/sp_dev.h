@@ -1,0 +1,103 @@
+/*
+ * sp_dev.h -- C ABI of the CUDA layer (device state of one reservoir).
+ *
+ * The host C code (api.c) owns an sp_host_model and one sp_dev per reservoir.
+ * Every function returns an SP_* status; CUDA errors map to SP_EINTERNAL and
+ * device allocation failures to SP_EALLOC. No function allocates device memory
+ * except sp_dev_create, sp_dev_destroy-paired buffers and the ridge/RLS
+ * working sets (which the reference also allocates per call).
+ */
+#ifndef SP_DEV_H
+#define SP_DEV_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "sp_model.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sp_dev sp_dev;
+
+/* Launch shape of the persistent step kernel. */
+typedef struct {
+    int ctas;        /* CTAs in the cooperative grid (1 = no grid barrier) */
+    int warps_max;   /* warps per CTA (blockDim = 32 * warps_max) */
+    int variant;     /* 0 = generic ring loads, 1 = bulk-copy ring pipeline (FLIF_GL) */
+    int stages;      /* pipeline depth of variant 1 */
+    int rows;        /* ring rows per stage of variant 1 */
+} sp_launch;
+
+int  sp_dev_create(const sp_host_model *m, sp_dev **out);
+void sp_dev_destroy(sp_dev *d);
+
+/* Re-initialise neuron state from m->nc (spike flags cleared, ring refilled,
+ * internal step = 0). Synapse state is left as it is, as in the reference. */
+int  sp_dev_reset_neurons(sp_dev *d, const sp_host_model *m);
+
+/* Run T macro steps. `u` holds T x din inputs; `u_on_device` says whether it is
+ * a device pointer (else host, staged in chunks); u == NULL means zeros.
+ * Optional device outputs: phi [T x n] states after each macro step, raster
+ * [T x nwords] spike words after each macro step, y [T x dout] readouts.
+ * Host outputs (h_*) are filled chunk by chunk when the device ones are NULL. */
+typedef struct {
+    const double *u;
+    int u_on_device;
+    size_t T;
+    double *d_phi;
+    uint32_t *d_raster;
+    double *d_y;
+    double *h_phi;
+    uint32_t *h_raster;
+    double *h_y;
+    int sync;        /* wait for completion and report kernel errors */
+} sp_run_args;
+
+int  sp_dev_run(sp_dev *d, const sp_run_args *a);
+int  sp_dev_sync(sp_dev *d);
+
+int  sp_dev_read_state(sp_dev *d, double *h_V);
+int  sp_dev_read_spikes(sp_dev *d, double *h_spk);
+int  sp_dev_set_state(sp_dev *d, const double *h_V);
+int  sp_dev_compute_output(sp_dev *d, double *h_y);
+int  sp_dev_upload_w_out(sp_dev *d, const double *h_W_out);
+int  sp_dev_download_w_out(sp_dev *d, double *h_W_out);
+void *sp_dev_stream(sp_dev *d);
+int  sp_dev_get_launch(sp_dev *d, sp_launch *l);
+int  sp_dev_set_launch(sp_dev *d, const sp_launch *l);
+int  sp_dev_set_seed(sp_dev *d, uint64_t seed);
+size_t sp_dev_nwords(const sp_dev *d);
+long long sp_dev_kernel_launches(const sp_dev *d);
+
+/* Readouts on the device (dev_readout.cu). */
+typedef struct {
+    int gram_mode;      /* 0 = FP64 Gram, 1 = BF16x3 split tensor-core Gram */
+    int max_refine;     /* iterative-refinement sweeps (mode 1) */
+    double refine_tol;  /* stop when ||r|| / ||b|| falls below */
+    size_t washout;     /* rows of phi skipped before the Gram */
+} sp_ridge_opts;
+
+typedef struct {
+    int gram_mode_used;
+    int refine_iters;
+    double rel_residual;      /* ||B - (G + lambda I) W|| / ||B|| in FP64 */
+    double gram_ms, factor_ms, refine_ms, collect_ms;
+    int factor_failed;        /* Cholesky met a non-positive pivot */
+    int lu_fallback;          /* solved by pivoted LU instead */
+} sp_ridge_report;
+
+int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,
+                       const double *h_y, size_t T, double lambda,
+                       const sp_ridge_opts *o, sp_ridge_report *rep,
+                       double *h_W_out);
+int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double *h_u,
+                     const double *h_y, size_t T, double delta, double lambda,
+                     double *h_W_out);
+int sp_dev_train_online(sp_dev *d, const double *h_target, double lr,
+                        double *h_W_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

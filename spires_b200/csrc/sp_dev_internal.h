@@ -1,0 +1,61 @@
+// sp_dev_internal.h -- layout of the device state of one reservoir (CUDA side
+// only; the host C code sees sp_dev as an opaque type).
+//
+// HBM layout (n neurons, L ring rows, nw = ceil(n/32) spike words):
+//   V[n], tprev[n]                   membrane potential, refractory clock
+//   ring[L][n]   (FLIF_GL)           time-major history: lag k of every neuron
+//                                    is one contiguous n*8-byte row
+//   ring[n][D]   (FLIF_CAPUTO)       per-neuron shift register (own head)
+//   spk[2][nw]                       spike bits, double-buffered per micro-step
+//   row_ptr[n+1] (int64), col[nnz] (int32), w[nnz] (double)   recurrent CSR
+//   eff[2][n]                        per-neuron synaptic drive (non-SIMPLE)
+//   Iring[Ls][n] (FRACTIONAL)        time-major fractional-current ring
+#pragma once
+#include <cuda_runtime.h>
+#include "sp_dev.h"
+
+struct sp_dev {
+    int device, num_sms, coop;
+    cudaStream_t stream;
+    int n, din, dout, micro;
+    size_t nwords, nnz;
+    double dt, gamma;
+    int ntype, stype;
+    sp_neuron_consts nc;
+    sp_synapse_consts sc;
+    unsigned long long seed;
+    long long step;      // neuron micro-step counter (reset -> 0)
+    long long syn_step;  // fractional-synapse micro-step counter (never reset)
+    int phase;           // spk buffer holding the latest spike words
+    long long launches;
+    sp_launch launch;
+
+    double *V, *tprev, *ring;
+    int *cap_pos;
+    long long *refr_until;
+    unsigned long long *rng;
+    unsigned *spk;
+    long long *row_ptr;
+    int *col;
+    double *w, *coef;
+    double *eff, *trace, *edge_decay, *edge_omd, *edge_trace;
+    double *scoef, *Iring;
+    double *mx_decay, *mx_omd, *mx_c, *mx_tr;
+    double *W_in, *W_out;
+
+    // staging for host-driven runs
+    size_t chunk;        // macro steps per chunk
+    double *d_u;         // [chunk][din]
+    double *d_phi;       // [chunk][n]
+    double *d_y;         // [chunk][dout]
+    unsigned *d_ras;     // [chunk][nw]
+    double *d_spkd;      // [n]
+    double *h_stage;     // pinned [chunk][dout]
+    unsigned *bar;
+    int *err;
+};
+
+extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double *phi,
+                                   unsigned *raster);
+extern "C" int sp_dev_readout(sp_dev *d, const double *X, size_t T, double *Y);
+extern "C" void sp_dev_note_error(const char *what, int code);

@@ -1,0 +1,13 @@
+// sp_gram.h -- mixed-precision Gram on the tensor cores (gram_tc.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+
+// 1 when the BF16x3 tcgen05 Gram is compiled in and the device supports it.
+extern "C" int sp_gram_bf16x3_available(void);
+
+// C[n][n] (ldc) = sum_{t in [t0, t1)} X[t][:]^T X[t][:] with X (T x n, FP64,
+// row-major) split as x = hi + lo (both BF16): hi*hi + hi*lo + lo*hi with FP32
+// accumulation, written back as FP64. Returns an SP_* status.
+extern "C" int sp_gram_bf16x3(cudaStream_t s, const double *X, int n, size_t t0, size_t t1,
+                              double *C, int ldc);

@@ -1,0 +1,76 @@
+"""Host construction parity: W, W_in, W_out drawn with rand() exactly as the
+reference draws them (src/reservoir.c:308-571). Runs on the CPU only: the
+library's host-only model build is compared with the reference compiled from
+source (oracle/_ref)."""
+import numpy as np
+import pytest
+
+import spires_b200 as sp
+from tests import _oracle
+
+pytestmark = pytest.mark.skipif(not _oracle.have_ref(), reason="reference build absent")
+
+GL = (1.0, 0.0, 0.0, 20.0, 0.7, 64.0, 0.1, 2.0)
+
+CASES = [
+    # n, topo, conn, din, dout, neuron, params, synapse, backend, sparams
+    (60, sp.CONN_RANDOM, 0.1, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 0, None),
+    (200, sp.CONN_RANDOM, 0.05, 3, 2, sp.FLIF_GL, GL, sp.SYN_SIMPLE, 0, None),
+    (200, sp.CONN_SMALL_WORLD, 10 / 199, 1, 1, sp.FLIF_GL, GL, sp.SYN_SIMPLE, 0, None),
+    (300, sp.CONN_SMALL_WORLD, 0.2, 2, 1, sp.FLIF_GL, GL, sp.SYN_SIMPLE, 1, None),
+    (3, sp.CONN_SMALL_WORLD, 0.9, 1, 1, sp.LIF_BIO, (0, 1, 20, 0.1), sp.SYN_SIMPLE, 0, None),
+    (250, sp.CONN_SCALE_FREE, 5 / 249, 13, 10, sp.FLIF_GL, GL, sp.SYN_SIMPLE, 0, None),
+    (150, sp.CONN_SCALE_FREE, 0.1, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 1, None),
+    (2, sp.CONN_SCALE_FREE, 0.5, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 0, None),
+    (120, sp.CONN_RANDOM, 0.1, 1, 1, sp.FLIF_GL, GL, sp.SYN_PSC_HET, 0, (1.0, 20.0)),
+    (80, sp.CONN_SMALL_WORLD, 0.1, 1, 1, sp.FLIF_GL, GL, sp.SYN_PSC_HET, 1, (2.0, 8.0)),
+    (100, sp.CONN_SCALE_FREE, 0.03, 1, 1, sp.FLIF_GL, GL, sp.SYN_FRAC_MEXP, 0,
+     (0.5, 5.0, 1.0, 50.0, 6)),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"n{c[0]}-topo{c[1]}-syn{c[7]}-be{c[8]}")
+@pytest.mark.parametrize("seed", [1, 42])
+def test_weights_match_reference(case, seed):
+    n, topo, conn, din, dout, neuron, params, syn, be, sparams = case
+    cfg = sp.make_config(n, din, dout, rho=0.93, ei=0.6, gamma=0.5, conn=conn, dt=1.0,
+                         topo=topo, neuron=neuron, nparams=params, synapse=syn, backend=be,
+                         sparams=sparams)
+    mine = sp.HostModel(cfg, seed=seed)
+    ref = sp.Reservoir(cfg, lib=_oracle.ref_lib(), seed=seed)
+    Wr = ref.weights()
+    Wm = mine.dense()
+    assert np.array_equal(Wr.view(np.uint64), Wm.view(np.uint64)) or np.array_equal(Wr, Wm)
+    assert np.array_equal(ref.readout(), mine.w_out())
+    # W_in comes first in the draw order: replay it with the C library's rand()
+    sp.libc.srand(seed)
+    RAND_MAX = 2147483647.0
+    win = np.empty(n * din)
+    for k in range(n * din):
+        mag = sp.libc.rand() / RAND_MAX
+        win[k] = mag if sp.libc.rand() / RAND_MAX < 0.6 else -mag
+    assert np.array_equal(win.reshape(n, din), mine.w_in())
+    ref.close()
+
+
+def test_rand_stream_position_after_create():
+    """The next rand() after construction is the same in both libraries, so
+    callers that build several reservoirs from one seed get the same sequence."""
+    cfg = sp.make_config(300, 2, 2, conn=5 / 299, topo=sp.CONN_SCALE_FREE, neuron=sp.FLIF_GL,
+                         nparams=GL)
+    sp.HostModel(cfg, seed=7)
+    a = [sp.libc.rand() for _ in range(4)]
+    r = sp.Reservoir(cfg, lib=_oracle.ref_lib(), seed=7)
+    b = [sp.libc.rand() for _ in range(4)]
+    r.close()
+    assert a == b
+
+
+def test_invalid_configs_rejected():
+    lib = sp.load()
+    import ctypes as C
+    h = C.c_void_p()
+    for kw in [dict(dt=0.0), dict(dt=0.3), dict(dt=1.5), dict(neuron=9), dict(topo=5)]:
+        cfg = sp.make_config(10, **kw)
+        assert lib.spires_ext_model_build(C.byref(cfg), C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
+    assert lib.spires_reservoir_create(None, C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
