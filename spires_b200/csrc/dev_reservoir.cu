@@ -28,381 +28,47 @@
 #include "sp_dev.h"
 #include "sp_kernels.cuh"
 #include "sp_dev_internal.h"
+#include "sp_step_kernel.cuh"
+
+typedef void (*kfn_t)(sp::KP);
 
 using namespace sp;
 
 namespace {
 
-// Kernel parameters (passed by value; < 4 KB).
-struct KP {
-    int n, nwords, din, micro, G, n_macro, phase0;
-    long long step0, syn_step0;
-    // neuron constants
-    double a, b, c, d, e, f, g, h, ci, cj, ck, cl, dt;
-    int L, det_refr, diff_sto;
-    const double *coef;
-    // neuron state
-    double *V, *tprev, *ring;
-    int *cap_pos;
-    long long *refr_until;
-    unsigned long long *rng;
-    unsigned *spk;  // [2][nwords]
-    // synapse
-    const long long *row_ptr;
-    const int *col;
-    const double *w;
-    double *eff;    // [2][n]
-    double psc_decay, psc_omd;
-    double *trace;
-    const double *edge_decay, *edge_omd;
-    double *edge_trace;
-    int Ls;
-    const double *scoef;
-    double s_dta, s_tau;
-    double *Iring;
-    int Nc;
-    const double *mx_decay, *mx_omd, *mx_c;
-    double *mx_tr;
-    // input / output
-    const double *W_in;
-    double gamma;
-    const double *u;       // [n_macro][din] or null (zeros)
-    double *phi;           // [n_macro][n] or null
-    unsigned *raster;      // [n_macro][nwords] or null
-    unsigned *bar;
-    int *err;
-};
-
-template <int NT, int ST>
-__global__ void __launch_bounds__(1024, 1) k_run(KP p)
-{
-    extern __shared__ unsigned s_spk[];
-    __shared__ int s_flag;
-
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int wb0 = (int)(((long long)blockIdx.x * p.nwords) / p.G);
-    const int wb1 = (int)(((long long)(blockIdx.x + 1) * p.nwords) / p.G);
-    const int gw = wb0 + warp;
-    const bool wact = gw < wb1;
-    const int i = gw * 32 + lane;
-    const bool act = wact && i < p.n;
-    const int n = p.n;
-
-    // ---- per-neuron state into registers
-    double V = act ? p.V[i] : 0.0;
-    double tprev = 0.0, vlast = 0.0;
-    int cpos = 0;
-    long long refr = 0;
-    unsigned long long rng = 0;
-    if (act) {
-        if (NT == SP_FLIF_GL || NT == SP_FLIF_CAPUTO)
-            tprev = p.tprev[i];
-        if (NT == SP_FLIF_GL) {
-            long long pr = (p.step0 - 1) % p.L;
-            if (pr < 0)
-                pr += p.L;
-            vlast = p.ring[(size_t)pr * n + i];
-        }
-        if (NT == SP_FLIF_CAPUTO)
-            cpos = p.cap_pos[i];
-        if (NT == SP_FLIF_DIFFUSIVE) {
-            refr = p.refr_until[i];
-            rng = p.rng[i];
-        }
-    }
-    double ptrace = (ST == SP_SYN_PSC_HOM && act) ? p.trace[i] : 0.0;
-    double Ilast = 0.0;
-    if (ST == SP_SYN_FRAC && act) {
-        long long pr = (p.syn_step0 - 1) % p.Ls;
-        if (pr < 0)
-            pr += p.Ls;
-        Ilast = p.Iring[(size_t)pr * n + i];
-    }
-    int phase = p.phase0;
-    double sprev = 0.0;
-    if (act)
-        sprev = ((p.spk[phase * p.nwords + gw] >> lane) & 1u) ? 1.0 : 0.0;
-    unsigned lastword = 0;
-    unsigned nbar = 0;
-
-    for (int s = 0; s < p.n_macro; ++s) {
-        // ext = 0 + gamma * (sum_j W_in[i][j] u[j]): netlib dgemv order,
-        // src/reservoir.c:132-136
-        double ext = 0.0;
-        if (act && p.din > 0 && p.gamma != 0.0 && p.u) {
-            const double *ur = p.u + (size_t)s * p.din;
-            const double *wr = p.W_in + (size_t)i * p.din;
-            double t = 0.0;
-            for (int j = 0; j < p.din; ++j)
-                t = add(t, mul(__ldg(wr + j), __ldg(ur + j)));
-            ext = add(0.0, mul(p.gamma, t));
-        }
-        for (int m = 0; m < p.micro; ++m) {
-            const long long g = p.step0 + (long long)s * p.micro + m;
-            const long long gs = p.syn_step0 + (long long)s * p.micro + m;
-            const int cur = phase;
-
-            // ---- 1. synapse prepare for the own neuron
-            if (act) {
-                if (ST == SP_SYN_PSC_HOM) {
-                    ptrace = add(mul(ptrace, p.psc_decay), mul(p.psc_omd, sprev));
-                    p.eff[(size_t)cur * n + i] = ptrace;
-                } else if (ST == SP_SYN_FRAC) {
-                    const int Ls = p.Ls;
-                    const int head = (int)(gs % Ls);
-                    const long long lim = gs < Ls ? gs : Ls - 1;
-                    double hist = 0.0;
-                    if (lim >= 1)
-                        hist = add(hist, mul(__ldg(p.scoef + 1), Ilast));
-                    for (int k = 2; k <= lim; ++k) {
-                        int r = head - k;
-                        if (r < 0)
-                            r += Ls;
-                        hist = add(hist, mul(__ldg(p.scoef + k), __ldcg(p.Iring + (size_t)r * n + i)));
-                    }
-                    double rhs = dvd(add(-Ilast, sprev), p.s_tau);
-                    double In = sub(mul(p.s_dta, rhs), hist);
-                    p.Iring[(size_t)head * n + i] = In;
-                    Ilast = In;
-                    p.eff[(size_t)cur * n + i] = In;
-                } else if (ST == SP_SYN_FRAC_MEXP) {
-                    double sum = 0.0;
-                    for (int c = 0; c < p.Nc; ++c) {
-                        double tr = p.mx_tr[(size_t)c * n + i];
-                        tr = add(mul(tr, __ldg(p.mx_decay + c)), mul(__ldg(p.mx_omd + c), sprev));
-                        p.mx_tr[(size_t)c * n + i] = tr;
-                        sum = add(sum, mul(__ldg(p.mx_c + c), tr));
-                    }
-                    p.eff[(size_t)cur * n + i] = sum;
-                }
-            }
-
-            // ---- 2. FLIF_GL history sum (own ring column, ascending lag)
-            bool integ = false;
-            double hist = 0.0;
-            int head = 0;
-            if (NT == SP_FLIF_GL) {
-                const int L = p.L;
-                head = (int)(g % L);
-                integ = tprev > p.f;
-                if (act && integ) {
-                    const long long lim = g < L ? g : L - 1;
-                    if (lim >= 1)
-                        hist = add(hist, mul(__ldg(p.coef + 1), vlast));
-                    int r = head - 2;
-                    if (r < 0)
-                        r += L;
-                    const double *col_i = p.ring + i;
-#pragma unroll 8
-                    for (int k = 2; k <= (int)lim; ++k) {
-                        hist = add(hist, mul(__ldg(p.coef + k), __ldcg(col_i + (size_t)r * n)));
-                        r = (r == 0) ? L - 1 : r - 1;
-                    }
-                }
-            }
-
-            // ---- 3. grid barrier
-            if (p.G > 1) {
-                ++nbar;
-                if (!grid_barrier(p.bar, nbar * (unsigned)p.G, p.err, g, &s_flag))
-                    return;
-            } else {
-                __syncthreads();
-            }
-            if (ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET) {
-                for (int wi = threadIdx.x; wi < p.nwords; wi += blockDim.x)
-                    s_spk[wi] = __ldcg(p.spk + (size_t)cur * p.nwords + wi);
-                __syncthreads();
-            }
-
-            // ---- 4. recurrent input
-            double rec = 0.0;
-            if (act) {
-                const long long k0 = __ldg(p.row_ptr + i), k1 = __ldg(p.row_ptr + i + 1);
-                if (ST == SP_SYN_SIMPLE) {
-                    for (long long k = k0; k < k1; ++k) {
-                        const int c = __ldg(p.col + k);
-                        if ((s_spk[c >> 5] >> (c & 31)) & 1u)
-                            rec = add(rec, __ldg(p.w + k));
-                    }
-                } else if (ST == SP_SYN_PSC_HET) {
-                    for (long long k = k0; k < k1; ++k) {
-                        const int c = __ldg(p.col + k);
-                        const double sv = ((s_spk[c >> 5] >> (c & 31)) & 1u) ? 1.0 : 0.0;
-                        double tr = add(mul(p.edge_trace[k], __ldg(p.edge_decay + k)),
-                                        mul(__ldg(p.edge_omd + k), sv));
-                        p.edge_trace[k] = tr;
-                        rec = add(rec, mul(__ldg(p.w + k), tr));
-                    }
-                } else {
-                    const double *ef = p.eff + (size_t)cur * n;
-                    for (long long k = k0; k < k1; ++k) {
-                        const int c = __ldg(p.col + k);
-                        rec = add(rec, mul(__ldg(p.w + k), __ldcg(ef + c)));
-                    }
-                }
-            }
-
-            // ---- 5. neuron update
-            bool fired = false;
-            if (act) {
-                const double in = add(ext, rec);
-                if (NT == SP_LIF_DISCRETE) {
-                    // V = (1 - leak) V + I + bias; spike if V > V_th
-                    V = add(add(mul(p.c, V), in), p.d);
-                    if (V > p.b) {
-                        V = p.a;
-                        fired = true;
-                    }
-                } else if (NT == SP_LIF_BIO) {
-                    // dV = (-V + I + bias) / tau; V += dV dt; spike if V >= V_th
-                    double dV = dvd(add(add(-V, in), p.d), p.c);
-                    V = add(V, mul(dV, p.dt));
-                    if (V >= p.b) {
-                        V = p.a;
-                        fired = true;
-                    }
-                } else if (NT == SP_FLIF_GL) {
-                    if (integ) {
-                        // rhs = -(V_prev - V_rest)/tau_m + I + bias; V = dt^a rhs - hist
-                        double rhs = add(add(dvd(-sub(vlast, p.c), p.d), in), p.e);
-                        V = sub(mul(p.g, rhs), hist);
-                        if (V >= p.a) {
-                            V = p.b;
-                            fired = true;
-                            tprev = 0.0;
-                        }
-                    } else {
-                        V = p.b;
-                    }
-                    p.ring[(size_t)head * n + i] = V;
-                    vlast = V;
-                    tprev = add(tprev, p.dt);
-                } else if (NT == SP_FLIF_CAPUTO) {
-                    if (tprev > p.f) {
-                        // dV = (-g_l (V - V_l) + I) / C_m; markov = kr dV
-                        double dV = dvd(add(mul(-p.c, sub(V, p.d)), in), p.e);
-                        double markov = mul(p.g, dV);
-                        const int D = p.L;
-                        double *rg = p.ring + (size_t)i * D;
-                        rg[cpos] = sub(V, p.b);
-                        int q = cpos;
-                        cpos = (cpos + 1 == D) ? 0 : cpos + 1;
-                        double mem = 0.0;
-                        for (int k = 0; k < D; ++k) {
-                            mem = add(mem, mul(__ldg(p.coef + k), rg[q]));
-                            q = (q == 0) ? D - 1 : q - 1;
-                        }
-                        V = add(V, sub(markov, mem));
-                        if (V >= p.a) {
-                            V = p.b;
-                            fired = true;
-                            tprev = 0.0;
-                        }
-                    } else {
-                        V = p.b;
-                    }
-                    tprev = add(tprev, p.dt);
-                } else if (NT == SP_FLIF_DIFFUSIVE) {
-                    double Vp = V;
-                    double rhs = add(add(-sub(Vp, p.c), in), p.d);
-                    V = add(Vp, mul(p.e, rhs));
-                    if (g >= refr && V >= p.a) {
-                        V = p.b;
-                        fired = true;
-                        long long steps;
-                        if (p.diff_sto) {
-                            // alpha-controlled refractory window, flif_diffusive.c:25-63
-                            double W;
-                            double u0 = u01(&rng);
-                            if (u0 < p.ci) {
-                                W = p.h;
-                            } else {
-                                double u1 = u01(&rng);
-                                const double tmin = p.f, tmax = p.g, q = p.cj;
-                                if (tmax <= tmin)
-                                    W = tmin;
-                                else if (q <= 1e-12)
-                                    W = tmin + u1 * (tmax - tmin);
-                                else if (fabs(q - 1.0) < 1e-12)
-                                    W = tmin * pow(tmax / tmin, u1);
-                                else
-                                    W = pow((1.0 - u1) * p.ck + u1 * p.cl, 1.0 / (1.0 - q));
-                            }
-                            steps = (W <= 0.0) ? 0 : (long long)ceil(W / p.dt);
-                            if (steps < 1)
-                                steps = 1;
-                        } else {
-                            steps = p.det_refr;
-                        }
-                        refr = g + steps;
-                    }
-                }
-            }
-
-            // ---- 6. spike word of this micro-step
-            const unsigned word = __ballot_sync(kFull, fired);
-            if (wact && lane == 0)
-                p.spk[(size_t)(cur ^ 1) * p.nwords + gw] = word;
-            lastword = word;
-            sprev = fired ? 1.0 : 0.0;
-            phase = cur ^ 1;
-        }
-        if (act && p.phi)
-            p.phi[(size_t)s * n + i] = V;
-        if (wact && lane == 0 && p.raster)
-            p.raster[(size_t)s * p.nwords + gw] = lastword;
-    }
-
-    // ---- write back
-    if (act) {
-        p.V[i] = V;
-        if (NT == SP_FLIF_GL || NT == SP_FLIF_CAPUTO)
-            p.tprev[i] = tprev;
-        if (NT == SP_FLIF_CAPUTO)
-            p.cap_pos[i] = cpos;
-        if (NT == SP_FLIF_DIFFUSIVE) {
-            p.refr_until[i] = refr;
-            p.rng[i] = rng;
-        }
-        if (ST == SP_SYN_PSC_HOM)
-            p.trace[i] = ptrace;
-    }
-}
-
-typedef void (*kfn)(KP);
-
-template <int NT>
-kfn pick_syn(int st)
+template <int NT, int VAR>
+kfn_t pick_syn(int st)
 {
     switch (st) {
-    case SP_SYN_SIMPLE: return k_run<NT, SP_SYN_SIMPLE>;
-    case SP_SYN_PSC_HOM: return k_run<NT, SP_SYN_PSC_HOM>;
-    case SP_SYN_PSC_HET: return k_run<NT, SP_SYN_PSC_HET>;
-    case SP_SYN_FRAC: return k_run<NT, SP_SYN_FRAC>;
-    case SP_SYN_FRAC_MEXP: return k_run<NT, SP_SYN_FRAC_MEXP>;
+    case SP_SYN_SIMPLE: return k_run<NT, SP_SYN_SIMPLE, VAR>;
+    case SP_SYN_PSC_HOM: return k_run<NT, SP_SYN_PSC_HOM, VAR>;
+    case SP_SYN_PSC_HET: return k_run<NT, SP_SYN_PSC_HET, VAR>;
+    case SP_SYN_FRAC: return k_run<NT, SP_SYN_FRAC, VAR>;
+    case SP_SYN_FRAC_MEXP: return k_run<NT, SP_SYN_FRAC_MEXP, VAR>;
     }
     return nullptr;
 }
 
-kfn pick_kernel(int nt, int st)
+kfn_t pick_kernel(int nt, int st, int variant)
 {
+    if (variant == 1)
+        return nt == SP_FLIF_GL ? pick_syn<SP_FLIF_GL, 1>(st) : nullptr;
     switch (nt) {
-    case SP_LIF_DISCRETE: return pick_syn<SP_LIF_DISCRETE>(st);
-    case SP_LIF_BIO: return pick_syn<SP_LIF_BIO>(st);
-    case SP_FLIF_CAPUTO: return pick_syn<SP_FLIF_CAPUTO>(st);
-    case SP_FLIF_GL: return pick_syn<SP_FLIF_GL>(st);
-    case SP_FLIF_DIFFUSIVE: return pick_syn<SP_FLIF_DIFFUSIVE>(st);
+    case SP_LIF_DISCRETE: return pick_syn<SP_LIF_DISCRETE, 0>(st);
+    case SP_LIF_BIO: return pick_syn<SP_LIF_BIO, 0>(st);
+    case SP_FLIF_CAPUTO: return pick_syn<SP_FLIF_CAPUTO, 0>(st);
+    case SP_FLIF_GL: return pick_syn<SP_FLIF_GL, 0>(st);
+    case SP_FLIF_DIFFUSIVE: return pick_syn<SP_FLIF_DIFFUSIVE, 0>(st);
     }
     return nullptr;
 }
 
 // ---------------------------------------------------------------- resets --
 
-__global__ void k_reset_neurons(int n, int L, int ntype, double v_init, double tprev_init,
-                                double *V, double *tprev, double *ring, int *cap_pos,
-                                long long *refr, unsigned long long *rng, unsigned long long seed)
+__global__ void k_reset_neurons(int n, int L, size_t ring_elems, int ntype, double v_init,
+                                double tprev_init, double *V, double *tprev, double *ring,
+                                int *cap_pos, long long *refr, unsigned long long *rng,
+                                unsigned long long seed)
 {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
@@ -421,8 +87,8 @@ __global__ void k_reset_neurons(int n, int L, int ntype, double v_init, double t
     if (ring) {
         // FLIF_GL ring holds V_rest; the Caputo shift register starts at zero
         const double fill = (ntype == SP_FLIF_GL) ? v_init : 0.0;
-        const size_t total = (size_t)n * (size_t)L;
-        for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += stride)
+        for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < ring_elems;
+             k += stride)
             ring[k] = fill;
     }
 }
@@ -516,6 +182,24 @@ static int upload_consts(sp_dev *d, const sp_host_model *m)
     return SP_OK;
 }
 
+// dynamic shared memory of a launch shape: spike words, then (variant 1) the
+// ring-row stages and their full/empty mbarriers
+static size_t launch_smem(const sp_dev *d, const sp_launch &l)
+{
+    size_t spk = ((d->nwords * 4) + 127) & ~(size_t)127;
+    if (l.variant == 1)
+        return spk + (size_t)l.stages * l.rows * 32 * l.warps_max * sizeof(double) +
+               2 * (size_t)l.stages * sizeof(unsigned long long);
+    return spk;
+}
+
+static int max_smem(const sp_dev *d)
+{
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device);
+    return v > 0 ? v : 48 * 1024;
+}
+
 static void default_launch(sp_dev *d)
 {
     int nw = (int)d->nwords;
@@ -528,8 +212,22 @@ static void default_launch(sp_dev *d)
         int G = d->num_sms < nw ? d->num_sms : nw;
         l.ctas = G;
         l.warps_max = (nw + G - 1) / G;
-        if (l.warps_max > 32) { /* n beyond 32 * 32 * SMs: not supported by one grid */
+        if (l.warps_max > 32)
             l.warps_max = 32;
+    }
+    if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 31) {
+        sp_launch v = l;
+        v.variant = 1;
+        v.rows = 16;
+        const size_t stage = (size_t)v.rows * 32 * v.warps_max * sizeof(double);
+        const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
+        const size_t spk = ((d->nwords * 4) + 127) & ~(size_t)127;
+        long long st = budget > spk ? (long long)((budget - spk) / (stage + 16)) : 0;
+        if (st > 16)
+            st = 16;
+        if (st >= 2) {
+            v.stages = (int)st;
+            l = v;
         }
     }
     d->launch = l;
@@ -589,9 +287,13 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         TRY(dupload(&d->w, m->w, m->nnz, s));
         TRY(dupload(&d->W_in, m->W_in, n * m->din, s));
         TRY(dupload(&d->W_out, m->W_out, n * m->dout, s));
+        d->rs = (int)((n + 31) / 32 * 32);
         if (m->neuron_type == SP_FLIF_GL || m->neuron_type == SP_FLIF_CAPUTO) {
             TRY(dupload(&d->coef, m->coef, (size_t)m->nc.L, s));
-            TRY(dalloc(&d->ring, n * (size_t)m->nc.L));
+            // FLIF_GL: [L][rs] time-major rows; Caputo: [n][D] per-neuron registers
+            d->ring_elems = (m->neuron_type == SP_FLIF_GL) ? (size_t)d->rs * m->nc.L
+                                                            : n * (size_t)m->nc.L;
+            TRY(dalloc(&d->ring, d->ring_elems));
         }
         if (m->neuron_type == SP_FLIF_CAPUTO)
             TRY(dalloc(&d->cap_pos, n));
@@ -685,8 +387,8 @@ extern "C" int sp_dev_reset_neurons(sp_dev *d, const sp_host_model *m)
     SP_CK(cudaMemsetAsync(d->spk, 0, 2 * d->nwords * sizeof(unsigned), d->stream));
     int blocks = d->num_sms * 4;
     k_reset_neurons<<<blocks, 256, 0, d->stream>>>(
-        d->n, d->nc.L, d->ntype, d->nc.v_init, d->nc.tprev_init, d->V, d->tprev, d->ring,
-        d->cap_pos, d->refr_until, d->rng, d->seed);
+        d->n, d->nc.L, d->ring_elems, d->ntype, d->nc.v_init, d->nc.tprev_init, d->V, d->tprev,
+        d->ring, d->cap_pos, d->refr_until, d->rng, d->seed);
     SP_CK(cudaGetLastError());
     return SP_OK;
 }
@@ -723,7 +425,7 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
 {
     if (T == 0)
         return SP_OK;
-    KP p;
+    sp::KP p;
     memset(&p, 0, sizeof(p));
     const sp_launch &l = d->launch;
     p.n = d->n;
@@ -733,6 +435,10 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.G = l.ctas;
     p.n_macro = (int)T;
     p.phase0 = d->phase;
+    p.rs = d->rs;
+    p.warps = l.warps_max;
+    p.R = l.variant == 1 ? l.rows : 0;
+    p.NST = l.variant == 1 ? l.stages : 0;
     p.step0 = d->step;
     p.syn_step0 = d->syn_step;
     p.a = d->nc.a; p.b = d->nc.b; p.c = d->nc.c; p.d = d->nc.d; p.e = d->nc.e; p.f = d->nc.f;
@@ -755,11 +461,11 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.phi = phi; p.raster = raster;
     p.bar = d->bar; p.err = d->err;
 
-    kfn fn = pick_kernel(d->ntype, d->stype);
+    kfn_t fn = pick_kernel(d->ntype, d->stype, l.variant);
     if (!fn)
         return SP_EINVAL;
-    const size_t smem = d->nwords * sizeof(unsigned);
-    dim3 grid(l.ctas), block(32 * l.warps_max);
+    const size_t smem = launch_smem(d, l);
+    dim3 grid(l.ctas), block(32 * (l.warps_max + (l.variant == 1 ? 1 : 0)));
     if (smem > 48 * 1024)
         SP_CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
@@ -908,13 +614,27 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
         return SP_EINVAL;
     if ((long long)l->ctas * l->warps_max < (long long)d->nwords)
         return SP_EINVAL;
+    if (l->variant == 1) {
+        if (d->ntype != SP_FLIF_GL || l->warps_max > 31 || l->rows < 1 || l->stages < 2 ||
+            l->rows > 64)
+            return SP_EINVAL;
+    } else if (l->variant != 0) {
+        return SP_EINVAL;
+    }
+    const size_t smem = launch_smem(d, *l);
+    if (smem > (size_t)max_smem(d))
+        return SP_EINVAL;
+    kfn_t fn = pick_kernel(d->ntype, d->stype, l->variant);
+    if (!fn)
+        return SP_EINVAL;
     if (l->ctas > 1) {
-        kfn fn = pick_kernel(d->ntype, d->stype);
+        if (smem > 48 * 1024)
+            SP_CK(cudaFuncSetAttribute((const void *)fn,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn,
-                                                          32 * l->warps_max,
-                                                          d->nwords * sizeof(unsigned)) !=
-            cudaSuccess)
+        const int threads = 32 * (l->warps_max + (l->variant == 1 ? 1 : 0));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, threads,
+                                                          smem) != cudaSuccess)
             return SP_EINTERNAL;
         if (!d->coop || per_sm * d->num_sms < l->ctas)
             return SP_EINVAL;

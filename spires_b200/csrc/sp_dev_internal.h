@@ -18,6 +18,8 @@ struct sp_dev {
     int device, num_sms, coop;
     cudaStream_t stream;
     int n, din, dout, micro;
+    int rs;              // FLIF_GL ring row stride (n rounded up to 32)
+    size_t ring_elems;
     size_t nwords, nnz;
     double dt, gamma;
     int ntype, stype;

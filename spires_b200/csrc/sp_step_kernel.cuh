@@ -1,0 +1,671 @@
+// sp_step_kernel.cuh -- the persistent reservoir step kernel (all neuron and
+// synapse models), included by dev_reservoir.cu.
+//
+// Launch: a cooperative grid of G CTAs; CTA b owns the whole warps
+// [b*nw/G, (b+1)*nw/G) of neurons (nw = ceil(n/32)); a consumer thread owns
+// one neuron and keeps its state in registers for the whole launch.
+//
+// Variant 0: the FLIF_GL history is summed with direct loads from the
+//   time-major ring (each lag is one coalesced row segment).
+// Variant 1 (FLIF_GL only): one extra producer warp streams the ring rows of
+//   the CTA's neuron range into a multi-stage shared-memory pipeline with
+//   cp.async.bulk (bulk-copy TMA) on mbarriers; the consumers read lags from
+//   shared memory. The producer runs up to one step ahead of the consumers:
+//   the rows of step g are the states of steps <= g-2 (lag 1 is the register
+//   copy of the previous state), so they only wait for step g-2 to finish.
+//
+// Per micro-step (both variants), with a split-phase grid barrier:
+//   history sum of step g      (overlaps the barrier wait)
+//   wait barrier g             (spike words / eff of step g-1 visible)
+//   recurrent input            SIMPLE: warp-cooperative walk over the warp's
+//                              CSR edges, ballot of spiking presynaptic bits,
+//                              owner lane adds the weights in ascending edge
+//                              order; others: per-row walk over eff[]
+//   neuron update, ring write, ballot -> spike word of step g
+//   synapse prepare for g+1 (own spike), publish, arrive barrier g+1
+#pragma once
+#include "sp_kernels.cuh"
+#include "sp_model.h"
+
+namespace sp {
+
+struct KP {
+    int n, nwords, din, micro, G, n_macro, phase0;
+    int rs;         // ring row stride in doubles (multiple of 32)
+    int warps;      // consumer warps per CTA
+    int R, NST;     // variant 1: ring rows per stage, stages
+    long long step0, syn_step0;
+    double a, b, c, d, e, f, g, h, ci, cj, ck, cl, dt;
+    int L, det_refr, diff_sto;
+    const double *coef;
+    double *V, *tprev, *ring;
+    int *cap_pos;
+    long long *refr_until;
+    unsigned long long *rng;
+    unsigned *spk;
+    const long long *row_ptr;
+    const int *col;
+    const double *w;
+    double *eff;
+    double psc_decay, psc_omd;
+    double *trace;
+    const double *edge_decay, *edge_omd;
+    double *edge_trace;
+    int Ls;
+    const double *scoef;
+    double s_dta, s_tau;
+    double *Iring;
+    int Nc;
+    const double *mx_decay, *mx_omd, *mx_c;
+    double *mx_tr;
+    const double *W_in;
+    double gamma;
+    const double *u;
+    double *phi;
+    unsigned *raster;
+    unsigned *bar;
+    int *err;
+};
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void named_sync(int n)
+{
+    asm volatile("bar.sync 1, %0;" ::"r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long *b, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, P;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+                 "r"(bytes)
+                 : "memory");
+}
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size % 16 == 0),
+// completion counted on the mbarrier. No multicast.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void st_release_cta(volatile int *ptr, int v)
+{
+    asm volatile("st.release.cta.shared::cta.s32 [%0], %1;" ::"r"(smem_u32((const void *)ptr)),
+                 "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ int ld_acquire_cta(volatile int *ptr)
+{
+    int v;
+    asm volatile("ld.acquire.cta.shared::cta.s32 %0, [%1];"
+                 : "=r"(v)
+                 : "r"(smem_u32((const void *)ptr))
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+// Bounded mbarrier wait; false on timeout or when the launch is aborting.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity,
+                                          volatile int *s_abort, int *err)
+{
+    if (mbar_test(b, parity))
+        return true;
+    unsigned long long t0 = globaltimer_ns();
+    unsigned polls = 0;
+    while (!mbar_test(b, parity)) {
+        if ((++polls & 63u) == 0) {
+            if (*s_abort || ld_volatile_i32(err) != kErrNone)
+                return false;
+            if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                atomicCAS(err, kErrNone, kErrBarrierTimeout);
+                *s_abort = 1;
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
+// SIMPLE synapse, one warp: recurrent input of rows [row0, row0 + nv) for the
+// lane that owns row row0 + lane. Edges are scanned 32 at a time; spiking
+// presynaptic columns are found by a ballot over the spike bits and each
+// weight is added by the owner lane of its row in ascending edge order, i.e.
+// exactly the non-zero terms of csr_row_dot (src/sparse.c:68-76) in order.
+__device__ __forceinline__ double rowpass_simple_warp(const long long *__restrict__ row_ptr,
+                                                      const int *__restrict__ col,
+                                                      const double *__restrict__ w,
+                                                      const unsigned *s_spk, int row0, int nv,
+                                                      int lane)
+{
+    const long long e0 = __ldg(row_ptr + row0);
+    const long long e1 = __ldg(row_ptr + row0 + nv);
+    const long long my_end = (lane < nv) ? __ldg(row_ptr + row0 + lane + 1) : e1;
+    double acc = 0.0;
+    for (long long base = e0; base < e1; base += 32) {
+        const long long e = base + lane;
+        bool s = false;
+        double wv = 0.0;
+        if (e < e1) {
+            const int c = __ldg(col + e);
+            s = (s_spk[c >> 5] >> (c & 31)) & 1u;
+            if (s)
+                wv = __ldg(w + e);
+        }
+        unsigned m = __ballot_sync(kFull, s);
+        while (m) {
+            const int bpos = __ffs(m) - 1;
+            m &= m - 1;
+            const long long eb = base + bpos;
+            const double wb = __shfl_sync(kFull, wv, bpos);
+            const unsigned owner = __ballot_sync(kFull, my_end > eb);
+            if (lane == __ffs(owner) - 1)
+                acc = add(acc, wb);
+        }
+    }
+    return acc;
+}
+
+template <int NT, int ST, int VAR>
+__global__ void __launch_bounds__(1024, 1) k_run(KP p)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_flag;
+    __shared__ volatile int s_abort;
+    __shared__ volatile int s_done;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int NC = 32 * p.warps;  // consumer threads
+    const int wb0 = (int)(((long long)blockIdx.x * p.nwords) / p.G);
+    const int wb1 = (int)(((long long)(blockIdx.x + 1) * p.nwords) / p.G);
+    const int n = p.n;
+    const int L = p.L;
+    const long long B = (long long)p.n_macro * p.micro;
+
+    unsigned *s_spk = (unsigned *)smem;
+    const size_t spk_bytes = (((size_t)p.nwords * 4) + 127) & ~(size_t)127;
+    double *s_stage = (double *)(smem + spk_bytes);
+    const int SW = NC;  // stage row pitch (doubles)
+    unsigned long long *full =
+        (unsigned long long *)(smem + spk_bytes + (size_t)p.NST * p.R * SW * sizeof(double));
+    unsigned long long *empty = full + p.NST;
+    const int lo = wb0 * 32;
+    const int S_b = 32 * (wb1 - wb0);
+
+    if (tid == 0) {
+        s_abort = 0;
+        s_done = 0;
+    }
+    if (VAR == 1) {
+        if (tid == 0) {
+            for (int s = 0; s < p.NST; ++s) {
+                mbar_init(&full[s], 1);
+                mbar_init(&empty[s], p.warps);
+            }
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
+    __syncthreads();
+
+    // ------------------------------------------------------------ producer
+    if (VAR == 1 && tid >= NC) {
+        if (lane != 0 || S_b == 0)
+            return;
+        long long q = 0;  // stages issued
+        bool ok = true;
+        for (long long b = 0; b < B && ok; ++b) {
+            const long long g = p.step0 + b;
+            const int lim = (int)(g < L ? g : L - 1);
+            if (lim < 2)
+                continue;
+            if (b >= 2) {
+                // rows of step g are states of steps <= g-2
+                unsigned long long t0 = globaltimer_ns();
+                unsigned polls = 0;
+                while (ld_acquire_cta(&s_done) < b - 1) {
+                    if ((++polls & 63u) == 0) {
+                        if (s_abort || ld_volatile_i32(p.err) != kErrNone) {
+                            ok = false;
+                            break;
+                        }
+                        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                            atomicCAS(p.err, kErrNone, kErrBarrierTimeout);
+                            s_abort = 1;
+                            ok = false;
+                            break;
+                        }
+                    }
+                    __nanosleep(64);
+                }
+                if (!ok)
+                    break;
+            }
+            for (int k = 2; k <= lim && ok; k += p.R) {
+                const int cnt = (lim - k + 1 < p.R) ? lim - k + 1 : p.R;
+                const int st = (int)(q % p.NST);
+                const long long u = q / p.NST;
+                if (u > 0 && !mbar_wait(&empty[st], (unsigned)((u - 1) & 1), &s_abort, p.err)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[st], (unsigned)(cnt * S_b * 8));
+                double *dst = s_stage + (size_t)st * p.R * SW;
+                for (int j = 0; j < cnt; ++j) {
+                    long long r = (g - k - j) % L;
+                    if (r < 0)
+                        r += L;
+                    bulk_g2s(dst + (size_t)j * SW, p.ring + (size_t)r * p.rs + lo,
+                             (unsigned)(S_b * 8), &full[st]);
+                }
+                ++q;
+            }
+        }
+        // every issued copy must land before the CTA may exit
+        for (long long qq = (q > p.NST ? q - p.NST : 0); qq < q; ++qq) {
+            const int st = (int)(qq % p.NST);
+            unsigned long long t0 = globaltimer_ns();
+            while (!mbar_test(&full[st], (unsigned)((qq / p.NST) & 1))) {
+                if (globaltimer_ns() - t0 > kBarrierTimeoutNs)
+                    break;
+            }
+        }
+        return;
+    }
+
+    // ------------------------------------------------------------ consumers
+    const int gw = wb0 + warp;
+    const bool wact = gw < wb1;
+    const int i = gw * 32 + lane;
+    const bool act = wact && i < n;
+
+    double V = act ? p.V[i] : 0.0;
+    double tprev = 0.0, vlast = 0.0;
+    int cpos = 0;
+    long long refr = 0;
+    unsigned long long rng = 0;
+    if (act) {
+        if (NT == SP_FLIF_GL || NT == SP_FLIF_CAPUTO)
+            tprev = p.tprev[i];
+        if (NT == SP_FLIF_GL) {
+            long long pr = (p.step0 - 1) % L;
+            if (pr < 0)
+                pr += L;
+            vlast = p.ring[(size_t)pr * p.rs + i];
+        }
+        if (NT == SP_FLIF_CAPUTO)
+            cpos = p.cap_pos[i];
+        if (NT == SP_FLIF_DIFFUSIVE) {
+            refr = p.refr_until[i];
+            rng = p.rng[i];
+        }
+    }
+    double ptrace = (ST == SP_SYN_PSC_HOM && act) ? p.trace[i] : 0.0;
+    double Ilast = 0.0;
+    if (ST == SP_SYN_FRAC && act) {
+        long long pr = (p.syn_step0 - 1) % p.Ls;
+        if (pr < 0)
+            pr += p.Ls;
+        Ilast = p.Iring[(size_t)pr * n + i];
+    }
+    int cur = p.phase0;
+    double sprev = 0.0;
+    if (act)
+        sprev = ((p.spk[cur * p.nwords + gw] >> lane) & 1u) ? 1.0 : 0.0;
+    unsigned lastword = 0;
+    long long q = 0;  // stages consumed (variant 1)
+    double ext = 0.0;
+
+    // synapse prepare for the own neuron before micro-step b (src/synapse.c:145-160)
+    auto prepare = [&](long long b, int buf) {
+        if (!act)
+            return;
+        if (ST == SP_SYN_PSC_HOM) {
+            ptrace = add(mul(ptrace, p.psc_decay), mul(p.psc_omd, sprev));
+            p.eff[(size_t)buf * n + i] = ptrace;
+        } else if (ST == SP_SYN_FRAC) {
+            const long long gs = p.syn_step0 + b;
+            const int Ls = p.Ls;
+            const int head = (int)(gs % Ls);
+            const long long lim = gs < Ls ? gs : Ls - 1;
+            double hist = 0.0;
+            if (lim >= 1)
+                hist = add(hist, mul(__ldg(p.scoef + 1), Ilast));
+            int r = head - 2;
+            if (r < 0)
+                r += Ls;
+            for (int k = 2; k <= lim; ++k) {
+                hist = add(hist, mul(__ldg(p.scoef + k), __ldcg(p.Iring + (size_t)r * n + i)));
+                r = (r == 0) ? Ls - 1 : r - 1;
+            }
+            const double rhs = dvd(add(-Ilast, sprev), p.s_tau);
+            const double In = sub(mul(p.s_dta, rhs), hist);
+            p.Iring[(size_t)head * n + i] = In;
+            Ilast = In;
+            p.eff[(size_t)buf * n + i] = In;
+        } else if (ST == SP_SYN_FRAC_MEXP) {
+            double sum = 0.0;
+            for (int c = 0; c < p.Nc; ++c) {
+                double tr = p.mx_tr[(size_t)c * n + i];
+                tr = add(mul(tr, __ldg(p.mx_decay + c)), mul(__ldg(p.mx_omd + c), sprev));
+                p.mx_tr[(size_t)c * n + i] = tr;
+                sum = add(sum, mul(__ldg(p.mx_c + c), tr));
+            }
+            p.eff[(size_t)buf * n + i] = sum;
+        }
+    };
+
+    auto barrier_arrive = [&]() {
+        named_sync(NC);
+        if (tid == 0 && p.G > 1) {
+            __threadfence();
+            atomicAdd(p.bar, 1u);
+        }
+    };
+    // returns false when the launch must stop
+    auto barrier_wait = [&](long long b) -> bool {
+        if (tid == 0) {
+            int ok = 1;
+            if (p.G > 1) {
+                const unsigned target = (unsigned)(b + 1) * (unsigned)p.G;
+                if (ld_volatile_u32(p.bar) < target) {
+                    unsigned long long t0 = globaltimer_ns();
+                    unsigned long long polls = 0;
+                    while (ld_volatile_u32(p.bar) < target) {
+                        if ((++polls & 255ull) == 0) {
+                            if (ld_volatile_i32(p.err) != kErrNone) {
+                                ok = 0;
+                                break;
+                            }
+                            if (globaltimer_ns() - t0 > kBarrierTimeoutNs ||
+                                polls > kBarrierMaxPolls) {
+                                if (atomicCAS(p.err, kErrNone, kErrBarrierTimeout) == kErrNone)
+                                    p.err[1] = (int)(p.step0 + b);
+                                ok = 0;
+                                break;
+                            }
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                __threadfence();
+            }
+            if (s_abort)
+                ok = 0;
+            s_flag = ok;
+            if (!ok)
+                s_abort = 1;
+        }
+        named_sync(NC);
+        return s_flag != 0;
+    };
+
+    // prologue: drive of micro-step 0, then arrive at barrier 0
+    if (ST != SP_SYN_SIMPLE && ST != SP_SYN_PSC_HET)
+        prepare(0, cur);
+    barrier_arrive();
+
+    for (long long b = 0; b < B; ++b) {
+        const long long g = p.step0 + b;
+        const int s = (int)(b / p.micro);
+        const int m = (int)(b % p.micro);
+        if (m == 0) {
+            // ext = 0 + gamma * sum_j W_in[i][j] u[j] (netlib dgemv order)
+            ext = 0.0;
+            if (act && p.din > 0 && p.gamma != 0.0 && p.u) {
+                const double *ur = p.u + (size_t)s * p.din;
+                const double *wr = p.W_in + (size_t)i * p.din;
+                double t = 0.0;
+                for (int j = 0; j < p.din; ++j)
+                    t = add(t, mul(__ldg(wr + j), __ldg(ur + j)));
+                ext = add(0.0, mul(p.gamma, t));
+            }
+        }
+
+        // ---- FLIF_GL history sum of step g
+        bool integ = false;
+        double hist = 0.0;
+        int head = 0;
+        if (NT == SP_FLIF_GL) {
+            head = (int)(g % L);
+            integ = tprev > p.f;
+            const int lim = (int)(g < L ? g : L - 1);
+            if (act && integ && lim >= 1)
+                hist = add(hist, mul(__ldg(p.coef + 1), vlast));
+            if (VAR == 0) {
+                if (act && integ) {
+                    int r = head - 2;
+                    if (r < 0)
+                        r += L;
+                    const double *ci = p.ring + i;
+#pragma unroll 8
+                    for (int k = 2; k <= lim; ++k) {
+                        hist = add(hist, mul(__ldg(p.coef + k), __ldcg(ci + (size_t)r * p.rs)));
+                        r = (r == 0) ? L - 1 : r - 1;
+                    }
+                }
+            } else {
+                const int j = tid;
+                for (int k = 2; k <= lim && S_b > 0; k += p.R) {
+                    const int cnt = (lim - k + 1 < p.R) ? lim - k + 1 : p.R;
+                    const int st = (int)(q % p.NST);
+                    // on a failed wait the launch aborts at the next barrier_wait;
+                    // every consumer keeps the same control flow until then
+                    const bool landed =
+                        mbar_wait(&full[st], (unsigned)((q / p.NST) & 1), &s_abort, p.err);
+                    const double *buf = s_stage + (size_t)st * p.R * SW + j;
+                    if (landed && act && integ) {
+                        if (cnt == 16) {
+#pragma unroll
+                            for (int jr = 0; jr < 16; ++jr)
+                                hist = add(hist, mul(__ldg(p.coef + k + jr), buf[(size_t)jr * SW]));
+                        } else {
+                            for (int jr = 0; jr < cnt; ++jr)
+                                hist = add(hist, mul(__ldg(p.coef + k + jr), buf[(size_t)jr * SW]));
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                        mbar_arrive(&empty[st]);
+                    ++q;
+                }
+            }
+        }
+
+        // ---- barrier: spikes / eff of step g-1 are visible
+        if (!barrier_wait(b))
+            return;
+        if (ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET) {
+            for (int wi = tid; wi < p.nwords; wi += NC)
+                s_spk[wi] = __ldcg(p.spk + (size_t)cur * p.nwords + wi);
+            named_sync(NC);
+        }
+
+        // ---- recurrent input
+        double rec = 0.0;
+        if (ST == SP_SYN_SIMPLE) {
+            if (wact) {
+                const int row0 = gw * 32;
+                const int nv = (n - row0 < 32) ? n - row0 : 32;
+                rec = rowpass_simple_warp(p.row_ptr, p.col, p.w, s_spk, row0, nv, lane);
+            }
+        } else if (act) {
+            const long long k0 = __ldg(p.row_ptr + i), k1 = __ldg(p.row_ptr + i + 1);
+            if (ST == SP_SYN_PSC_HET) {
+                for (long long k = k0; k < k1; ++k) {
+                    const int c = __ldg(p.col + k);
+                    const double sv = ((s_spk[c >> 5] >> (c & 31)) & 1u) ? 1.0 : 0.0;
+                    const double tr = add(mul(p.edge_trace[k], __ldg(p.edge_decay + k)),
+                                          mul(__ldg(p.edge_omd + k), sv));
+                    p.edge_trace[k] = tr;
+                    rec = add(rec, mul(__ldg(p.w + k), tr));
+                }
+            } else {
+                const double *ef = p.eff + (size_t)cur * n;
+                for (long long k = k0; k < k1; ++k) {
+                    const int c = __ldg(p.col + k);
+                    rec = add(rec, mul(__ldg(p.w + k), __ldcg(ef + c)));
+                }
+            }
+        }
+
+        // ---- neuron update (operation order of src/neurons/<model>.c)
+        bool fired = false;
+        if (act) {
+            const double in = add(ext, rec);
+            if (NT == SP_LIF_DISCRETE) {
+                V = add(add(mul(p.c, V), in), p.d);
+                if (V > p.b) {
+                    V = p.a;
+                    fired = true;
+                }
+            } else if (NT == SP_LIF_BIO) {
+                const double dV = dvd(add(add(-V, in), p.d), p.c);
+                V = add(V, mul(dV, p.dt));
+                if (V >= p.b) {
+                    V = p.a;
+                    fired = true;
+                }
+            } else if (NT == SP_FLIF_GL) {
+                if (integ) {
+                    const double rhs = add(add(dvd(-sub(vlast, p.c), p.d), in), p.e);
+                    V = sub(mul(p.g, rhs), hist);
+                    if (V >= p.a) {
+                        V = p.b;
+                        fired = true;
+                        tprev = 0.0;
+                    }
+                } else {
+                    V = p.b;
+                }
+                p.ring[(size_t)head * p.rs + i] = V;
+                vlast = V;
+                tprev = add(tprev, p.dt);
+            } else if (NT == SP_FLIF_CAPUTO) {
+                if (tprev > p.f) {
+                    const double dV = dvd(add(mul(-p.c, sub(V, p.d)), in), p.e);
+                    const double markov = mul(p.g, dV);
+                    const int D = L;
+                    double *rg = p.ring + (size_t)i * D;
+                    rg[cpos] = sub(V, p.b);
+                    int qq = cpos;
+                    cpos = (cpos + 1 == D) ? 0 : cpos + 1;
+                    double mem = 0.0;
+                    for (int k = 0; k < D; ++k) {
+                        mem = add(mem, mul(__ldg(p.coef + k), rg[qq]));
+                        qq = (qq == 0) ? D - 1 : qq - 1;
+                    }
+                    V = add(V, sub(markov, mem));
+                    if (V >= p.a) {
+                        V = p.b;
+                        fired = true;
+                        tprev = 0.0;
+                    }
+                } else {
+                    V = p.b;
+                }
+                tprev = add(tprev, p.dt);
+            } else if (NT == SP_FLIF_DIFFUSIVE) {
+                const double Vp = V;
+                const double rhs = add(add(-sub(Vp, p.c), in), p.d);
+                V = add(Vp, mul(p.e, rhs));
+                if (g >= refr && V >= p.a) {
+                    V = p.b;
+                    fired = true;
+                    long long steps;
+                    if (p.diff_sto) {
+                        double W;
+                        const double u0 = u01(&rng);
+                        if (u0 < p.ci) {
+                            W = p.h;
+                        } else {
+                            const double u1 = u01(&rng);
+                            const double tmin = p.f, tmax = p.g, qx = p.cj;
+                            if (tmax <= tmin)
+                                W = tmin;
+                            else if (qx <= 1e-12)
+                                W = tmin + u1 * (tmax - tmin);
+                            else if (fabs(qx - 1.0) < 1e-12)
+                                W = tmin * pow(tmax / tmin, u1);
+                            else
+                                W = pow((1.0 - u1) * p.ck + u1 * p.cl, 1.0 / (1.0 - qx));
+                        }
+                        steps = (W <= 0.0) ? 0 : (long long)ceil(W / p.dt);
+                        if (steps < 1)
+                            steps = 1;
+                    } else {
+                        steps = p.det_refr;
+                    }
+                    refr = g + steps;
+                }
+            }
+        }
+        if (VAR == 1)
+            fence_proxy_async();  // ring row of step g is read by bulk copies later
+
+        // ---- spike word of step g
+        const unsigned word = __ballot_sync(kFull, fired);
+        if (wact && lane == 0)
+            p.spk[(size_t)(cur ^ 1) * p.nwords + gw] = word;
+        lastword = word;
+        sprev = fired ? 1.0 : 0.0;
+        if (m == p.micro - 1) {
+            if (act && p.phi)
+                p.phi[(size_t)s * n + i] = V;
+            if (wact && lane == 0 && p.raster)
+                p.raster[(size_t)s * p.nwords + gw] = lastword;
+        }
+        if (b + 1 < B) {
+            if (ST != SP_SYN_SIMPLE && ST != SP_SYN_PSC_HET)
+                prepare(b + 1, cur ^ 1);
+            barrier_arrive();
+            if (VAR == 1 && tid == 0)
+                st_release_cta(&s_done, (int)(b + 1));
+        }
+        cur ^= 1;
+    }
+
+    if (act) {
+        p.V[i] = V;
+        if (NT == SP_FLIF_GL || NT == SP_FLIF_CAPUTO)
+            p.tprev[i] = tprev;
+        if (NT == SP_FLIF_CAPUTO)
+            p.cap_pos[i] = cpos;
+        if (NT == SP_FLIF_DIFFUSIVE) {
+            p.refr_until[i] = refr;
+            p.rng[i] = rng;
+        }
+        if (ST == SP_SYN_PSC_HOM)
+            p.trace[i] = ptrace;
+    }
+}
+
+}  // namespace sp

@@ -178,3 +178,42 @@ def test_flif_gl_n4000_l512_small_world():
     assert ras.mean() > 0.01
     assert np.array_equal(ras, ras_o)
     assert same_bits(phi, phi_o)
+
+
+GL_L = lambda L: (1.0, 0.0, 0.0, 20.0, 0.7, float(L), 0.1, 2.0)
+
+
+@pytest.mark.parametrize("L", [3, 8, 33, 200])
+@pytest.mark.parametrize("shape", [dict(ctas=1, warps_max=8, rows=16, stages=2),
+                                   dict(ctas=4, warps_max=2, rows=3, stages=3),
+                                   dict(ctas=8, warps_max=1, rows=1, stages=4),
+                                   dict(ctas=2, warps_max=4, rows=16, stages=8)])
+def test_flif_gl_bulk_copy_pipeline(L, shape):
+    """The bulk-copy ring pipeline (variant 1) gives the bits of the oracle for
+    ring lengths shorter and longer than its depth, during ramp-up (step < L)
+    and after the ring wraps."""
+    cfg = make(sp.FLIF_GL, sp.SYN_SIMPLE, n=250, conn=0.03, nparams=GL_L(L))
+    mine, ref, _ = run_both(cfg, seed=13, T=2 * L + 40, launch=dict(variant=1, **shape))
+    assert_parity(mine, ref, 2)
+
+
+@pytest.mark.parametrize("synapse", SYNAPSES)
+def test_flif_gl_pipeline_all_synapses(synapse):
+    cfg = make(sp.FLIF_GL, synapse, n=300, conn=0.03, nparams=GL_L(96))
+    a, ref, _ = run_both(cfg, seed=17, T=150, launch=dict(variant=1, ctas=3, warps_max=4,
+                                                          rows=16, stages=4))
+    assert_parity(a, ref, 2)
+    b, _, _ = run_both(cfg, seed=17, T=150, launch=dict(variant=0, ctas=3, warps_max=4))
+    assert same_bits(a[0], b[0])
+
+
+def test_flif_gl_pipeline_chunked_runs_continue():
+    """Several launches in a row (state carried in HBM between them) equal one."""
+    cfg = make(sp.FLIF_GL, sp.SYN_SIMPLE, n=500, conn=0.02, nparams=GL_L(128))
+    u = inputs(300, 2)
+    r = sp.Reservoir(cfg, seed=19)
+    parts = [r.run_record(u[a:b])[0] for a, b in [(0, 1), (1, 50), (50, 129), (129, 300)]]
+    r.close()
+    phi = np.concatenate(parts)
+    phi_o, _, _ = O.Oracle(cfg, sp.HostModel(cfg, seed=19)).run(u)
+    assert same_bits(phi, phi_o)
