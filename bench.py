@@ -227,6 +227,9 @@ def run_gpu_arm(args, rank, world):
     lib = sp.load()
     cfg = workload_config(sp)
     r = sp.Reservoir(cfg, seed=SEED + rank)
+    if args.variant >= 0:
+        assert r.set_launch(variant=args.variant) == sp.SPIRES_OK
+    lau = r.launch()
     S = args.chunk
     fill = L_HIST + 8
     total = fill + (args.warmup + args.steps) * S
@@ -325,6 +328,8 @@ def run_gpu_arm(args, rank, world):
                      "algorithmic_bytes_per_launch": bpl, "avg_launch_ms": avg_ms,
                      "spike_rate": rate},
         "clocks": clocks, "gpu_launches": int(launches), "e2e": e2e,
+        "launch": {"ctas": lau.ctas, "warps": lau.warps_max, "variant": lau.variant,
+                   "stages": lau.stages, "rows": lau.rows},
     }
     return line
 
@@ -340,6 +345,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1, help="force step-kernel variant")
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
     args = ap.parse_args()

@@ -778,8 +778,12 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
 
     {
         const size_t tot = (size_t)n * dout;
-        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, d->W_out);
-        RK(cudaMemcpyAsync(h_W_out, d->W_out, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+        // W (n x dout) -> W_out (dout x n) in R, host mirror, position-space copy
+        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, R);
+        RK(cudaMemcpyAsync(h_W_out, R, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+        rc = sp_dev_w_out_from_nat(d, R);
+        if (rc)
+            goto out;
         RK(cudaStreamSynchronize(s));
         RK(cudaGetLastError());
     }
@@ -796,16 +800,18 @@ extern "C" int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double 
                                 const double *h_y, size_t T, double delta, double lambda,
                                 double *h_W_out)
 {
+    // state, W_out and P live in position space (holes keep x = 0 and stay inert)
     int rc = SP_OK;
-    const int n = d->n, dout = d->dout;
+    const int rs = d->rs, n = d->n, dout = d->dout;
     cudaStream_t s = d->stream;
-    double *P = nullptr, *Px = nullptr, *scal = nullptr, *Yd = nullptr;
-    RK(cudaMalloc(&P, (size_t)n * n * sizeof(double)));
-    RK(cudaMalloc(&Px, (size_t)n * sizeof(double)));
+    double *P = nullptr, *Px = nullptr, *scal = nullptr, *Yd = nullptr, *Wn = nullptr;
+    RK(cudaMalloc(&P, (size_t)rs * rs * sizeof(double)));
+    RK(cudaMalloc(&Px, (size_t)rs * sizeof(double)));
     RK(cudaMalloc(&scal, (size_t)(dout + 1) * sizeof(double)));
     RK(cudaMalloc(&Yd, (T ? T : 1) * (size_t)(dout ? dout : 1) * sizeof(double)));
-    k_diag_init<<<1024, 256, 0, s>>>(P, n, 1.0 / delta);
-    RK(cudaMemsetAsync(d->W_out, 0, (size_t)n * dout * sizeof(double), s));
+    RK(cudaMalloc(&Wn, (size_t)(dout ? dout : 1) * n * sizeof(double)));
+    k_diag_init<<<1024, 256, 0, s>>>(P, rs, 1.0 / delta);
+    RK(cudaMemsetAsync(d->W_out, 0, (size_t)rs * dout * sizeof(double), s));
     if (T && dout)
         RK(cudaMemcpyAsync(Yd, h_y, T * dout * sizeof(double), cudaMemcpyHostToDevice, s));
     rc = sp_dev_reset_neurons(d, m);
@@ -819,12 +825,16 @@ extern "C" int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double 
         rc = sp_dev_run(d, &a);
         if (rc)
             goto out;
-        k_gemv_rows<<<(n + 7) / 8, 256, 0, s>>>(P, n, d->V, Px);
-        k_rls_scalars<<<1, 256, 0, s>>>(d->V, Px, n, lambda, d->W_out, dout, Yd + t * dout, scal);
-        k_rls_update<<<4 * d->num_sms, 256, 0, s>>>(P, n, Px, scal, lambda, d->W_out, dout);
+        k_gemv_rows<<<(rs + 7) / 8, 256, 0, s>>>(P, rs, d->V, Px);
+        k_rls_scalars<<<1, 256, 0, s>>>(d->V, Px, rs, lambda, d->W_out, dout, Yd + t * dout,
+                                        scal);
+        k_rls_update<<<4 * d->num_sms, 256, 0, s>>>(P, rs, Px, scal, lambda, d->W_out, dout);
     }
-    RK(cudaMemcpyAsync(h_W_out, d->W_out, (size_t)n * dout * sizeof(double),
-                       cudaMemcpyDeviceToHost, s));
+    rc = sp_dev_w_out_to_nat(d, Wn);
+    if (rc)
+        goto out;
+    RK(cudaMemcpyAsync(h_W_out, Wn, (size_t)n * dout * sizeof(double), cudaMemcpyDeviceToHost,
+                       s));
     RK(cudaStreamSynchronize(s));
     RK(cudaGetLastError());
 out:
@@ -833,28 +843,37 @@ out:
     if (Px) cudaFree(Px);
     if (scal) cudaFree(scal);
     if (Yd) cudaFree(Yd);
+    if (Wn) cudaFree(Wn);
     return rc;
 }
 
 extern "C" int sp_dev_train_online(sp_dev *d, const double *h_target, double lr, double *h_W_out)
 {
     int rc = SP_OK;
-    const int n = d->n, dout = d->dout;
+    const int rs = d->rs, n = d->n, dout = d->dout;
     cudaStream_t s = d->stream;
+    double *Wn = nullptr;
     if (dout == 0)
         return SP_OK;
     // prediction with the same readout kernel as spires_compute_output
     rc = sp_dev_readout(d, d->V, 1, d->d_y);
     if (rc)
         return rc;
+    RK(cudaMalloc(&Wn, (size_t)dout * n * sizeof(double)));
     RK(cudaMemcpyAsync(d->d_y + dout, h_target, (size_t)dout * sizeof(double),
                        cudaMemcpyHostToDevice, s));
-    k_online<<<(unsigned)(((size_t)n * dout + 255) / 256), 256, 0, s>>>(d->W_out, n, dout, d->V,
-                                                                       d->d_y, d->d_y + dout, lr);
-    RK(cudaMemcpyAsync(h_W_out, d->W_out, (size_t)n * dout * sizeof(double),
-                       cudaMemcpyDeviceToHost, s));
+    k_online<<<(unsigned)(((size_t)rs * dout + 255) / 256), 256, 0, s>>>(d->W_out, rs, dout, d->V,
+                                                                        d->d_y, d->d_y + dout, lr);
+    rc = sp_dev_w_out_to_nat(d, Wn);
+    if (rc)
+        goto out;
+    RK(cudaMemcpyAsync(h_W_out, Wn, (size_t)n * dout * sizeof(double), cudaMemcpyDeviceToHost,
+                       s));
     RK(cudaStreamSynchronize(s));
     RK(cudaGetLastError());
 out:
+    cudaStreamSynchronize(s);
+    if (Wn)
+        cudaFree(Wn);
     return rc;
 }

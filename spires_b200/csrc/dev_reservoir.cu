@@ -1,22 +1,15 @@
-// dev_reservoir.cu -- device state of one reservoir and the persistent
-// multi-step kernel that advances it.
+// dev_reservoir.cu -- device state of one reservoir and the host side of the
+// persistent step kernel (sp_step_kernel.cuh).
 //
-// One cooperative launch runs T macro steps x (1/dt) micro-steps. Each CTA owns
-// a contiguous range of whole warps of neurons; a thread owns one neuron and
-// keeps its state in registers for the whole launch. Per micro-step:
-//
-//   1. synapse "prepare" for the thread's own neuron (needs only its own spike
-//      of the previous micro-step): PSC traces, fractional current, multi-exp
-//      traces -> eff[i]                               (src/synapse.c:145-160)
-//   2. FLIF_GL history sum over the time-major ring (own column only)
-//                                                     (src/neurons/flif_gl.c:61-72)
-//   3. grid barrier: every eff[] and every spike word of the previous
-//      micro-step is visible
-//   4. recurrent input: ascending-column walk over the neuron's CSR row
-//      (src/sparse.c:68-76); SIMPLE adds w only where the presynaptic spike
-//      bit is set (w * 0.0 = +-0 leaves a sum that started at +0 unchanged)
-//   5. neuron update in the reference's operation order (src/neurons/*.c)
-//   6. warp ballot -> one 32-bit spike word per warp, double-buffered
+// Neuron layout. Device state lives in "position" space: neurons are sorted by
+// CSR row length (descending) and dealt round-robin over the ceil(n/32) warps,
+// rank r going to warp r % nw, lane r / nw. Every warp (and so every CTA) gets
+// the same mix of long and short rows; without it a heavy-tailed graph
+// (Barabasi-Albert hubs are the oldest, lowest-index nodes) puts most CSR
+// edges in one warp, whose row walk then paces the whole grid every step.
+// Only storage moves: each row keeps its edges in the original ascending
+// column order, so every sum is formed in the reference's order, and results
+// are returned in neuron order (gather kernels below).
 //
 // Reference for the whole loop: step_reservoir, src/reservoir.c:113-165.
 #include <cuda_runtime.h>
@@ -25,6 +18,9 @@
 #include <cstring>
 #include <cstdio>
 #include <cmath>
+#include <algorithm>
+#include <numeric>
+#include <vector>
 #include "sp_dev.h"
 #include "sp_kernels.cuh"
 #include "sp_dev_internal.h"
@@ -65,23 +61,29 @@ kfn_t pick_kernel(int nt, int st, int variant)
 
 // ---------------------------------------------------------------- resets --
 
-__global__ void k_reset_neurons(int n, int L, size_t ring_elems, int ntype, double v_init,
-                                double tprev_init, double *V, double *tprev, double *ring,
-                                int *cap_pos, long long *refr, unsigned long long *rng,
+__global__ void k_reset_neurons(int n, int nw, int L, size_t ring_elems, int ntype,
+                                double v_init, double tprev_init, double *V, double *tprev,
+                                double *ring, int *cap_pos, long long *refr,
+                                unsigned long long *rng, const int *nid_of,
                                 unsigned long long seed)
 {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
-        V[i] = v_init;
+    const size_t rs = (size_t)nw * 32;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < rs; q += stride) {
+        const bool act = nid_of[q] >= 0;
+        V[q] = act ? v_init : 0.0;
         if (ntype == SP_FLIF_GL || ntype == SP_FLIF_CAPUTO)
-            tprev[i] = tprev_init;
+            tprev[q] = tprev_init;
         if (ntype == SP_FLIF_CAPUTO)
-            cap_pos[i] = 0;
+            cap_pos[q] = 0;
         if (ntype == SP_FLIF_DIFFUSIVE) {
-            refr[i] = -1;
-            unsigned long long s = seed ^ (0xD1B54A32D192ED03ull * (i + 1));
+            refr[q] = -1;
+            // stream of neuron nid: seeded from the reservoir seed and the neuron
+            // index, so it does not depend on the storage layout
+            unsigned long long s =
+                seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)((act ? nid_of[q] : 0) + 1));
             splitmix64(&s);
-            rng[i] = s;
+            rng[q] = s;
         }
     }
     if (ring) {
@@ -93,19 +95,19 @@ __global__ void k_reset_neurons(int n, int L, size_t ring_elems, int ntype, doub
     }
 }
 
-// Readout y[t][o] = sum_i W_out[o][i] x[t][i]: one CTA per (t, o), a fixed
-// thread-strided partition and a fixed shuffle tree, so the result is the same
-// bit pattern whichever path (spires_run, spires_compute_output) asks for it.
+// Readout y[t][o] = sum_q W_out[o][q] x[t][q] over positions: one CTA per
+// (t, o), a fixed thread-strided partition and a fixed shuffle tree, so every
+// path (spires_run, spires_compute_output) gets the same bits.
 __global__ void __launch_bounds__(256) k_readout(const double *__restrict__ W_out,
-                                                 const double *__restrict__ X, int n, int dout,
+                                                 const double *__restrict__ X, int rs, int dout,
                                                  double *__restrict__ Y)
 {
     __shared__ double part[8];
     const int t = blockIdx.x, o = blockIdx.y;
-    const double *x = X + (size_t)t * n;
-    const double *wr = W_out + (size_t)o * n;
+    const double *x = X + (size_t)t * rs;
+    const double *wr = W_out + (size_t)o * rs;
     double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += 256)
+    for (int i = threadIdx.x; i < rs; i += 256)
         s = add(s, mul(wr[i], x[i]));
     for (int off = 16; off > 0; off >>= 1)
         s = add(s, __shfl_xor_sync(kFull, s, off));
@@ -120,10 +122,67 @@ __global__ void __launch_bounds__(256) k_readout(const double *__restrict__ W_ou
     }
 }
 
-__global__ void k_spikes_to_double(const unsigned *words, int n, double *out)
+// out[t][i] = in[t][pos[i]]  (T rows; position rows have stride rs)
+__global__ void k_gather_rows(const double *__restrict__ in, int rs, const int *__restrict__ pos,
+                              int n, size_t T, double *__restrict__ out)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        out[i] = ((words[i >> 5] >> (i & 31)) & 1u) ? 1.0 : 0.0;
+    const size_t total = T * (size_t)n;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = k / n;
+        const int i = (int)(k % n);
+        out[k] = in[t * rs + pos[i]];
+    }
+}
+
+// out[q] = in[nid_of[q]] (0 at holes); in has n entries, out rs
+__global__ void k_scatter_vec(const double *__restrict__ in, const int *__restrict__ nid_of,
+                              int rs, double *__restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rs; q += gridDim.x * blockDim.x)
+        out[q] = nid_of[q] >= 0 ? in[nid_of[q]] : 0.0;
+}
+
+// W_out in position space [dout][rs] <-> neuron space [dout][n]
+__global__ void k_wout_to_pos(const double *__restrict__ w_nat, const int *__restrict__ nid_of,
+                              int n, int rs, int dout, double *__restrict__ w_pos)
+{
+    const size_t total = (size_t)dout * rs;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int o = (int)(k / rs), q = (int)(k % rs);
+        const int i = nid_of[q];
+        w_pos[k] = i >= 0 ? w_nat[(size_t)o * n + i] : 0.0;
+    }
+}
+
+// spike words in neuron order from position-space words: bit i%32 of word i/32
+__global__ void k_gather_bits(const unsigned *__restrict__ in, int nw, const int *__restrict__ pos,
+                              int n, size_t T, unsigned *__restrict__ out)
+{
+    const size_t words = (size_t)nw;
+    const size_t total = T * words * 32;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = k / (words * 32);
+        const int i = (int)(k % (words * 32));
+        bool b = false;
+        if (i < n) {
+            const int q = pos[i];
+            b = (in[t * words + (q >> 5)] >> (q & 31)) & 1u;
+        }
+        const unsigned m = __ballot_sync(kFull, b);
+        if ((threadIdx.x & 31) == 0)
+            out[t * words + (i >> 5)] = m;
+    }
+}
+
+__global__ void k_bits_to_double(const unsigned *words, const int *pos, int n, double *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int q = pos[i];
+        out[i] = ((words[q >> 5] >> (q & 31)) & 1u) ? 1.0 : 0.0;
+    }
 }
 
 }  // namespace
@@ -182,15 +241,73 @@ static int upload_consts(sp_dev *d, const sp_host_model *m)
     return SP_OK;
 }
 
+static unsigned gather_blocks(size_t total)
+{
+    size_t b = (total + 255) / 256;
+    return (unsigned)(b > 8192 ? 8192 : (b ? b : 1));
+}
+
+static void box_geometry(const sp_launch &l, int *bw, int *nbx)
+{
+    const int sw = 32 * l.warps_max;
+    *bw = sw < 256 ? sw : 256;
+    *nbx = (sw + *bw - 1) / *bw;
+}
+
+// variant 1 stages the coefficient table in shared memory up to 64 KB
+static size_t coef_smem_bytes(const sp_dev *d)
+{
+    const size_t b = ((size_t)d->nc.L * 8 + 127) & ~(size_t)127;
+    return b <= 64 * 1024 ? b : 0;
+}
+
 // dynamic shared memory of a launch shape: spike words, then (variant 1) the
 // ring-row stages and their full/empty mbarriers
 static size_t launch_smem(const sp_dev *d, const sp_launch &l)
 {
     size_t spk = ((d->nwords * 4) + 127) & ~(size_t)127;
-    if (l.variant == 1)
-        return spk + (size_t)l.stages * l.rows * 32 * l.warps_max * sizeof(double) +
+    if (l.variant == 1) {
+        int bw, nbx;
+        box_geometry(l, &bw, &nbx);
+        return spk + coef_smem_bytes(d) + (size_t)l.stages * nbx * l.rows * bw * sizeof(double) +
                2 * (size_t)l.stages * sizeof(unsigned long long);
+    }
     return spk;
+}
+
+typedef CUresult (*encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                    const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                    const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// Tiled map of the FLIF_GL ring: dims {rs, L}, row pitch rs*8 bytes, box
+// {bw, r}; out-of-range rows/columns of a box read as zero.
+static int encode_ring_map(sp_dev *d, int bw, int r)
+{
+    if (d->tmap_bw == bw && d->tmap_r == r)
+        return SP_OK;
+    static encode_tiled_fn enc = nullptr;
+    if (!enc) {
+        void *fp = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            !fp)
+            return SP_EINTERNAL;
+        enc = (encode_tiled_fn)fp;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)d->rs, (cuuint64_t)d->nc.L};
+    cuuint64_t strides[1] = {(cuuint64_t)d->rs * sizeof(double)};
+    cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)r};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult res = enc(&d->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, d->ring, dims, strides, box,
+                       estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (res != CUDA_SUCCESS)
+        return SP_EINTERNAL;
+    d->tmap_bw = bw;
+    d->tmap_r = r;
+    return SP_OK;
 }
 
 static int max_smem(const sp_dev *d)
@@ -215,22 +332,65 @@ static void default_launch(sp_dev *d)
         if (l.warps_max > 32)
             l.warps_max = 32;
     }
-    if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 31) {
+    if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 16) {
         sp_launch v = l;
         v.variant = 1;
         v.rows = 16;
-        const size_t stage = (size_t)v.rows * 32 * v.warps_max * sizeof(double);
+        int bw, nbx;
+        box_geometry(v, &bw, &nbx);
+        const size_t stage = (size_t)v.rows * nbx * bw * sizeof(double);
         const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
-        const size_t spk = ((d->nwords * 4) + 127) & ~(size_t)127;
+        const size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d);
         long long st = budget > spk ? (long long)((budget - spk) / (stage + 16)) : 0;
         if (st > 16)
             st = 16;
-        if (st >= 2) {
+        if (st >= 2 && v.rows <= 256 &&
+            encode_ring_map(d, bw, v.rows < d->nc.L ? v.rows : d->nc.L) == SP_OK) {
             v.stages = (int)st;
             l = v;
         }
     }
     d->launch = l;
+}
+
+
+// Position layout: neurons in order of decreasing row length go, one by one,
+// to the warp with the fewest CSR edges so far that still has a free lane
+// (longest-processing-time assignment), lanes filled from 0. Every warp, and
+// so every CTA, ends up with about the same number of edges to walk.
+// pos_of[i] = position of neuron i, nid_of[q] = neuron at position q or -1.
+static void make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
+                        std::vector<int> &nid_of)
+{
+    const int n = (int)m->n;
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    auto deg = [&](int i) { return (long long)(m->row_ptr[i + 1] - m->row_ptr[i]); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return deg(a) > deg(b); });
+    pos_of.assign(n, 0);
+    nid_of.assign((size_t)nw * 32, -1);
+    // min-heap of (edges, warp) over warps with a free lane
+    typedef std::pair<long long, int> ent;
+    std::vector<ent> heap;
+    heap.reserve(nw);
+    for (int w = 0; w < nw; ++w)
+        heap.push_back(ent(0, w));
+    std::vector<int> fill(nw, 0);
+    auto cmp = [](const ent &a, const ent &b) { return a > b; };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    for (int r = 0; r < n; ++r) {
+        std::pop_heap(heap.begin(), heap.end(), cmp);
+        ent e = heap.back();
+        heap.pop_back();
+        const int w = e.second;
+        const int q = w * 32 + fill[w]++;
+        pos_of[order[r]] = q;
+        nid_of[q] = order[r];
+        if (fill[w] < 32) {
+            heap.push_back(ent(e.first + deg(order[r]), w));
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+    }
 }
 
 extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
@@ -265,6 +425,8 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
     d->din = (int)m->din;
     d->dout = (int)m->dout;
     d->nwords = (m->n + 31) / 32;
+    d->nw = (int)d->nwords;
+    d->rs = d->nw * 32;
     d->micro = m->micro_steps;
     d->dt = m->dt;
     d->gamma = m->input_strength;
@@ -275,74 +437,105 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
     d->sc = m->sc;
     d->seed = m->diffusive_seed;
     {
-        const size_t n = m->n;
+        const size_t n = m->n, rs = (size_t)d->rs, din = m->din, dout = m->dout;
         cudaStream_t s = d->stream;
-        TRY(dalloc(&d->V, n));
-        TRY(dalloc(&d->tprev, n));
+        std::vector<int> pos_of, nid_of;
+        make_layout(m, d->nw, pos_of, nid_of);
+        // CSR in position order: row q = neuron nid_of[q], edges in their original
+        // order, column index mapped to the presynaptic neuron's position
+        std::vector<long long> rp(rs + 1, 0);
+        std::vector<int> col(m->nnz ? m->nnz : 1);
+        std::vector<double> w(m->nnz ? m->nnz : 1), ed, eo;
+        if (m->syn_type == SP_SYN_PSC_HET) {
+            ed.resize(m->nnz ? m->nnz : 1);
+            eo.resize(m->nnz ? m->nnz : 1);
+        }
+        std::vector<double> win(rs * (din ? din : 1), 0.0), wout(dout * rs, 0.0);
+        size_t e = 0;
+        for (size_t q = 0; q < rs; ++q) {
+            rp[q] = (long long)e;
+            const int i = nid_of[q];
+            if (i < 0)
+                continue;
+            for (int64_t k = m->row_ptr[i]; k < m->row_ptr[i + 1]; ++k, ++e) {
+                col[e] = pos_of[m->col[k]];
+                w[e] = m->w[k];
+                if (m->syn_type == SP_SYN_PSC_HET) {
+                    ed[e] = m->edge_decay[k];
+                    eo[e] = m->edge_omd[k];
+                }
+            }
+            for (size_t j = 0; j < din; ++j)
+                win[q * din + j] = m->W_in[(size_t)i * din + j];
+            for (size_t o = 0; o < dout; ++o)
+                wout[o * rs + q] = m->W_out[o * n + i];
+        }
+        rp[rs] = (long long)e;
+        TRY(dupload(&d->pos_of, pos_of.data(), n, s));
+        TRY(dupload(&d->nid_of, nid_of.data(), rs, s));
+        TRY(dalloc(&d->V, rs));
+        TRY(dalloc(&d->tprev, rs));
         TRY(dalloc(&d->spk, 2 * d->nwords));
         TRY(dalloc(&d->bar, 4));
         TRY(dalloc(&d->err, 4));
-        TRY(dupload(&d->row_ptr, (const long long *)m->row_ptr, n + 1, s));
-        TRY(dupload(&d->col, (const int *)m->col, m->nnz, s));
-        TRY(dupload(&d->w, m->w, m->nnz, s));
-        TRY(dupload(&d->W_in, m->W_in, n * m->din, s));
-        TRY(dupload(&d->W_out, m->W_out, n * m->dout, s));
-        d->rs = (int)((n + 31) / 32 * 32);
+        TRY(dupload(&d->row_ptr, rp.data(), rs + 1, s));
+        TRY(dupload(&d->col, col.data(), m->nnz, s));
+        TRY(dupload(&d->w, w.data(), m->nnz, s));
+        TRY(dupload(&d->W_in, win.data(), rs * din, s));
+        TRY(dupload(&d->W_out, wout.data(), rs * dout, s));
         if (m->neuron_type == SP_FLIF_GL || m->neuron_type == SP_FLIF_CAPUTO) {
             TRY(dupload(&d->coef, m->coef, (size_t)m->nc.L, s));
-            // FLIF_GL: [L][rs] time-major rows; Caputo: [n][D] per-neuron registers
-            d->ring_elems = (m->neuron_type == SP_FLIF_GL) ? (size_t)d->rs * m->nc.L
-                                                            : n * (size_t)m->nc.L;
+            // FLIF_GL: [L][rs] time-major rows; Caputo: [rs][D] per-position registers
+            d->ring_elems = rs * (size_t)m->nc.L;
             TRY(dalloc(&d->ring, d->ring_elems));
         }
         if (m->neuron_type == SP_FLIF_CAPUTO)
-            TRY(dalloc(&d->cap_pos, n));
+            TRY(dalloc(&d->cap_pos, rs));
         if (m->neuron_type == SP_FLIF_DIFFUSIVE) {
-            TRY(dalloc(&d->refr_until, n));
-            TRY(dalloc(&d->rng, n));
+            TRY(dalloc(&d->refr_until, rs));
+            TRY(dalloc(&d->rng, rs));
         }
-        if (m->syn_type != SP_SYN_SIMPLE)
-            TRY(dalloc(&d->eff, 2 * n));
+        if (m->syn_type != SP_SYN_SIMPLE) {
+            TRY(dalloc(&d->eff, 2 * rs));
+            SP_CK(cudaMemsetAsync(d->eff, 0, 2 * rs * sizeof(double), s));
+        }
         if (m->syn_type == SP_SYN_PSC_HOM) {
-            TRY(dalloc(&d->trace, n));
-            SP_CK(cudaMemsetAsync(d->trace, 0, n * sizeof(double), s));
+            TRY(dalloc(&d->trace, rs));
+            SP_CK(cudaMemsetAsync(d->trace, 0, rs * sizeof(double), s));
         }
         if (m->syn_type == SP_SYN_PSC_HET) {
-            TRY(dupload(&d->edge_decay, m->edge_decay, m->nnz, s));
-            TRY(dupload(&d->edge_omd, m->edge_omd, m->nnz, s));
+            TRY(dupload(&d->edge_decay, ed.data(), m->nnz, s));
+            TRY(dupload(&d->edge_omd, eo.data(), m->nnz, s));
             TRY(dalloc(&d->edge_trace, m->nnz));
             SP_CK(cudaMemsetAsync(d->edge_trace, 0, (m->nnz ? m->nnz : 1) * sizeof(double), s));
         }
         if (m->syn_type == SP_SYN_FRAC) {
             TRY(dupload(&d->scoef, m->syn_coef, (size_t)m->sc.frac_L, s));
-            TRY(dalloc(&d->Iring, n * (size_t)m->sc.frac_L));
-            SP_CK(cudaMemsetAsync(d->Iring, 0, n * (size_t)m->sc.frac_L * sizeof(double), s));
+            TRY(dalloc(&d->Iring, rs * (size_t)m->sc.frac_L));
+            SP_CK(cudaMemsetAsync(d->Iring, 0, rs * (size_t)m->sc.frac_L * sizeof(double), s));
         }
         if (m->syn_type == SP_SYN_FRAC_MEXP) {
             TRY(dupload(&d->mx_decay, m->mexp_decay, (size_t)m->sc.mexp_N, s));
             TRY(dupload(&d->mx_omd, m->mexp_omd, (size_t)m->sc.mexp_N, s));
             TRY(dupload(&d->mx_c, m->mexp_c, (size_t)m->sc.mexp_N, s));
-            TRY(dalloc(&d->mx_tr, n * (size_t)m->sc.mexp_N));
-            SP_CK(cudaMemsetAsync(d->mx_tr, 0, n * (size_t)m->sc.mexp_N * sizeof(double), s));
+            TRY(dalloc(&d->mx_tr, rs * (size_t)m->sc.mexp_N));
+            SP_CK(cudaMemsetAsync(d->mx_tr, 0, rs * (size_t)m->sc.mexp_N * sizeof(double), s));
         }
-        // chunk buffers for host-driven runs: inputs, states and readouts
-        size_t rows = (size_t)(128u << 20) / (n * sizeof(double));
+        // staging for host-driven runs: inputs, position-space states, readouts
+        size_t rows = (size_t)(128u << 20) / (rs * sizeof(double));
         if (rows < 1)
             rows = 1;
         if (rows > 8192)
             rows = 8192;
         d->chunk = rows;
-        TRY(dalloc(&d->d_u, rows * (m->din ? m->din : 1)));
-        TRY(dalloc(&d->d_phi, rows * n));
-        TRY(dalloc(&d->d_y, rows * (m->dout ? m->dout : 1)));
+        TRY(dalloc(&d->d_u, rows * (din ? din : 1)));
+        TRY(dalloc(&d->d_phi, rows * rs));
+        TRY(dalloc(&d->d_nat, rows * n));
+        TRY(dalloc(&d->d_y, rows * (dout ? dout : 1) + 2 * (dout ? dout : 1)));
         TRY(dalloc(&d->d_spkd, n));
         TRY(dalloc(&d->d_ras, rows * d->nwords));
-        if (cudaMallocHost((void **)&d->h_stage, rows * (m->dout ? m->dout : 1) * sizeof(double)) !=
-            cudaSuccess) {
-            d->h_stage = nullptr;
-            rc = SP_EALLOC;
-            goto fail;
-        }
+        TRY(dalloc(&d->d_ras_nat, rows * d->nwords));
+        SP_CK(cudaStreamSynchronize(s));  // host vectors above go out of scope
     }
     default_launch(d);
     TRY(sp_dev_reset_neurons(d, m));
@@ -365,13 +558,11 @@ extern "C" void sp_dev_destroy(sp_dev *d)
     void *bufs[] = {d->V, d->tprev, d->ring, d->cap_pos, d->refr_until, d->rng, d->spk,
                     d->row_ptr, d->col, d->w, d->coef, d->eff, d->trace, d->edge_decay,
                     d->edge_omd, d->edge_trace, d->scoef, d->Iring, d->mx_decay, d->mx_omd,
-                    d->mx_c, d->mx_tr, d->W_in, d->W_out, d->d_u, d->d_phi, d->d_y,
-                    d->d_spkd, d->d_ras, d->bar, d->err};
+                    d->mx_c, d->mx_tr, d->W_in, d->W_out, d->d_u, d->d_phi, d->d_nat, d->d_y,
+                    d->d_spkd, d->d_ras, d->d_ras_nat, d->bar, d->err, d->pos_of, d->nid_of};
     for (void *b : bufs)
         if (b)
             cudaFree(b);
-    if (d->h_stage)
-        cudaFreeHost(d->h_stage);
     if (d->stream)
         cudaStreamDestroy(d->stream);
     free(d);
@@ -387,8 +578,8 @@ extern "C" int sp_dev_reset_neurons(sp_dev *d, const sp_host_model *m)
     SP_CK(cudaMemsetAsync(d->spk, 0, 2 * d->nwords * sizeof(unsigned), d->stream));
     int blocks = d->num_sms * 4;
     k_reset_neurons<<<blocks, 256, 0, d->stream>>>(
-        d->n, d->nc.L, d->ring_elems, d->ntype, d->nc.v_init, d->nc.tprev_init, d->V, d->tprev,
-        d->ring, d->cap_pos, d->refr_until, d->rng, d->seed);
+        d->n, d->nw, d->nc.L, d->ring_elems, d->ntype, d->nc.v_init, d->nc.tprev_init, d->V,
+        d->tprev, d->ring, d->cap_pos, d->refr_until, d->rng, d->nid_of, d->seed);
     SP_CK(cudaGetLastError());
     return SP_OK;
 }
@@ -419,7 +610,6 @@ extern "C" int sp_dev_sync(sp_dev *d)
     return check_err(d);
 }
 
-// Launch one chunk of `T` macro steps. u, phi, raster are device pointers.
 extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double *phi,
                                    unsigned *raster)
 {
@@ -439,6 +629,15 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.warps = l.warps_max;
     p.R = l.variant == 1 ? l.rows : 0;
     p.NST = l.variant == 1 ? l.stages : 0;
+    if (l.variant == 1) {
+        box_geometry(l, &p.BW, &p.NBX);
+        p.RB = p.R < d->nc.L ? p.R : d->nc.L;
+        p.coef_smem = coef_smem_bytes(d) > 0;
+        int rc = encode_ring_map(d, p.BW, p.RB);
+        if (rc)
+            return rc;
+        p.tmap = d->tmap;
+    }
     p.step0 = d->step;
     p.syn_step0 = d->syn_step;
     p.a = d->nc.a; p.b = d->nc.b; p.c = d->nc.c; p.d = d->nc.d; p.e = d->nc.e; p.f = d->nc.f;
@@ -460,6 +659,7 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.W_in = d->W_in; p.gamma = d->gamma; p.u = u;
     p.phi = phi; p.raster = raster;
     p.bar = d->bar; p.err = d->err;
+    p.nid_of = d->nid_of;
 
     kfn_t fn = pick_kernel(d->ntype, d->stype, l.variant);
     if (!fn)
@@ -485,12 +685,24 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     return SP_OK;
 }
 
+
 extern "C" int sp_dev_readout(sp_dev *d, const double *X, size_t T, double *Y)
 {
     if (T == 0 || d->dout == 0)
         return SP_OK;
     dim3 grid((unsigned)T, (unsigned)d->dout);
-    k_readout<<<grid, 256, 0, d->stream>>>(d->W_out, X, d->n, d->dout, Y);
+    k_readout<<<grid, 256, 0, d->stream>>>(d->W_out, X, d->rs, d->dout, Y);
+    SP_CK(cudaGetLastError());
+    return SP_OK;
+}
+
+// position-space rows [T][rs] -> neuron-space rows [T][n]
+extern "C" int sp_dev_gather_rows(sp_dev *d, const double *pos_rows, size_t T, double *nat_rows)
+{
+    if (T == 0)
+        return SP_OK;
+    k_gather_rows<<<gather_blocks(T * d->n), 256, 0, d->stream>>>(pos_rows, d->rs, d->pos_of,
+                                                                   d->n, T, nat_rows);
     SP_CK(cudaGetLastError());
     return SP_OK;
 }
@@ -498,13 +710,13 @@ extern "C" int sp_dev_readout(sp_dev *d, const double *X, size_t T, double *Y)
 extern "C" int sp_dev_run(sp_dev *d, const sp_run_args *a)
 {
     const size_t T = a->T;
-    const size_t n = (size_t)d->n;
+    const size_t n = (size_t)d->n, rs = (size_t)d->rs;
     const bool want_y = (a->h_y || a->d_y) && d->dout > 0;
-    // states are needed on the device for readouts and host copies
-    const bool phi_staged = !a->d_phi && (a->h_phi || want_y);
-    const bool ras_staged = !a->d_raster && a->h_raster;
+    const bool want_phi = a->h_phi || a->d_phi;
+    const bool phi_pos = want_phi || want_y;  // kernel writes states
+    const bool want_ras = a->h_raster || a->d_raster;
     size_t chunk = T;
-    if (!a->u_on_device || phi_staged || ras_staged)
+    if (!a->u_on_device || phi_pos || want_ras)
         chunk = d->chunk;
     if (chunk == 0)
         chunk = 1;
@@ -520,31 +732,42 @@ extern "C" int sp_dev_run(sp_dev *d, const sp_run_args *a)
                 u = d->d_u;
             }
         }
-        double *phi = a->d_phi ? a->d_phi + t0 * n : (phi_staged ? d->d_phi : nullptr);
-        unsigned *ras = a->d_raster ? a->d_raster + t0 * d->nwords
-                                    : (ras_staged ? d->d_ras : nullptr);
-        int rc = sp_dev_launch_chunk(d, u, tc, phi, ras);
+        int rc = sp_dev_launch_chunk(d, u, tc, phi_pos ? d->d_phi : nullptr,
+                                     want_ras ? d->d_ras : nullptr);
         if (rc)
             return rc;
-        if (ras_staged)
-            SP_CK(cudaMemcpyAsync(a->h_raster + t0 * d->nwords, ras,
-                                  tc * d->nwords * sizeof(unsigned), cudaMemcpyDeviceToHost,
-                                  d->stream));
-        if (a->h_phi)
-            SP_CK(cudaMemcpyAsync(a->h_phi + t0 * n, phi, tc * n * sizeof(double),
-                                  cudaMemcpyDeviceToHost, d->stream));
+        if (want_ras) {
+            unsigned *dst = a->d_raster ? a->d_raster + t0 * d->nwords : d->d_ras_nat;
+            k_gather_bits<<<gather_blocks(tc * d->nwords * 32), 256, 0, d->stream>>>(
+                d->d_ras, d->nw, d->pos_of, d->n, tc, dst);
+            SP_CK(cudaGetLastError());
+            if (a->h_raster)
+                SP_CK(cudaMemcpyAsync(a->h_raster + t0 * d->nwords, dst,
+                                      tc * d->nwords * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                      d->stream));
+        }
+        if (want_phi) {
+            double *dst = a->d_phi ? a->d_phi + t0 * n : d->d_nat;
+            rc = sp_dev_gather_rows(d, d->d_phi, tc, dst);
+            if (rc)
+                return rc;
+            if (a->h_phi)
+                SP_CK(cudaMemcpyAsync(a->h_phi + t0 * n, dst, tc * n * sizeof(double),
+                                      cudaMemcpyDeviceToHost, d->stream));
+        }
         if (want_y) {
             double *Y = a->d_y ? a->d_y + t0 * d->dout : d->d_y;
-            rc = sp_dev_readout(d, phi, tc, Y);
+            rc = sp_dev_readout(d, d->d_phi, tc, Y);
             if (rc)
                 return rc;
             if (a->h_y)
                 SP_CK(cudaMemcpyAsync(a->h_y + t0 * d->dout, Y, tc * d->dout * sizeof(double),
                                       cudaMemcpyDeviceToHost, d->stream));
         }
-        if (t0 + tc < T && (!a->u_on_device || phi_staged || ras_staged))
+        if (t0 + tc < T && (!a->u_on_device || phi_pos || want_ras))
             SP_CK(cudaStreamSynchronize(d->stream)); /* staging buffers are reused */
     }
+    (void)rs;
     if (a->sync)
         return sp_dev_sync(d);
     return SP_OK;
@@ -552,22 +775,27 @@ extern "C" int sp_dev_run(sp_dev *d, const sp_run_args *a)
 
 extern "C" int sp_dev_read_state(sp_dev *d, double *h_V)
 {
-    SP_CK(cudaMemcpyAsync(h_V, d->V, (size_t)d->n * sizeof(double), cudaMemcpyDeviceToHost,
+    int rc = sp_dev_gather_rows(d, d->V, 1, d->d_nat);
+    if (rc)
+        return rc;
+    SP_CK(cudaMemcpyAsync(h_V, d->d_nat, (size_t)d->n * sizeof(double), cudaMemcpyDeviceToHost,
                           d->stream));
     return sp_dev_sync(d);
 }
 
 extern "C" int sp_dev_set_state(sp_dev *d, const double *h_V)
 {
-    SP_CK(cudaMemcpyAsync(d->V, h_V, (size_t)d->n * sizeof(double), cudaMemcpyHostToDevice,
+    SP_CK(cudaMemcpyAsync(d->d_nat, h_V, (size_t)d->n * sizeof(double), cudaMemcpyHostToDevice,
                           d->stream));
+    k_scatter_vec<<<gather_blocks(d->rs), 256, 0, d->stream>>>(d->d_nat, d->nid_of, d->rs, d->V);
+    SP_CK(cudaGetLastError());
     return sp_dev_sync(d);
 }
 
 extern "C" int sp_dev_read_spikes(sp_dev *d, double *h_spk)
 {
-    k_spikes_to_double<<<(d->n + 255) / 256, 256, 0, d->stream>>>(
-        d->spk + (size_t)d->phase * d->nwords, d->n, d->d_spkd);
+    k_bits_to_double<<<gather_blocks(d->n), 256, 0, d->stream>>>(
+        d->spk + (size_t)d->phase * d->nwords, d->pos_of, d->n, d->d_spkd);
     SP_CK(cudaGetLastError());
     SP_CK(cudaMemcpyAsync(h_spk, d->d_spkd, (size_t)d->n * sizeof(double),
                           cudaMemcpyDeviceToHost, d->stream));
@@ -586,18 +814,47 @@ extern "C" int sp_dev_compute_output(sp_dev *d, double *h_y)
     return sp_dev_sync(d);
 }
 
+// W_out (dout x n, neuron order) in device memory -> position-space copy
+extern "C" int sp_dev_w_out_from_nat(sp_dev *d, const double *dev_w_nat)
+{
+    k_wout_to_pos<<<gather_blocks((size_t)d->dout * d->rs), 256, 0, d->stream>>>(
+        dev_w_nat, d->nid_of, d->n, d->rs, d->dout, d->W_out);
+    SP_CK(cudaGetLastError());
+    return SP_OK;
+}
+
+// position-space W_out -> neuron order (dout x n) in device memory
+extern "C" int sp_dev_w_out_to_nat(sp_dev *d, double *dev_w_nat)
+{
+    k_gather_rows<<<gather_blocks((size_t)d->dout * d->n), 256, 0, d->stream>>>(
+        d->W_out, d->rs, d->pos_of, d->n, (size_t)d->dout, dev_w_nat);
+    SP_CK(cudaGetLastError());
+    return SP_OK;
+}
+
 extern "C" int sp_dev_upload_w_out(sp_dev *d, const double *h_W_out)
 {
-    SP_CK(cudaMemcpyAsync(d->W_out, h_W_out, (size_t)d->n * d->dout * sizeof(double),
-                          cudaMemcpyHostToDevice, d->stream));
-    return sp_dev_sync(d);
+    double *tmp = nullptr;
+    SP_CK(cudaMalloc(&tmp, (size_t)d->n * d->dout * sizeof(double) + 8));
+    cudaMemcpyAsync(tmp, h_W_out, (size_t)d->n * d->dout * sizeof(double),
+                    cudaMemcpyHostToDevice, d->stream);
+    int rc = sp_dev_w_out_from_nat(d, tmp);
+    cudaStreamSynchronize(d->stream);
+    cudaFree(tmp);
+    return rc ? rc : sp_dev_sync(d);
 }
 
 extern "C" int sp_dev_download_w_out(sp_dev *d, double *h_W_out)
 {
-    SP_CK(cudaMemcpyAsync(h_W_out, d->W_out, (size_t)d->n * d->dout * sizeof(double),
-                          cudaMemcpyDeviceToHost, d->stream));
-    return sp_dev_sync(d);
+    double *tmp = nullptr;
+    SP_CK(cudaMalloc(&tmp, (size_t)d->n * d->dout * sizeof(double) + 8));
+    int rc = sp_dev_w_out_to_nat(d, tmp);
+    if (!rc)
+        cudaMemcpyAsync(h_W_out, tmp, (size_t)d->n * d->dout * sizeof(double),
+                        cudaMemcpyDeviceToHost, d->stream);
+    cudaStreamSynchronize(d->stream);
+    cudaFree(tmp);
+    return rc ? rc : sp_dev_sync(d);
 }
 
 extern "C" void *sp_dev_stream(sp_dev *d) { return (void *)d->stream; }
@@ -615,9 +872,13 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
     if ((long long)l->ctas * l->warps_max < (long long)d->nwords)
         return SP_EINVAL;
     if (l->variant == 1) {
-        if (d->ntype != SP_FLIF_GL || l->warps_max > 31 || l->rows < 1 || l->stages < 2 ||
-            l->rows > 64)
+        if (d->ntype != SP_FLIF_GL || l->warps_max > 16 || l->rows < 1 || l->stages < 2 ||
+            l->rows > 256)
             return SP_EINVAL;
+        int bw, nbx;
+        box_geometry(*l, &bw, &nbx);
+        if (encode_ring_map(d, bw, l->rows < d->nc.L ? l->rows : d->nc.L) != SP_OK)
+            return SP_EINTERNAL;
     } else if (l->variant != 0) {
         return SP_EINVAL;
     }

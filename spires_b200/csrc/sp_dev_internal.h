@@ -11,6 +11,7 @@
 //   eff[2][n]                        per-neuron synaptic drive (non-SIMPLE)
 //   Iring[Ls][n] (FRACTIONAL)        time-major fractional-current ring
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "sp_dev.h"
 
@@ -18,7 +19,8 @@ struct sp_dev {
     int device, num_sms, coop;
     cudaStream_t stream;
     int n, din, dout, micro;
-    int rs;              // FLIF_GL ring row stride (n rounded up to 32)
+    int nw;              // warps of neurons = ceil(n / 32)
+    int rs;              // positions = 32 * nw (device arrays are in position order)
     size_t ring_elems;
     size_t nwords, nnz;
     double dt, gamma;
@@ -43,21 +45,32 @@ struct sp_dev {
     double *eff, *trace, *edge_decay, *edge_omd, *edge_trace;
     double *scoef, *Iring;
     double *mx_decay, *mx_omd, *mx_c, *mx_tr;
-    double *W_in, *W_out;
+    double *W_in, *W_out;  // rows / columns in position order
+    int *pos_of;           // [n] position of neuron i
+    int *nid_of;           // [rs] neuron at position q, or -1
 
     // staging for host-driven runs
     size_t chunk;        // macro steps per chunk
     double *d_u;         // [chunk][din]
-    double *d_phi;       // [chunk][n]
+    double *d_phi;       // [chunk][rs] position-space states
+    double *d_nat;       // [chunk][n] neuron-order states
     double *d_y;         // [chunk][dout]
-    unsigned *d_ras;     // [chunk][nw]
+    unsigned *d_ras;     // [chunk][nw] position-space spike words
+    unsigned *d_ras_nat; // [chunk][nw] neuron-order spike words
     double *d_spkd;      // [n]
     double *h_stage;     // pinned [chunk][dout]
     unsigned *bar;
     int *err;
+
+    // 2-D tiled tensor map over the FLIF_GL ring (variant 1), box BW x R
+    CUtensorMap tmap;
+    int tmap_bw, tmap_r;
 };
 
 extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double *phi,
                                    unsigned *raster);
 extern "C" int sp_dev_readout(sp_dev *d, const double *X, size_t T, double *Y);
 extern "C" void sp_dev_note_error(const char *what, int code);
+extern "C" int sp_dev_gather_rows(sp_dev *d, const double *pos_rows, size_t T, double *nat_rows);
+extern "C" int sp_dev_w_out_from_nat(sp_dev *d, const double *dev_w_nat);
+extern "C" int sp_dev_w_out_to_nat(sp_dev *d, double *dev_w_nat);

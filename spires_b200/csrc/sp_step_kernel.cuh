@@ -24,6 +24,7 @@
 //   neuron update, ring write, ballot -> spike word of step g
 //   synapse prepare for g+1 (own spike), publish, arrive barrier g+1
 #pragma once
+#include <cuda.h>
 #include "sp_kernels.cuh"
 #include "sp_model.h"
 
@@ -34,6 +35,10 @@ struct KP {
     int rs;         // ring row stride in doubles (multiple of 32)
     int warps;      // consumer warps per CTA
     int R, NST;     // variant 1: ring rows per stage, stages
+    int BW, NBX;    // variant 1: box width (neurons) and boxes side by side per stage
+    int RB;         // variant 1: rows per box = min(R, L)
+    int coef_smem;  // variant 1: coefficient table staged in shared memory
+    const int *nid_of;  // neuron at each position, -1 for an empty lane
     long long step0, syn_step0;
     double a, b, c, d, e, f, g, h, ci, cj, ck, cl, dt;
     int L, det_refr, diff_sto;
@@ -65,6 +70,9 @@ struct KP {
     unsigned *raster;
     unsigned *bar;
     int *err;
+    // variant 1: 2-D tiled map of the ring [L rows][rs columns] of doubles,
+    // box = BW columns x R rows
+    alignas(64) CUtensorMap tmap;
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -102,14 +110,23 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned b
                  "r"(bytes)
                  : "memory");
 }
-// 1-D bulk copy global -> shared (16-byte aligned addresses, size % 16 == 0),
-// completion counted on the mbarrier. No multicast.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
-                                         unsigned long long *bar)
+// read-only load that does not allocate in L1 (per-step input weights must not
+// evict the coefficient table and the CSR slice)
+__device__ __forceinline__ double ldg_na(const double *ptr)
+{
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(ptr));
+    return v;
+}
+
+// 2-D tiled bulk-tensor load of one box at (x = column, y = row); no multicast.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            unsigned long long *bar)
 {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
 __device__ __forceinline__ void st_release_cta(volatile int *ptr, int v)
@@ -169,16 +186,23 @@ __device__ __forceinline__ double rowpass_simple_warp(const long long *__restric
     const long long e1 = __ldg(row_ptr + row0 + nv);
     const long long my_end = (lane < nv) ? __ldg(row_ptr + row0 + lane + 1) : e1;
     double acc = 0.0;
+    // next chunk's column index and weight are loaded one chunk ahead
+    int cn = -1;
+    double wn = 0.0;
+    if (e0 + lane < e1) {
+        cn = __ldg(col + e0 + lane);
+        wn = __ldg(w + e0 + lane);
+    }
     for (long long base = e0; base < e1; base += 32) {
-        const long long e = base + lane;
-        bool s = false;
-        double wv = 0.0;
-        if (e < e1) {
-            const int c = __ldg(col + e);
-            s = (s_spk[c >> 5] >> (c & 31)) & 1u;
-            if (s)
-                wv = __ldg(w + e);
+        const int c = cn;
+        const double wv = wn;
+        const long long nx = base + 32 + lane;
+        cn = -1;
+        if (nx < e1) {
+            cn = __ldg(col + nx);
+            wn = __ldg(w + nx);
         }
+        const bool s = c >= 0 && ((s_spk[c >> 5] >> (c & 31)) & 1u);
         unsigned m = __ballot_sync(kFull, s);
         while (m) {
             const int bpos = __ffs(m) - 1;
@@ -193,8 +217,31 @@ __device__ __forceinline__ double rowpass_simple_warp(const long long *__restric
     return acc;
 }
 
+template <int R>
+__device__ __forceinline__ double stage_sum(double hist, const double *coef_k, const double *buf,
+                                            int bw)
+{
+    double c[R], v[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        c[j] = coef_k[j];
+        v[j] = buf[(size_t)(R - 1 - j) * bw];
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j)
+        hist = add(hist, mul(c[j], v[j]));
+    return hist;
+}
+
+// Variant 1 runs at most 16 consumer warps + 1 producer warp per CTA, which
+// leaves registers for a whole stage of lags in flight per thread.
+template <int VAR>
+struct Bounds {
+    static constexpr int threads = VAR == 1 ? 544 : 1024;
+};
+
 template <int NT, int ST, int VAR>
-__global__ void __launch_bounds__(1024, 1) k_run(KP p)
+__global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_constant__ KP p)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_flag;
@@ -207,16 +254,17 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
     const int NC = 32 * p.warps;  // consumer threads
     const int wb0 = (int)(((long long)blockIdx.x * p.nwords) / p.G);
     const int wb1 = (int)(((long long)(blockIdx.x + 1) * p.nwords) / p.G);
-    const int n = p.n;
     const int L = p.L;
     const long long B = (long long)p.n_macro * p.micro;
 
     unsigned *s_spk = (unsigned *)smem;
     const size_t spk_bytes = (((size_t)p.nwords * 4) + 127) & ~(size_t)127;
-    double *s_stage = (double *)(smem + spk_bytes);
-    const int SW = NC;  // stage row pitch (doubles)
-    unsigned long long *full =
-        (unsigned long long *)(smem + spk_bytes + (size_t)p.NST * p.R * SW * sizeof(double));
+    const size_t coef_bytes = p.coef_smem ? (((size_t)L * 8) + 127) & ~(size_t)127 : 0;
+    double *s_coef = (double *)(smem + spk_bytes);
+    double *s_stage = (double *)(smem + spk_bytes + coef_bytes);
+    const size_t STAGE = (size_t)p.NBX * p.R * p.BW;  // doubles per stage
+    unsigned long long *full = (unsigned long long *)(smem + spk_bytes + coef_bytes +
+                                                      (size_t)p.NST * STAGE * sizeof(double));
     unsigned long long *empty = full + p.NST;
     const int lo = wb0 * 32;
     const int S_b = 32 * (wb1 - wb0);
@@ -225,6 +273,9 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
         s_abort = 0;
         s_done = 0;
     }
+    if (VAR == 1 && p.coef_smem)
+        for (int k = tid; k < L; k += blockDim.x)
+            s_coef[k] = p.coef[k];
     if (VAR == 1) {
         if (tid == 0) {
             for (int s = 0; s < p.NST; ++s) {
@@ -241,7 +292,10 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
         if (lane != 0 || S_b == 0)
             return;
         long long q = 0;  // stages issued
+        int st = 0;       // q % NST
+        long long rounds = 0;  // q / NST
         bool ok = true;
+        const int nbox = (S_b + p.BW - 1) / p.BW;
         for (long long b = 0; b < B && ok; ++b) {
             const long long g = p.step0 + b;
             const int lim = (int)(g < L ? g : L - 1);
@@ -269,30 +323,43 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
                 if (!ok)
                     break;
             }
-            for (int k = 2; k <= lim && ok; k += p.R) {
-                const int cnt = (lim - k + 1 < p.R) ? lim - k + 1 : p.R;
-                const int st = (int)(q % p.NST);
-                const long long u = q / p.NST;
-                if (u > 0 && !mbar_wait(&empty[st], (unsigned)((u - 1) & 1), &s_abort, p.err)) {
+            // lags k..k+cnt-1 are rows rh down to rh-cnt+1: one contiguous
+            // ascending row range per stage (split at the wrap)
+            int rh = (int)(g % L) - 2;
+            if (rh < 0)
+                rh += L;
+            for (int k = 2; k <= lim && ok;) {
+                int cnt = lim - k + 1;
+                if (cnt > p.R)
+                    cnt = p.R;
+                if (cnt > rh + 1)
+                    cnt = rh + 1;
+                const int y0 = rh - cnt + 1;
+                if (rounds > 0 &&
+                    !mbar_wait(&empty[st], (unsigned)((rounds - 1) & 1), &s_abort, p.err)) {
                     ok = false;
                     break;
                 }
-                mbar_expect_tx(&full[st], (unsigned)(cnt * S_b * 8));
-                double *dst = s_stage + (size_t)st * p.R * SW;
-                for (int j = 0; j < cnt; ++j) {
-                    long long r = (g - k - j) % L;
-                    if (r < 0)
-                        r += L;
-                    bulk_g2s(dst + (size_t)j * SW, p.ring + (size_t)r * p.rs + lo,
-                             (unsigned)(S_b * 8), &full[st]);
-                }
+                mbar_expect_tx(&full[st], (unsigned)(nbox * p.RB * p.BW * 8));
+                double *dst = s_stage + (size_t)st * STAGE;
+                for (int c = 0; c < nbox; ++c)
+                    tma_load_2d(dst + (size_t)c * p.R * p.BW, &p.tmap, lo + c * p.BW, y0,
+                                &full[st]);
                 ++q;
+                if (++st == p.NST) {
+                    st = 0;
+                    ++rounds;
+                }
+                k += cnt;
+                rh -= cnt;
+                if (rh < 0)
+                    rh += L;
             }
         }
         // every issued copy must land before the CTA may exit
+        const unsigned long long t0 = globaltimer_ns();
         for (long long qq = (q > p.NST ? q - p.NST : 0); qq < q; ++qq) {
             const int st = (int)(qq % p.NST);
-            unsigned long long t0 = globaltimer_ns();
             while (!mbar_test(&full[st], (unsigned)((qq / p.NST) & 1))) {
                 if (globaltimer_ns() - t0 > kBarrierTimeoutNs)
                     break;
@@ -305,7 +372,7 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
     const int gw = wb0 + warp;
     const bool wact = gw < wb1;
     const int i = gw * 32 + lane;
-    const bool act = wact && i < n;
+    const bool act = wact && __ldg(p.nid_of + i) >= 0;
 
     double V = act ? p.V[i] : 0.0;
     double tprev = 0.0, vlast = 0.0;
@@ -334,14 +401,14 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
         long long pr = (p.syn_step0 - 1) % p.Ls;
         if (pr < 0)
             pr += p.Ls;
-        Ilast = p.Iring[(size_t)pr * n + i];
+        Ilast = p.Iring[(size_t)pr * p.rs + i];
     }
     int cur = p.phase0;
     double sprev = 0.0;
     if (act)
         sprev = ((p.spk[cur * p.nwords + gw] >> lane) & 1u) ? 1.0 : 0.0;
     unsigned lastword = 0;
-    long long q = 0;  // stages consumed (variant 1)
+    int cst = 0, cph = 0;  // variant 1: stage consumed next and its phase parity
     double ext = 0.0;
 
     // synapse prepare for the own neuron before micro-step b (src/synapse.c:145-160)
@@ -350,7 +417,7 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
             return;
         if (ST == SP_SYN_PSC_HOM) {
             ptrace = add(mul(ptrace, p.psc_decay), mul(p.psc_omd, sprev));
-            p.eff[(size_t)buf * n + i] = ptrace;
+            p.eff[(size_t)buf * p.rs + i] = ptrace;
         } else if (ST == SP_SYN_FRAC) {
             const long long gs = p.syn_step0 + b;
             const int Ls = p.Ls;
@@ -363,23 +430,23 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
             if (r < 0)
                 r += Ls;
             for (int k = 2; k <= lim; ++k) {
-                hist = add(hist, mul(__ldg(p.scoef + k), __ldcg(p.Iring + (size_t)r * n + i)));
+                hist = add(hist, mul(__ldg(p.scoef + k), __ldcg(p.Iring + (size_t)r * p.rs + i)));
                 r = (r == 0) ? Ls - 1 : r - 1;
             }
             const double rhs = dvd(add(-Ilast, sprev), p.s_tau);
             const double In = sub(mul(p.s_dta, rhs), hist);
-            p.Iring[(size_t)head * n + i] = In;
+            p.Iring[(size_t)head * p.rs + i] = In;
             Ilast = In;
-            p.eff[(size_t)buf * n + i] = In;
+            p.eff[(size_t)buf * p.rs + i] = In;
         } else if (ST == SP_SYN_FRAC_MEXP) {
             double sum = 0.0;
             for (int c = 0; c < p.Nc; ++c) {
-                double tr = p.mx_tr[(size_t)c * n + i];
+                double tr = p.mx_tr[(size_t)c * p.rs + i];
                 tr = add(mul(tr, __ldg(p.mx_decay + c)), mul(__ldg(p.mx_omd + c), sprev));
-                p.mx_tr[(size_t)c * n + i] = tr;
+                p.mx_tr[(size_t)c * p.rs + i] = tr;
                 sum = add(sum, mul(__ldg(p.mx_c + c), tr));
             }
-            p.eff[(size_t)buf * n + i] = sum;
+            p.eff[(size_t)buf * p.rs + i] = sum;
         }
     };
 
@@ -445,7 +512,7 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
                 const double *wr = p.W_in + (size_t)i * p.din;
                 double t = 0.0;
                 for (int j = 0; j < p.din; ++j)
-                    t = add(t, mul(__ldg(wr + j), __ldg(ur + j)));
+                    t = add(t, mul(ldg_na(wr + j), ldg_na(ur + j)));
                 ext = add(0.0, mul(p.gamma, t));
             }
         }
@@ -473,29 +540,43 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
                     }
                 }
             } else {
-                const int j = tid;
-                for (int k = 2; k <= lim && S_b > 0; k += p.R) {
-                    const int cnt = (lim - k + 1 < p.R) ? lim - k + 1 : p.R;
-                    const int st = (int)(q % p.NST);
+                const int boff = (tid / p.BW) * p.R * p.BW + (tid % p.BW);
+                const double *cf = p.coef_smem ? s_coef : p.coef;
+                int rh = head - 2;
+                if (rh < 0)
+                    rh += L;
+                for (int k = 2; k <= lim && S_b > 0;) {
+                    int cnt = lim - k + 1;
+                    if (cnt > p.R)
+                        cnt = p.R;
+                    if (cnt > rh + 1)
+                        cnt = rh + 1;
                     // on a failed wait the launch aborts at the next barrier_wait;
                     // every consumer keeps the same control flow until then
-                    const bool landed =
-                        mbar_wait(&full[st], (unsigned)((q / p.NST) & 1), &s_abort, p.err);
-                    const double *buf = s_stage + (size_t)st * p.R * SW + j;
+                    const bool landed = mbar_wait(&full[cst], (unsigned)cph, &s_abort, p.err);
+                    const double *buf = s_stage + (size_t)cst * STAGE + boff;
                     if (landed && act && integ) {
                         if (cnt == 16) {
-#pragma unroll
-                            for (int jr = 0; jr < 16; ++jr)
-                                hist = add(hist, mul(__ldg(p.coef + k + jr), buf[(size_t)jr * SW]));
+                            hist = stage_sum<16>(hist, cf + k, buf, p.BW);
+                        } else if (cnt == 8) {
+                            hist = stage_sum<8>(hist, cf + k, buf, p.BW);
                         } else {
                             for (int jr = 0; jr < cnt; ++jr)
-                                hist = add(hist, mul(__ldg(p.coef + k + jr), buf[(size_t)jr * SW]));
+                                hist = add(hist, mul(cf[k + jr],
+                                                     buf[(size_t)(cnt - 1 - jr) * p.BW]));
                         }
                     }
                     __syncwarp();
                     if (lane == 0)
-                        mbar_arrive(&empty[st]);
-                    ++q;
+                        mbar_arrive(&empty[cst]);
+                    if (++cst == p.NST) {
+                        cst = 0;
+                        cph ^= 1;
+                    }
+                    k += cnt;
+                    rh -= cnt;
+                    if (rh < 0)
+                        rh += L;
                 }
             }
         }
@@ -513,9 +594,8 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
         double rec = 0.0;
         if (ST == SP_SYN_SIMPLE) {
             if (wact) {
-                const int row0 = gw * 32;
-                const int nv = (n - row0 < 32) ? n - row0 : 32;
-                rec = rowpass_simple_warp(p.row_ptr, p.col, p.w, s_spk, row0, nv, lane);
+                // CSR rows are in position order; holes are empty rows
+                rec = rowpass_simple_warp(p.row_ptr, p.col, p.w, s_spk, gw * 32, 32, lane);
             }
         } else if (act) {
             const long long k0 = __ldg(p.row_ptr + i), k1 = __ldg(p.row_ptr + i + 1);
@@ -529,7 +609,7 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
                     rec = add(rec, mul(__ldg(p.w + k), tr));
                 }
             } else {
-                const double *ef = p.eff + (size_t)cur * n;
+                const double *ef = p.eff + (size_t)cur * p.rs;
                 for (long long k = k0; k < k1; ++k) {
                     const int c = __ldg(p.col + k);
                     rec = add(rec, mul(__ldg(p.w + k), __ldcg(ef + c)));
@@ -639,7 +719,7 @@ __global__ void __launch_bounds__(1024, 1) k_run(KP p)
         sprev = fired ? 1.0 : 0.0;
         if (m == p.micro - 1) {
             if (act && p.phi)
-                p.phi[(size_t)s * n + i] = V;
+                p.phi[(size_t)s * p.rs + i] = V;
             if (wact && lane == 0 && p.raster)
                 p.raster[(size_t)s * p.nwords + gw] = lastword;
         }

@@ -187,7 +187,9 @@ GL_L = lambda L: (1.0, 0.0, 0.0, 20.0, 0.7, float(L), 0.1, 2.0)
 @pytest.mark.parametrize("shape", [dict(ctas=1, warps_max=8, rows=16, stages=2),
                                    dict(ctas=4, warps_max=2, rows=3, stages=3),
                                    dict(ctas=8, warps_max=1, rows=1, stages=4),
-                                   dict(ctas=2, warps_max=4, rows=16, stages=8)])
+                                   dict(ctas=2, warps_max=4, rows=16, stages=8),
+                                   dict(ctas=4, warps_max=2, rows=8, stages=5),
+                                   dict(ctas=1, warps_max=8, rows=32, stages=2)])
 def test_flif_gl_bulk_copy_pipeline(L, shape):
     """The bulk-copy ring pipeline (variant 1) gives the bits of the oracle for
     ring lengths shorter and longer than its depth, during ramp-up (step < L)
