@@ -334,6 +334,28 @@ def run_gpu_arm(args, rank, world):
     return line
 
 
+def run_profile_case(args):
+    """The bench reservoir, 1032 fill steps in one launch, then exactly one
+    launch of args.chunk steps: the launch an ncu capture with -s 1 -c 1 sees."""
+    import torch
+
+    import spires_b200 as sp
+
+    lib = sp.load()
+    r = sp.Reservoir(workload_config(sp), seed=SEED)
+    if args.variant >= 0:
+        assert r.set_launch(variant=args.variant) == sp.SPIRES_OK
+    fill = L_HIST + 8
+    u = torch.from_numpy(input_stream(fill + args.chunk)).cuda()
+    torch.cuda.synchronize()
+    assert lib.spires_ext_run_device(r.h, C.c_void_p(u.data_ptr()), fill, None, None, None) == 0
+    assert lib.spires_ext_run_device(r.h, C.c_void_p(u.data_ptr() + fill * DIN * 8), args.chunk,
+                                     None, None, None) == 0
+    assert lib.spires_ext_sync(r.h) == 0
+    r.close()
+    print("profile case done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,6 +368,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="force step-kernel variant")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="fill the ring, then one launch of --chunk steps (for ncu -s 1 -c 1)")
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
     args = ap.parse_args()
@@ -357,6 +381,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference_arm(args)
+        return
+    if args.profile_case:
+        run_profile_case(args)
         return
 
     if world > 1:

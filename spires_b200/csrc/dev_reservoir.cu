@@ -335,7 +335,7 @@ static void default_launch(sp_dev *d)
     if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 16) {
         sp_launch v = l;
         v.variant = 1;
-        v.rows = 16;
+        v.rows = 32;
         int bw, nbx;
         box_geometry(v, &bw, &nbx);
         const size_t stage = (size_t)v.rows * nbx * bw * sizeof(double);
