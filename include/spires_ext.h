@@ -117,6 +117,29 @@ spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_se
                                      double lambda, const spires_ext_ridge_opts *opts,
                                      spires_ext_ridge_report *report);
 
+/* ---- ridge readout without device allocation -----------------------------
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory themselves -- a host framework that owns every device buffer through
+ * its own allocator or quota, or a control loop that cannot afford the
+ * implicit device-wide synchronisation of cudaMalloc/cudaFree -- this solves
+ * W_out = (X^T X + lambda I)^-1 X^T Y for states X = d_states[T][n] (rows
+ * washout..T-1 used) and targets Y = d_targets[T][dout], both already in
+ * device memory, and writes d_w_out[dout][n] (the spires_read_readout
+ * layout). FP64 Gram, Cholesky and iterative refinement: the same kernels, in
+ * the same order, as spires_ext_train_ridge with SPIRES_EXT_GRAM_FP64.
+ * It calls no cudaMalloc/cudaFree: its working memory is one fixed array of
+ * this library (8.6 MB, held on every GPU that loads the library until the
+ * process exits), which bounds the sizes: n <= 512, dout <= 16, T <= 16384;
+ * larger requests return SPIRES_ERR_INVALID_ARG. The first call on a device
+ * looks up the array's device address, so make that first call before any
+ * stream capture. Every call shares the one array, so calls that overlap on
+ * the GPU (other streams, other host threads) race; serialise them. `stream`
+ * is a cudaStream_t (NULL = default stream); the call returns after the work
+ * on that stream has finished. */
+spires_status spires_ext_ridge_solve_noalloc(const double *d_states, const double *d_targets,
+                                             size_t T, size_t n, size_t dout, size_t washout,
+                                             double lambda, double *d_w_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

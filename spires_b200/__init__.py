@@ -144,6 +144,8 @@ EXT_SIGNATURES = {
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),
     "spires_ext_train_ridge": (C.c_int, [_VP, _dp, _dp, C.c_size_t, C.c_double,
                                          C.POINTER(RidgeOpts), C.POINTER(RidgeReport)]),
+    "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
+                                                 C.c_size_t, C.c_double, _VP, _VP]),
 }
 
 _lib = None

@@ -877,3 +877,126 @@ out:
         cudaFree(Wn);
     return rc;
 }
+
+// ---------------------------------------------------- allocation-free solve
+// Ridge readout from states the caller already holds in device memory, for
+// callers that cannot allocate device memory themselves: a host framework
+// that owns every device buffer through its own allocator or quota, or a
+// control loop that cannot afford the implicit device-wide synchronisation of
+// cudaMalloc/cudaFree. All working memory is the file-scope array below,
+// sized for at most SP_NA_MAX_N neurons, SP_NA_MAX_DOUT outputs and
+// SP_NA_MAX_T rows (8.6 MB); every GPU that loads this library holds it until
+// the process exits. The same kernels as spires_ext_train_ridge with the FP64
+// Gram run in the same order, so the two agree given the same states.
+#define SP_NA_MAX_N 512
+#define SP_NA_MAX_DOUT 16
+#define SP_NA_MAX_T 16384
+#define SP_NA_PARTS 64
+#define SP_NA_DOUBLES                                                                  \
+    ((size_t)SP_NA_MAX_N * SP_NA_MAX_N + 3 * (size_t)SP_NA_MAX_N * SP_NA_MAX_DOUT +    \
+     (size_t)SP_NA_MAX_T * SP_NA_MAX_DOUT +                                            \
+     (size_t)SP_NA_PARTS * SP_NA_MAX_N * SP_NA_MAX_DOUT + 8)
+
+static __device__ __align__(256) double g_na_scratch[SP_NA_DOUBLES];
+static __device__ __align__(256) int g_na_iscratch[SP_NA_MAX_N + 8];
+
+// Device addresses of the two arrays, looked up once per device (with that
+// device current) on the first call made on it.
+static double *g_na_dptr[64];
+static int *g_na_iptr[64];
+
+static int na_setup(int dev)
+{
+    if (dev < 0 || dev >= 64)
+        return SP_EINTERNAL;
+    if (g_na_dptr[dev] && g_na_iptr[dev])
+        return SP_OK;
+    void *pd = nullptr, *pi = nullptr;
+    if (cudaGetSymbolAddress(&pd, g_na_scratch) != cudaSuccess || !pd)
+        return SP_EINTERNAL;
+    if (cudaGetSymbolAddress(&pi, g_na_iscratch) != cudaSuccess || !pi)
+        return SP_EINTERNAL;
+    g_na_dptr[dev] = (double *)pd;
+    g_na_iptr[dev] = (int *)pi;
+    return SP_OK;
+}
+
+extern "C" __attribute__((visibility("default"))) int
+spires_ext_ridge_solve_noalloc(const double *d_states, const double *d_targets, size_t T,
+                               size_t n_, size_t dout_, size_t washout, double lambda,
+                               double *d_w_out, void *stream)
+{
+    if (!d_states || !d_targets || !d_w_out || T == 0 || n_ == 0 || dout_ == 0 || washout >= T)
+        return SP_EINVAL;
+    if (n_ > SP_NA_MAX_N || dout_ > SP_NA_MAX_DOUT || T > SP_NA_MAX_T) {
+        fprintf(stderr,
+                "spires_ext_ridge_solve_noalloc: size beyond the fixed work area "
+                "(N=%zu > %d, outputs=%zu > %d or rows=%zu > %d)\n",
+                n_, SP_NA_MAX_N, dout_, SP_NA_MAX_DOUT, T, SP_NA_MAX_T);
+        return SP_EINVAL;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return SP_EINTERNAL;
+    int rc = na_setup(dev);
+    if (rc)
+        return rc;
+    const int n = (int)n_, dout = (int)dout_;
+    cudaStream_t s = (cudaStream_t)stream;
+    double *A = g_na_dptr[dev];
+    double *B = A + (size_t)SP_NA_MAX_N * SP_NA_MAX_N;
+    double *W = B + (size_t)SP_NA_MAX_N * SP_NA_MAX_DOUT;
+    double *R = W + (size_t)SP_NA_MAX_N * SP_NA_MAX_DOUT;
+    double *E = R + (size_t)SP_NA_MAX_N * SP_NA_MAX_DOUT;
+    double *part = E + (size_t)SP_NA_MAX_T * SP_NA_MAX_DOUT;
+    double *tmp = part + (size_t)SP_NA_PARTS * SP_NA_MAX_N * SP_NA_MAX_DOUT;
+    int *info = g_na_iptr[dev];
+    int *piv = info + 8;
+    const int parts = SP_NA_PARTS;
+    const size_t tot = (size_t)n * dout;
+    const int maxit = 30;
+    const double tol = 1e-13;
+
+    // the work area keeps the previous call's contents: clear the flag that
+    // must start at zero; every other region is fully rewritten below
+    if (cudaMemsetAsync(info, 0, sizeof(int), s) != cudaSuccess)
+        return SP_EINTERNAL;
+    const int nt = (n + 63) / 64;
+    k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(d_states, n, washout, T, A, n);
+    {
+        dim3 g((n + 127) / 128, parts);
+        k_xt_e_part<<<g, 128, 0, s>>>(d_states, n, washout, T, d_targets, dout, parts, part);
+        k_reduce_parts<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, parts, n, dout,
+                                                                     nullptr, 0.0, B);
+    }
+    k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, lambda);
+    if (cudaMemcpyAsync(W, B, tot * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return SP_EINTERNAL;
+    int bad = cholesky_inplace(s, A, n, info);
+    bool lu = false;
+    if (bad) {
+        lu = true;
+        cudaMemsetAsync(info, 0, sizeof(int), s);
+        k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(d_states, n, washout, T, A, n);
+        k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, lambda);
+        if (lu_factor_solve(s, A, n, piv, info, W, dout) != 0) {
+            fprintf(stderr, "Warning: Ridge regression failed (singular system).\n");
+            return cudaStreamSynchronize(s) == cudaSuccess ? SP_OK : SP_EINTERNAL;
+        }
+    } else {
+        chol_solve(s, A, n, W, dout);
+    }
+    const double bnorm = device_norm(s, B, tot, tmp);
+    for (int it = 0;; ++it) {
+        ridge_residual(s, d_states, n, washout, T, d_targets, W, dout, lambda, E, part, parts, R);
+        const double rel = device_norm(s, R, tot, tmp) / (bnorm > 0 ? bnorm : 1.0);
+        if (rel <= tol || it >= (lu ? 0 : maxit))
+            break;
+        chol_solve(s, A, n, R, dout);
+        k_axpy<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, R, tot);
+    }
+    k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, d_w_out);
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+        return SP_EINTERNAL;
+    return SP_OK;
+}
