@@ -117,6 +117,34 @@ spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_se
                                      double lambda, const spires_ext_ridge_opts *opts,
                                      spires_ext_ridge_report *report);
 
+/* ---- AGILE search core ----------------------------------------------------
+ * The black-box optimiser behind spires_optimize (reference src/agile.h:21-91,
+ * same option and report layouts): Levy-step exploration with SPSA gradients,
+ * then SPSA gradient-descent refinement, minimising loss(theta) within
+ * [lower, upper]. Exposed so callers can tune their own objectives. */
+typedef struct {
+    double   mu, eta_min, eta_max, patience0, patience_decay;
+    double   refine_step;
+    int      refine_max_iters, refine_no_improve;
+    double   spsa_eps;
+    int      reflect_at_bounds;
+    uint64_t seed;
+    int      verbose;
+} spires_ext_agile_opts;
+
+typedef struct {
+    double best_loss;
+    int    best_iter, total_evals, total_iters, exited_refinement;
+} spires_ext_agile_report;
+
+typedef double (*spires_ext_loss_fn)(const double *theta, int dim, void *ctx);
+
+spires_status spires_ext_agile_minimize(const double *theta0, const double *lower,
+                                        const double *upper, int dim,
+                                        spires_ext_loss_fn loss, void *ctx,
+                                        const spires_ext_agile_opts *opts, double *theta_best,
+                                        spires_ext_agile_report *report);
+
 /* ---- ridge readout without device allocation -----------------------------
  * No counterpart in the reference. For callers that cannot allocate device
  * memory themselves -- a host framework that owns every device buffer through

@@ -588,3 +588,81 @@ int orc_ridge(const double *X, const double *Y, size_t T, size_t w0, int n, int 
     free(piv);
     return rc;
 }
+
+/* train_output_iteratively, src/reservoir.c:244-280: prediction by the
+ * sequential readout, then W_out row o += (lr * error_o) * state. */
+void orc_train_online(orc_state *s, const double *target, double lr, double *w_out)
+{
+    const int n = s->m.n, dout = s->m.dout;
+    for (int o = 0; o < dout; o++) {
+        double t = 0.0;
+        for (int i = 0; i < n; i++)
+            t = t + w_out[(size_t)o * n + i] * s->V[i];
+        double pred = 0.0 + 1.0 * t;
+        double a = lr * (target[o] - pred);
+        for (int i = 0; i < n; i++)
+            w_out[(size_t)o * n + i] = w_out[(size_t)o * n + i] + a * s->V[i];
+    }
+}
+
+/* train_output_rls, src/reservoir.c:681-767 (netlib-order BLAS steps). */
+int orc_train_rls(orc_state *s, const double *u, const double *y, size_t T, double delta,
+                  double lambda, double *w_out)
+{
+    const int n = s->m.n, dout = s->m.dout, din = s->m.din;
+    double *P = calloc((size_t)n * n, sizeof(double));
+    double *Px = malloc((size_t)n * sizeof(double));
+    double *Wx = malloc((size_t)(dout ? dout : 1) * sizeof(double));
+    if (!P || !Px || !Wx) {
+        free(P); free(Px); free(Wx);
+        return -1;
+    }
+    double inv_delta = 1.0 / delta;
+    for (int i = 0; i < n; i++)
+        P[(size_t)i * n + i] = inv_delta;
+    memset(w_out, 0, (size_t)dout * n * sizeof(double));
+    orc_reset(s);
+    for (size_t t = 0; t < T; t++) {
+        orc_step(s, u + t * din);
+        const double *x = s->V;
+        for (int i = 0; i < n; i++) { /* Px = P x */
+            double acc = 0.0;
+            for (int j = 0; j < n; j++)
+                acc = acc + P[(size_t)i * n + j] * x[j];
+            Px[i] = 0.0 + 1.0 * acc;
+        }
+        double dd = 0.0;
+        for (int i = 0; i < n; i++)
+            dd = dd + x[i] * Px[i];
+        double denom = lambda + dd;
+        double sc = 1.0 / denom;
+        for (int i = 0; i < n; i++)
+            Px[i] = sc * Px[i];
+        for (int o = 0; o < dout; o++) {
+            double acc = 0.0;
+            for (int i = 0; i < n; i++)
+                acc = acc + w_out[(size_t)o * n + i] * x[i];
+            Wx[o] = y[t * dout + o] - (0.0 + 1.0 * acc);
+        }
+        for (int o = 0; o < dout; o++) /* W_out += e k^T */
+            for (int i = 0; i < n; i++)
+                if (Px[i] != 0.0)
+                    w_out[(size_t)o * n + i] = w_out[(size_t)o * n + i] + Wx[o] * (1.0 * Px[i]);
+        for (int j = 0; j < n; j++) { /* P += (-denom) k k^T */
+            if (Px[j] == 0.0)
+                continue;
+            double tmp = -denom * Px[j];
+            for (int i = 0; i < n; i++)
+                P[(size_t)i * n + j] = P[(size_t)i * n + j] + Px[i] * tmp;
+        }
+        if (lambda != 1.0) {
+            double il = 1.0 / lambda;
+            for (size_t k = 0; k < (size_t)n * n; k++)
+                P[k] = il * P[k];
+        }
+    }
+    free(P);
+    free(Px);
+    free(Wx);
+    return 0;
+}

@@ -46,4 +46,9 @@ void orc_run(orc_state *s, const double *u, size_t T, double *phi, uint8_t *rast
 int orc_ridge(const double *X, const double *Y, size_t T, size_t washout, int n, int dout,
               double lam, double *w_out /* dout x n */);
 
+/* readout training restated from src/reservoir.c: w_out (dout x n) in/out */
+void orc_train_online(orc_state *s, const double *target, double lr, double *w_out);
+int  orc_train_rls(orc_state *s, const double *u, const double *y, size_t T, double delta,
+                   double lambda, double *w_out);
+
 #endif

@@ -94,6 +94,21 @@ class RidgeReport(C.Structure):
                 ("lu_fallback", C.c_int)]
 
 
+class AgileOpts(C.Structure):
+    _fields_ = [("mu", C.c_double), ("eta_min", C.c_double), ("eta_max", C.c_double),
+                ("patience0", C.c_double), ("patience_decay", C.c_double),
+                ("refine_step", C.c_double), ("refine_max_iters", C.c_int),
+                ("refine_no_improve", C.c_int), ("spsa_eps", C.c_double),
+                ("reflect_at_bounds", C.c_int), ("seed", C.c_uint64), ("verbose", C.c_int)]
+
+
+class AgileReport(C.Structure):
+    _fields_ = [("best_loss", C.c_double), ("best_iter", C.c_int), ("total_evals", C.c_int),
+                ("total_iters", C.c_int), ("exited_refinement", C.c_int)]
+
+
+LOSS_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_int, C.c_void_p)
+
 # Public symbols of include/spires.h and include/spires_ext.h with their
 # ctypes signatures (restype, argtypes).
 _VP = C.c_void_p
@@ -144,6 +159,8 @@ EXT_SIGNATURES = {
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),
     "spires_ext_train_ridge": (C.c_int, [_VP, _dp, _dp, C.c_size_t, C.c_double,
                                          C.POINTER(RidgeOpts), C.POINTER(RidgeReport)]),
+    "spires_ext_agile_minimize": (C.c_int, [_dp, _dp, _dp, C.c_int, LOSS_FN, _VP,
+                                            C.POINTER(AgileOpts), _dp, C.POINTER(AgileReport)]),
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
                                                  C.c_size_t, C.c_double, _VP, _VP]),
 }

@@ -85,7 +85,7 @@ static void project(double *x, const double *lo, const double *hi, int d, int re
 static void spsa(const double *th, const double *lo, const double *hi, int d, double eps,
                  loss_fn f, void *ctx, uint64_t *rng, double *g)
 {
-    double delta[64], tp[64], tm[64];
+    double delta[64] = {0}, tp[64] = {0}, tm[64] = {0};
     for (int i = 0; i < d; i++) {
         delta[i] = (pcg32_next(rng) & 1) ? 1.0 : -1.0;
         tp[i] = clampd(th[i] + eps * delta[i], lo[i], hi[i]);
@@ -443,6 +443,43 @@ SPIRES_EXPORT int spires_optimize(const spires_reservoir_config *base_config,
     out_pub->metric_std = sd;
     out_pub->best_score = mean - score_pub->lambda_var * sd - score_pub->lambda_cost * cost;
     return 0;
+}
+
+SPIRES_EXPORT spires_status spires_ext_agile_minimize(const double *theta0, const double *lower,
+                                                     const double *upper, int dim,
+                                                     spires_ext_loss_fn loss, void *ctx,
+                                                     const spires_ext_agile_opts *opts,
+                                                     double *theta_best,
+                                                     spires_ext_agile_report *report)
+{
+    if (!theta0 || !lower || !upper || !loss || !theta_best || dim <= 0 || dim > 64)
+        return SPIRES_ERR_INVALID_ARG;
+    /* defaults of src/agile.c:158-166 when no options are given */
+    agile_opts o = {1.3, 1e-3, 5e-1, 100.0, 0.9, 0.0, 200, 30, 1e-3, 1, 0xC0FFEEULL};
+    if (opts) {
+        o.mu = opts->mu;
+        o.eta_min = opts->eta_min;
+        o.eta_max = opts->eta_max;
+        o.patience0 = opts->patience0;
+        o.patience_decay = opts->patience_decay;
+        o.refine_step = opts->refine_step;
+        o.refine_max_iters = opts->refine_max_iters;
+        o.refine_no_improve = opts->refine_no_improve;
+        o.spsa_eps = opts->spsa_eps;
+        o.reflect = opts->reflect_at_bounds;
+        o.seed = opts->seed;
+    }
+    agile_report rep;
+    if (agile_run(theta0, lower, upper, dim, (loss_fn)loss, ctx, &o, theta_best, &rep) != 0)
+        return SPIRES_ERR_INVALID_ARG;
+    if (report) {
+        report->best_loss = rep.best_loss;
+        report->best_iter = rep.best_iter;
+        report->total_evals = rep.total_evals;
+        report->total_iters = rep.total_iters;
+        report->exited_refinement = rep.refined;
+    }
+    return SPIRES_OK;
 }
 
 int sp_default_gram_mode(void)

@@ -72,6 +72,9 @@ def _bind_oracle(lib):
     lib.orc_state_read.argtypes = [C.c_void_p, _dp, _dp]
     lib.orc_output.argtypes = [C.c_void_p, _dp]
     lib.orc_run.argtypes = [C.c_void_p, _dp, C.c_size_t, _dp, C.POINTER(C.c_uint8), _dp]
+    lib.orc_train_online.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
+    lib.orc_train_rls.restype = C.c_int
+    lib.orc_train_rls.argtypes = [C.c_void_p, _dp, _dp, C.c_size_t, C.c_double, C.c_double, _dp]
     lib.orc_ridge.restype = C.c_int
     lib.orc_ridge.argtypes = [_dp, _dp, C.c_size_t, C.c_size_t, C.c_int, C.c_int, C.c_double,
                               _dp]
@@ -128,6 +131,22 @@ class Oracle:
 
     def reset(self):
         self.lib.orc_reset(self.h)
+
+    def step(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self.lib.orc_step(self.h, sp.dptr(u))
+
+    def train_online(self, target, lr, w_out):
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        self.lib.orc_train_online(self.h, sp.dptr(t), lr, sp.dptr(w_out))
+
+    def train_rls(self, u, y, delta, lam):
+        u = np.ascontiguousarray(u, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        W = np.empty((self.dout, self.n))
+        assert self.lib.orc_train_rls(self.h, sp.dptr(u), sp.dptr(y), u.shape[0], delta, lam,
+                                      sp.dptr(W)) == 0
+        return W
 
 
 def oracle_ridge(X, Y, lam, washout=0):
