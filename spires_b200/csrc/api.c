@@ -497,6 +497,13 @@ SPIRES_EXPORT spires_status spires_ext_set_launch(spires_reservoir *r,
     return to_status(sp_dev_set_launch(r->dev, &s));
 }
 
+SPIRES_EXPORT spires_status spires_ext_autotune(spires_reservoir *r, size_t steps)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_autotune(r->dev, steps));
+}
+
 SPIRES_EXPORT spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed)
 {
     if (!r || !r->dev)

@@ -906,3 +906,139 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
 
 extern "C" size_t sp_dev_nwords(const sp_dev *d) { return d->nwords; }
 extern "C" long long sp_dev_kernel_launches(const sp_dev *d) { return d->launches; }
+
+// ------------------------------------------------------------- autotuner --
+// Candidate launch shapes are timed from one saved state (every mutable device
+// buffer and the step counters are snapshotted, and restored after each
+// candidate and at the end), with zero input, `steps` macro steps each.
+
+struct sp_snap_item {
+    void *ptr;
+    size_t bytes;
+    void *save;
+};
+
+static int snapshot(sp_dev *d, std::vector<sp_snap_item> &items, bool take)
+{
+    if (take) {
+        const size_t rs = (size_t)d->rs;
+        const size_t L = (size_t)(d->nc.L > 0 ? d->nc.L : 0);
+        items = {
+            {d->V, rs * 8, nullptr},
+            {d->tprev, rs * 8, nullptr},
+            {d->ring, d->ring ? d->ring_elems * 8 : 0, nullptr},
+            {d->cap_pos, d->cap_pos ? rs * 4 : 0, nullptr},
+            {d->refr_until, d->refr_until ? rs * 8 : 0, nullptr},
+            {d->rng, d->rng ? rs * 8 : 0, nullptr},
+            {d->spk, 2 * d->nwords * 4, nullptr},
+            {d->eff, d->eff ? 2 * rs * 8 : 0, nullptr},
+            {d->trace, d->trace ? rs * 8 : 0, nullptr},
+            {d->edge_trace, d->edge_trace ? d->nnz * 8 : 0, nullptr},
+            {d->Iring, d->Iring ? rs * (size_t)d->sc.frac_L * 8 : 0, nullptr},
+            {d->mx_tr, d->mx_tr ? rs * (size_t)d->sc.mexp_N * 8 : 0, nullptr},
+        };
+        (void)L;
+        for (auto &it : items) {
+            if (!it.ptr || !it.bytes)
+                continue;
+            if (cudaMalloc(&it.save, it.bytes) != cudaSuccess)
+                return SP_EALLOC;
+            SP_CK(cudaMemcpyAsync(it.save, it.ptr, it.bytes, cudaMemcpyDeviceToDevice, d->stream));
+        }
+        return SP_OK;
+    }
+    for (auto &it : items)
+        if (it.save)
+            SP_CK(cudaMemcpyAsync(it.ptr, it.save, it.bytes, cudaMemcpyDeviceToDevice, d->stream));
+    return SP_OK;
+}
+
+extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
+{
+    if (steps == 0)
+        steps = 64;
+    std::vector<sp_snap_item> items;
+    const long long step0 = d->step, syn0 = d->syn_step;
+    const int phase0 = d->phase;
+    int rc = snapshot(d, items, true);
+    std::vector<sp_launch> cand;
+    const int nw = d->nw;
+    std::vector<int> Gs;
+    auto addG = [&](int g) {
+        if (g >= 1 && g <= nw && std::find(Gs.begin(), Gs.end(), g) == Gs.end())
+            Gs.push_back(g);
+    };
+    addG(d->num_sms < nw ? d->num_sms : nw);
+    addG((nw + 1) / 2 < d->num_sms ? (nw + 1) / 2 : d->num_sms / 2);
+    addG((nw + 7) / 8);
+    addG((nw + 15) / 16);
+    addG((nw + 31) / 32);
+    for (int G : Gs) {
+        sp_launch l;
+        memset(&l, 0, sizeof(l));
+        l.ctas = G;
+        l.warps_max = (nw + G - 1) / G;
+        if (l.warps_max > 32)
+            continue;
+        cand.push_back(l);
+        if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 16) {
+            for (int rows : {16, 32, 64}) {
+                sp_launch v = l;
+                v.variant = 1;
+                v.rows = rows;
+                int bw, nbx;
+                box_geometry(v, &bw, &nbx);
+                const size_t stage = (size_t)rows * nbx * bw * 8;
+                const size_t base = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d);
+                const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
+                long long st = budget > base ? (long long)((budget - base) / (stage + 16)) : 0;
+                if (st > 16)
+                    st = 16;
+                if (st < 2)
+                    continue;
+                v.stages = (int)st;
+                cand.push_back(v);
+            }
+        }
+    }
+    const sp_launch keep = d->launch;
+    sp_launch best = keep;
+    float best_ms = 1e30f;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = SP_EINTERNAL;
+    for (size_t c = 0; c < cand.size() && !rc; ++c) {
+        if (sp_dev_set_launch(d, &cand[c]) != SP_OK)
+            continue;
+        cudaEventRecord(e0, d->stream);
+        int r2 = sp_dev_launch_chunk(d, nullptr, steps, nullptr, nullptr);
+        cudaEventRecord(e1, d->stream);
+        int r3 = sp_dev_sync(d);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (!r2 && !r3 && ms < best_ms) {
+            best_ms = ms;
+            best = cand[c];
+        }
+        // back to the saved state
+        snapshot(d, items, false);
+        d->step = step0;
+        d->syn_step = syn0;
+        d->phase = phase0;
+    }
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    cudaStreamSynchronize(d->stream);
+    for (auto &it : items)
+        if (it.save)
+            cudaFree(it.save);
+    if (rc) {
+        d->launch = keep;
+        return rc;
+    }
+    if (sp_dev_set_launch(d, &best) != SP_OK)
+        d->launch = keep;
+    return SP_OK;
+}

@@ -67,6 +67,7 @@ void *sp_dev_stream(sp_dev *d);
 int  sp_dev_get_launch(sp_dev *d, sp_launch *l);
 int  sp_dev_set_launch(sp_dev *d, const sp_launch *l);
 int  sp_dev_set_seed(sp_dev *d, uint64_t seed);
+int  sp_dev_autotune(sp_dev *d, size_t steps);
 size_t sp_dev_nwords(const sp_dev *d);
 long long sp_dev_kernel_launches(const sp_dev *d);
 

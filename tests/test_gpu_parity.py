@@ -219,3 +219,21 @@ def test_flif_gl_pipeline_chunked_runs_continue():
     phi = np.concatenate(parts)
     phi_o, _, _ = O.Oracle(cfg, sp.HostModel(cfg, seed=19)).run(u)
     assert same_bits(phi, phi_o)
+
+
+@pytest.mark.parametrize("neuron,L", [(sp.FLIF_GL, 256), (sp.LIF_DISCRETE, 1)])
+def test_autotune_keeps_state_and_results(neuron, L):
+    """spires_ext_autotune times launch shapes from a saved state and restores
+    it: a run continued after tuning equals an untuned run bit for bit."""
+    nparams = GL_L(L) if neuron == sp.FLIF_GL else O.NEURON_PARAMS[neuron]
+    cfg = make(neuron, sp.SYN_SIMPLE, n=3000, conn=0.003, nparams=nparams)
+    u = inputs(200, 2)
+    a = sp.Reservoir(cfg, seed=23)
+    pa1, _, _ = a.run_record(u[:100])
+    assert a.lib.spires_ext_autotune(a.h, 32) == sp.SPIRES_OK
+    pa2, _, _ = a.run_record(u[100:])
+    a.close()
+    b = sp.Reservoir(cfg, seed=23)
+    pb, _, _ = b.run_record(u)
+    b.close()
+    assert same_bits(np.concatenate([pa1, pa2]), pb)
