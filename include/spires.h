@@ -107,20 +107,27 @@ typedef struct {
 } spires_reservoir_config;
 
 /* ---- lifecycle ---- */
+/* replaces reference include/spires.h:131, src/spires_api.c:22-75 */
 spires_status spires_reservoir_create(const spires_reservoir_config *cfg,
                                       spires_reservoir **out_r);
+/* include/spires.h:133, src/spires_api.c:77-84 */
 void          spires_reservoir_destroy(spires_reservoir *r);
+/* include/spires.h:134, src/spires_api.c:86-92 */
 spires_status spires_reservoir_reset(spires_reservoir *r);
 
 /* ---- stepping ---- */
-/* One macro step (1/dt micro-steps) with input u_t[num_inputs]; NULL = zeros. */
+/* One macro step (1/dt micro-steps) with input u_t[num_inputs]; NULL = zeros.
+ * include/spires.h:142, src/spires_api.c:95-102 */
 spires_status spires_step(spires_reservoir *r, const double *u_t);
 
 /* Run input_series[series_length x num_inputs]; returns a malloc'd
- * [series_length x num_outputs] array of readouts (caller frees), or NULL. */
+ * [series_length x num_outputs] array of readouts (caller frees), or NULL.
+ * include/spires.h:155, src/spires_api.c:106-112 */
 double *spires_run(spires_reservoir *r, const double *input_series, size_t series_length);
 
-/* ---- training ---- */
+/* ---- training ----
+ * include/spires.h:161-177; src/spires_api.c:117-154 (online, ridge, RLS),
+ * src/spires_api.c:226-245 (coarse-grain) */
 spires_status spires_train_online(spires_reservoir *r,
                                   const double *target_vec, double lr);
 
@@ -139,7 +146,8 @@ spires_status spires_coarse_grain(const spires_reservoir *r,
                                   double weight_threshold,
                                   spires_reservoir **out_r);
 
-/* ---- state access ---- */
+/* ---- state access ----
+ * include/spires.h:185-218; src/spires_api.c:157-223 */
 double       *spires_copy_reservoir_state(spires_reservoir *r);          /* malloc'd [N] */
 spires_status spires_read_reservoir_state(spires_reservoir *r, double *buffer);
 spires_status spires_read_spike_state(spires_reservoir *r, double *buffer); /* 0.0 / 1.0 */
@@ -149,12 +157,13 @@ spires_status spires_compute_output(spires_reservoir *r, double *out);   /* y = 
 double       *spires_copy_readout(const spires_reservoir *r);            /* malloc'd [Dout*N] */
 spires_status spires_read_readout(const spires_reservoir *r, double *buffer);
 
-/* ---- introspection ---- */
+/* ---- introspection ---- include/spires.h:226-228, src/spires_api.c:248-261 */
 size_t spires_num_neurons(const spires_reservoir *r);
 size_t spires_num_inputs(const spires_reservoir *r);
 size_t spires_num_outputs(const spires_reservoir *r);
 
-/* ---- hyper-parameter search (AGILE) ---- */
+/* ---- hyper-parameter search (AGILE) ----
+ * include/spires.h:235-267, src/spires_api.c:440-498 */
 struct spires_opt_budget {
     double data_fraction;    /* 0..1 */
     int    num_seeds;
