@@ -168,6 +168,54 @@ spires_status spires_ext_ridge_solve_noalloc(const double *d_states, const doubl
                                              size_t T, size_t n, size_t dout, size_t washout,
                                              double lambda, double *d_w_out, void *stream);
 
+/* ---- many reservoirs in one launch ---------------------------------------
+ * No counterpart in the reference (its unit of work is one reservoir). A batch
+ * holds `count` reservoirs of uneven size, ring length, series length and
+ * model; instance k is built exactly as spires_reservoir_create builds it
+ * after srand(seeds[k]), so its weights, and its spike rasters and states from
+ * reset, are bit-identical to those of a separately created reservoir.
+ * Supported: SPIRES_NEURON_LIF_DISCRETE and SPIRES_NEURON_FLIF_GL with
+ * SPIRES_SYNAPSE_SIMPLE, num_outputs <= 16; anything else returns
+ * SPIRES_ERR_INVALID_ARG. Every call starts all instances from their reset
+ * state. Series arrays are indexed by instance: u[k] is T[k] x num_inputs_k
+ * (NULL array or NULL entry = zeros). The whole batch runs as one persistent
+ * cooperative kernel (one CUDA graph replay while the series lengths stay the
+ * same), so one call costs one launch sequence however many instances it has. */
+typedef struct spires_ext_batch spires_ext_batch;
+
+spires_status spires_ext_batch_create(const spires_reservoir_config *cfgs,
+                                      const unsigned *seeds, size_t count,
+                                      spires_ext_batch **out);
+void          spires_ext_batch_destroy(spires_ext_batch *b);
+
+/* Spike rasters (T[k] x ceil(N_k/32) words, bit i%32 of word i/32 = neuron i)
+ * and final membrane states (N_k) of every instance; NULL entries skip an
+ * output. elapsed_ms (optional): device time of the launch sequence. */
+spires_status spires_ext_batch_run(spires_ext_batch *b, const double *const *u,
+                                   const size_t *T, uint32_t *const *rasters,
+                                   double *const *final_states, double *elapsed_ms);
+
+/* Ridge readout of every instance (FP64, as spires_ext_train_ridge with
+ * opts; opts NULL = FP64 Gram, no washout): y[k] is T[k] x num_outputs_k, the
+ * fitted W_out (num_outputs_k x N_k) is kept for spires_ext_batch_predict and
+ * copied to w_out[k] when given. elapsed_ms: wall time of the call. */
+spires_status spires_ext_batch_train_ridge(spires_ext_batch *b, const double *const *u,
+                                           const double *const *y, const size_t *T,
+                                           const double *lambda,
+                                           const spires_ext_ridge_opts *opts,
+                                           double *const *w_out, double *elapsed_ms);
+
+/* Readouts y[k] (T[k] x num_outputs_k) of every instance over u[k] from reset
+ * with its current W_out (same arithmetic as spires_run). */
+spires_status spires_ext_batch_predict(spires_ext_batch *b, const double *const *u,
+                                       const size_t *T, double *const *y,
+                                       double *elapsed_ms);
+
+/* Schedule of the last run: CTAs of the grid, CTA groups, and whether the
+ * launch sequence runs as a CUDA graph (1) or as direct launches (-1). */
+spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas, int *groups,
+                                    int *graph);
+
 #ifdef __cplusplus
 }
 #endif

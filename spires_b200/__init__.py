@@ -163,6 +163,18 @@ EXT_SIGNATURES = {
                                             C.POINTER(AgileOpts), _dp, C.POINTER(AgileReport)]),
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
                                                  C.c_size_t, C.c_double, _VP, _VP]),
+    "spires_ext_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_uint), C.c_size_t,
+                                          C.POINTER(_VP)]),
+    "spires_ext_batch_destroy": (None, [_VP]),
+    "spires_ext_batch_run": (C.c_int, [_VP, C.POINTER(_dp), C.POINTER(C.c_size_t),
+                                       C.POINTER(_u32p), C.POINTER(_dp), _dp]),
+    "spires_ext_batch_train_ridge": (C.c_int, [_VP, C.POINTER(_dp), C.POINTER(_dp),
+                                               C.POINTER(C.c_size_t), _dp,
+                                               C.POINTER(RidgeOpts), C.POINTER(_dp), _dp]),
+    "spires_ext_batch_predict": (C.c_int, [_VP, C.POINTER(_dp), C.POINTER(C.c_size_t),
+                                           C.POINTER(_dp), _dp]),
+    "spires_ext_batch_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int)]),
 }
 
 _lib = None
@@ -396,6 +408,98 @@ class HostModel:
         c = np.empty(max(self.info.ring_len, 1))
         self.lib.spires_ext_model_coef(self.h, dptr(c))
         return c
+
+
+class Batch:
+    """spires_ext_batch: many reservoirs simulated in one persistent launch.
+
+    cfgs: list of Config; seeds: one srand() seed per instance (instance k is
+    built as spires_reservoir_create after srand(seeds[k]))."""
+
+    def __init__(self, cfgs, seeds, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+        self.count = len(cfgs)
+        arr = (Config * self.count)()
+        for k, c in enumerate(cfgs):
+            arr[k] = c
+        self._cfgs = list(cfgs)  # keeps parameter arrays alive
+        sd = (C.c_uint * self.count)(*[int(x) & 0xFFFFFFFF for x in seeds])
+        h = C.c_void_p()
+        st = self.lib.spires_ext_batch_create(arr, sd, self.count, C.byref(h))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_batch_create failed: {st}")
+        self.h = h
+        self.n = [int(c.num_neurons) for c in cfgs]
+        self.din = [int(c.num_inputs) for c in cfgs]
+        self.dout = [int(c.num_outputs) for c in cfgs]
+
+    def close(self):
+        if self.h:
+            self.lib.spires_ext_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _inputs(self, us, T):
+        if us is None:
+            return None, [int(t) for t in T], []
+        keep = [np.ascontiguousarray(u, dtype=np.float64) for u in us]
+        T = [u.shape[0] for u in keep] if T is None else [int(t) for t in T]
+        ptrs = (_dp * self.count)(*[dptr(u) for u in keep])
+        return ptrs, T, keep
+
+    def run(self, us=None, T=None, rasters=True, states=True):
+        """Run every instance from reset; returns (rasters, final states, device ms)."""
+        up, T, keep = self._inputs(us, T)
+        Ts = (C.c_size_t * self.count)(*T)
+        R = [np.empty((T[k], (self.n[k] + 31) // 32), np.uint32) for k in range(self.count)] \
+            if rasters else None
+        V = [np.empty(self.n[k]) for k in range(self.count)] if states else None
+        rp = (_u32p * self.count)(*[r.ctypes.data_as(_u32p) for r in R]) if R else None
+        vp = (_dp * self.count)(*[dptr(v) for v in V]) if V else None
+        ms = C.c_double(0.0)
+        st = self.lib.spires_ext_batch_run(self.h, up, Ts, rp, vp, C.byref(ms))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_batch_run failed: {st}")
+        return R, V, ms.value
+
+    def train_ridge(self, us, ys, lam, washout=0, gram_mode=0, T=None):
+        """Ridge readout of every instance; returns (list of W_out [dout, n], wall ms)."""
+        up, T, keep = self._inputs(us, T)
+        ykeep = [np.ascontiguousarray(y, dtype=np.float64) for y in ys]
+        yp = (_dp * self.count)(*[dptr(y) for y in ykeep])
+        Ts = (C.c_size_t * self.count)(*T)
+        lams = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, np.float64), (self.count,)))
+        W = [np.empty((self.dout[k], self.n[k])) for k in range(self.count)]
+        wp = (_dp * self.count)(*[dptr(w) for w in W])
+        o = RidgeOpts(gram_mode, 30, 1e-13, washout)
+        ms = C.c_double(0.0)
+        st = self.lib.spires_ext_batch_train_ridge(self.h, up, yp, Ts, dptr(lams), C.byref(o),
+                                                   wp, C.byref(ms))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_batch_train_ridge failed: {st}")
+        return W, ms.value
+
+    def predict(self, us, T=None):
+        """Readouts of every instance from reset with its current W_out."""
+        up, T, keep = self._inputs(us, T)
+        Ts = (C.c_size_t * self.count)(*T)
+        Y = [np.empty((T[k], max(self.dout[k], 1))) for k in range(self.count)]
+        yp = (_dp * self.count)(*[dptr(y) for y in Y])
+        ms = C.c_double(0.0)
+        st = self.lib.spires_ext_batch_predict(self.h, up, Ts, yp, C.byref(ms))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_batch_predict failed: {st}")
+        return Y, ms.value
+
+    def info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self.lib.spires_ext_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return {"ctas": a.value, "groups": b.value, "graph": c.value}
 
 
 def unpack_raster(R: np.ndarray, n: int) -> np.ndarray:

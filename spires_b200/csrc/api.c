@@ -553,3 +553,118 @@ SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
     }
     return to_status(rc);
 }
+
+/* ---- batched multi-reservoir path ---------------------------------------- */
+struct spires_ext_batch {
+    sp_batch *b;
+    size_t count;
+};
+
+SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_config *cfgs,
+                                                    const unsigned *seeds, size_t count,
+                                                    spires_ext_batch **out)
+{
+    if (!cfgs || !out || count == 0)
+        return SPIRES_ERR_INVALID_ARG;
+    *out = NULL;
+    sp_host_model *ms = calloc(count, sizeof(*ms));
+    spires_ext_batch *h = calloc(1, sizeof(*h));
+    if (!ms || !h) {
+        free(ms);
+        free(h);
+        return SPIRES_ERR_ALLOC;
+    }
+    int rc = SP_OK;
+    size_t built = 0;
+    for (; built < count && !rc; ++built) {
+        const spires_reservoir_config *c = &cfgs[built];
+        if (!dt_ok(c->dt)) {
+            rc = SP_EINVAL;
+            break;
+        }
+        if (seeds)
+            srand(seeds[built]);
+        rc = model_from_config(c, &ms[built]);
+        if (!rc)
+            rc = sp_model_build(&ms[built]);
+        if (rc) {
+            sp_model_free(&ms[built]);
+            break;
+        }
+    }
+    if (!rc)
+        rc = sp_batch_create(ms, count, &h->b);
+    if (rc) {
+        for (size_t k = 0; k < count; ++k)
+            sp_model_free(&ms[k]); /* no-op on zeroed or never-built entries */
+        free(ms);
+        free(h);
+        return to_status(rc);
+    }
+    free(ms);
+    h->count = count;
+    *out = h;
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT void spires_ext_batch_destroy(spires_ext_batch *b)
+{
+    if (!b)
+        return;
+    sp_batch_destroy(b->b);
+    free(b);
+}
+
+SPIRES_EXPORT spires_status spires_ext_batch_run(spires_ext_batch *b, const double *const *u,
+                                                 const size_t *T, uint32_t *const *rasters,
+                                                 double *const *final_states,
+                                                 double *elapsed_ms)
+{
+    if (!b || !T)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_batch_run(b->b, u, T, rasters, final_states, elapsed_ms));
+}
+
+SPIRES_EXPORT spires_status spires_ext_batch_train_ridge(spires_ext_batch *b,
+                                                         const double *const *u,
+                                                         const double *const *y,
+                                                         const size_t *T, const double *lambda,
+                                                         const spires_ext_ridge_opts *opts,
+                                                         double *const *w_out,
+                                                         double *elapsed_ms)
+{
+    if (!b || !T || !y || !lambda)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_opts o;
+    memset(&o, 0, sizeof(o));
+    o.gram_mode = SPIRES_EXT_GRAM_FP64;
+    o.max_refine = 30;
+    o.refine_tol = 1e-13;
+    if (opts) {
+        o.gram_mode = opts->gram_mode;
+        o.max_refine = opts->max_refine;
+        o.refine_tol = opts->refine_tol;
+        o.washout = opts->washout;
+    }
+    for (size_t k = 0; k < b->count; ++k)
+        if (!y[k] || o.washout >= T[k])
+            return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_batch_train_ridge(b->b, u, y, T, lambda, &o, w_out, elapsed_ms));
+}
+
+SPIRES_EXPORT spires_status spires_ext_batch_predict(spires_ext_batch *b, const double *const *u,
+                                                     const size_t *T, double *const *y,
+                                                     double *elapsed_ms)
+{
+    if (!b || !T)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_batch_predict(b->b, u, T, y, elapsed_ms));
+}
+
+SPIRES_EXPORT spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas,
+                                                  int *groups, int *graph)
+{
+    if (!b)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_batch_info(b->b, ctas, groups, graph));
+}

@@ -1,0 +1,987 @@
+// dev_batch.cu -- many reservoirs in one persistent launch.
+//
+// A batch holds `count` independent reservoirs of uneven size, ring length,
+// series length and model (LIF_DISCRETE or FLIF_GL, SIMPLE synapses). Each is
+// built on the host exactly as spires_reservoir_create builds it after
+// srand(seed_i), so its dynamics are those of the unbatched path, bit for bit.
+//
+// Work table. The host plans a static schedule: the cooperative grid of P CTAs
+// (256 threads each) is cut into groups of consecutive CTAs; each group runs a
+// list of instances one after another, all its CTAs on one instance at a time
+// with a group-local grid barrier (a counter per group). An instance needs at
+// least ceil(nw / 8) CTAs (one neuron per thread); instances are placed
+// heaviest first on the group that finishes them earliest (list scheduling on
+// an estimated time that takes both the history stream and the per-step
+// latency floor into account).
+//
+// The launch sequence of a run (input upload, state reset, barrier reset, the
+// cooperative kernel, the raster gather and download) is captured once into a
+// CUDA graph and replayed while the series lengths stay the same.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#include "sp_dev.h"
+#include "sp_kernels.cuh"
+#include "sp_dev_internal.h"
+#include "sp_step_kernel.cuh"
+
+using namespace sp;
+
+namespace {
+
+constexpr int kBatchThreads = 256;  // 8 warps per CTA
+
+struct BInst {
+    int n, nw, rs, din, L, ntype, micro;
+    long long T;  // macro steps of the current run
+    double a, b, c, d, e, f, g, dt, gamma, v_init, tprev_init;
+    double *V, *tprev, *ring;
+    unsigned *spk;  // [2][nw]
+    const long long *row_ptr;
+    const int *col;
+    const double *w, *W_in, *coef;
+    const int *nid_of, *pos_of;
+    const double *u;       // [T][din]
+    double *phi;           // [T][rs] position order, or null
+    unsigned *raster;      // [T][nw] position order
+    unsigned *raster_nat;  // [T][nw] neuron order
+    double *V_nat;         // [n] final state, neuron order
+};
+
+struct BParams {
+    const BInst *inst;
+    const int *cta_group, *group_start, *group_size, *job_off, *jobs;
+    unsigned long long *bar;  // one arrival counter per group
+    int *err;
+    int lmax;                 // longest FLIF_GL ring of the batch (coefficients in smem)
+};
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p)
+{
+    return *(const volatile unsigned long long *)p;
+}
+
+constexpr int kHistChunk = 16;  // ring values in flight per thread
+
+// FLIF_GL history of neuron column `ci` for lags k = 2..lim, in ascending k
+// (the order of src/neurons/flif_gl.c:68-72): the next chunk of ring values is
+// loaded while the current one is summed, so the dependent add chain does not
+// wait for memory at every chunk.
+__device__ __forceinline__ double batch_history(double hist, const double *s_coef,
+                                                const double *ci, int rs, int L, int head,
+                                                int lim)
+{
+    if (lim < 2)
+        return hist;
+    int r = head - 2;
+    if (r < 0)
+        r += L;
+    double cur[kHistChunk], nxt[kHistChunk];
+#pragma unroll
+    for (int j = 0; j < kHistChunk; ++j) {
+        cur[j] = (2 + j <= lim) ? __ldcg(ci + (size_t)r * rs) : 0.0;
+        r = (r == 0) ? L - 1 : r - 1;
+    }
+#pragma unroll 1
+    for (int k = 2; k <= lim; k += kHistChunk) {
+#pragma unroll
+        for (int j = 0; j < kHistChunk; ++j) {
+            nxt[j] = (k + kHistChunk + j <= lim) ? __ldcg(ci + (size_t)r * rs) : 0.0;
+            r = (r == 0) ? L - 1 : r - 1;
+        }
+#pragma unroll
+        for (int j = 0; j < kHistChunk; ++j)
+            if (k + j <= lim)
+                hist = add(hist, mul(s_coef[k + j], cur[j]));
+#pragma unroll
+        for (int j = 0; j < kHistChunk; ++j)
+            cur[j] = nxt[j];
+    }
+    return hist;
+}
+
+// One persistent cooperative launch over the whole batch. CTA c belongs to
+// group cta_group[c] (or to none, then it returns at once); a group runs its
+// job list in order, splitting each instance's warps evenly over its CTAs,
+// and meets at its own counter between micro-steps. The per-neuron arithmetic
+// is that of the single-reservoir kernel for LIF_DISCRETE / FLIF_GL with
+// SIMPLE synapses (src/neurons/lif_discrete.c:22-34, src/neurons/flif_gl.c:50-100,
+// src/synapses/simple.c:59-64, src/reservoir.c:113-165).
+__global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    double *s_coef = (double *)s_dyn;                    // [lmax]
+    unsigned *s_spk = (unsigned *)(s_coef + p.lmax);     // [nw]
+    __shared__ int s_flag, s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int grp = p.cta_group[blockIdx.x];
+    if (grp < 0)
+        return;  // CTA outside every group: takes part in no barrier
+    const int rank = blockIdx.x - p.group_start[grp];
+    const int gsize = p.group_size[grp];
+    unsigned long long *bar = p.bar + grp;
+    unsigned long long nbar = 0;
+    if (tid == 0)
+        s_abort = 0;
+
+    auto arrive = [&]() {
+        __syncthreads();
+        if (tid == 0 && gsize > 1) {
+            __threadfence();
+            atomicAdd(bar, 1ull);
+        }
+    };
+    auto wait = [&](long long step) -> bool {
+        ++nbar;
+        if (tid == 0) {
+            int ok = !s_abort;
+            if (ok && gsize > 1) {
+                const unsigned long long target = nbar * (unsigned long long)gsize;
+                unsigned long long t0 = globaltimer_ns(), polls = 0;
+                while (ld_volatile_u64(bar) < target) {
+                    if ((++polls & 255ull) == 0) {
+                        if (ld_volatile_i32(p.err) != kErrNone) {
+                            ok = 0;
+                            break;
+                        }
+                        if (globaltimer_ns() - t0 > kBarrierTimeoutNs || polls > kBarrierMaxPolls) {
+                            if (atomicCAS(p.err, kErrNone, kErrBarrierTimeout) == kErrNone)
+                                p.err[1] = (int)step;
+                            ok = 0;
+                            break;
+                        }
+                    }
+                    __nanosleep(32);
+                }
+                __threadfence();
+            }
+            s_flag = ok;
+            if (!ok)
+                s_abort = 1;
+        }
+        __syncthreads();
+        return s_flag != 0;
+    };
+
+    for (int j = p.job_off[grp]; j < p.job_off[grp + 1]; ++j) {
+        const BInst &I = p.inst[p.jobs[j]];
+        const long long B = I.T * I.micro;
+        if (B == 0)
+            continue;  // no steps: no arrival either, the counts stay matched
+        const int nw = I.nw, rs = I.rs, L = I.L;
+        const bool gl = I.ntype == SP_FLIF_GL;
+        const int wb0 = (int)((long long)rank * nw / gsize);
+        const int wb1 = (int)((long long)(rank + 1) * nw / gsize);
+        const int gw = wb0 + warp;
+        const bool wact = gw < wb1;
+        const int i = gw * 32 + lane;
+        const int nid = wact ? I.nid_of[i] : -1;
+        const bool act = nid >= 0;
+        __syncthreads();  // previous job's readers of s_coef are done
+        if (gl)
+            for (int k = tid; k < L; k += kBatchThreads)
+                s_coef[k] = I.coef[k];
+        double V = act ? I.V[i] : 0.0;
+        double tprev = (act && gl) ? I.tprev[i] : 0.0;
+        double vlast = (act && gl) ? I.ring[(size_t)(L - 1) * rs + i] : 0.0;
+        int cur = 0;
+        double ext = 0.0;
+        arrive();  // also publishes s_coef to the CTA
+        for (long long b = 0; b < B; ++b) {
+            const long long s = b / I.micro;
+            const int m = (int)(b % I.micro);
+            if (m == 0) {
+                // ext = 0 + gamma * sum_k W_in[i][k] u[k] (netlib dgemv order)
+                ext = 0.0;
+                if (act && I.din > 0 && I.gamma != 0.0) {
+                    const double *ur = I.u + (size_t)s * I.din;
+                    const double *wr = I.W_in + (size_t)i * I.din;
+                    double t = 0.0;
+                    for (int k = 0; k < I.din; ++k)
+                        t = add(t, mul(ldg_na(wr + k), ldg_na(ur + k)));
+                    ext = add(0.0, mul(I.gamma, t));
+                }
+            }
+            bool integ = false;
+            double hist = 0.0;
+            int head = 0;
+            if (gl) {
+                head = (int)(b % L);
+                integ = tprev > I.f;
+                const int lim = (int)(b < L ? b : L - 1);
+                if (act && integ) {
+                    if (lim >= 1)
+                        hist = add(hist, mul(s_coef[1], vlast));
+                    hist = batch_history(hist, s_coef, I.ring + i, rs, L, head, lim);
+                }
+            }
+            if (!wait(b))
+                return;
+            for (int wi = tid; wi < nw; wi += kBatchThreads)
+                s_spk[wi] = __ldcg(I.spk + (size_t)cur * nw + wi);
+            __syncthreads();
+            double rec = 0.0;
+            if (wact)
+                rec = rowpass_simple_warp(I.row_ptr, I.col, I.w, s_spk, gw * 32, 32, lane);
+            bool fired = false;
+            if (act) {
+                const double in = add(ext, rec);
+                if (!gl) {
+                    V = add(add(mul(I.c, V), in), I.d);
+                    if (V > I.b) {
+                        V = I.a;
+                        fired = true;
+                    }
+                } else {
+                    if (integ) {
+                        const double rhs = add(add(dvd(-sub(vlast, I.c), I.d), in), I.e);
+                        V = sub(mul(I.g, rhs), hist);
+                        if (V >= I.a) {
+                            V = I.b;
+                            fired = true;
+                            tprev = 0.0;
+                        }
+                    } else {
+                        V = I.b;
+                    }
+                    I.ring[(size_t)head * rs + i] = V;
+                    vlast = V;
+                    tprev = add(tprev, I.dt);
+                }
+            }
+            const unsigned word = __ballot_sync(kFull, fired);
+            if (wact && lane == 0)
+                I.spk[(size_t)(cur ^ 1) * nw + gw] = word;
+            if (m == I.micro - 1) {
+                if (act && I.phi)
+                    I.phi[(size_t)s * rs + i] = V;
+                if (wact && lane == 0)
+                    I.raster[(size_t)s * nw + gw] = word;
+            }
+            if (b + 1 < B)
+                arrive();
+            cur ^= 1;
+        }
+        if (act) {
+            I.V[i] = V;
+            if (gl)
+                I.tprev[i] = tprev;
+        }
+    }
+}
+
+// Reset every instance to its initial state: blockIdx.y = instance.
+__global__ void k_batch_reset(const BInst *inst)
+{
+    const BInst &I = inst[blockIdx.y];
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t start = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (size_t q = start; q < (size_t)I.rs; q += stride) {
+        const bool act = I.nid_of[q] >= 0;
+        I.V[q] = act ? I.v_init : 0.0;
+        if (I.ntype == SP_FLIF_GL)
+            I.tprev[q] = I.tprev_init;
+    }
+    for (size_t q = start; q < 2 * (size_t)I.nw; q += stride)
+        I.spk[q] = 0u;
+    if (I.ntype == SP_FLIF_GL)
+        for (size_t k = start; k < (size_t)I.L * I.rs; k += stride)
+            I.ring[k] = I.v_init;
+}
+
+// Rasters and final states of every instance back in neuron order.
+__global__ void k_batch_gather(const BInst *inst)
+{
+    const BInst &I = inst[blockIdx.y];
+    const size_t words = (size_t)I.nw;
+    const size_t total = (size_t)I.T * words * 32;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = k / (words * 32);
+        const int i = (int)(k % (words * 32));
+        bool b = false;
+        if (i < I.n) {
+            const int q = I.pos_of[i];
+            b = (I.raster[t * words + (q >> 5)] >> (q & 31)) & 1u;
+        }
+        const unsigned m = __ballot_sync(kFull, b);
+        if ((threadIdx.x & 31) == 0)
+            I.raster_nat[t * words + (i >> 5)] = m;
+    }
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)I.n;
+         i += (size_t)gridDim.x * blockDim.x)
+        I.V_nat[i] = I.V[I.pos_of[i]];
+}
+
+}  // namespace
+
+
+// ============================================================== host side ==
+
+struct sp_batch {
+    int device = 0, num_sms = 0, P = 0;
+    size_t smem = 0;
+    int lmax = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<sp_host_model> models;
+    std::vector<BInst> inst;
+    std::vector<double *> w_pos;  // per instance W_out [dout][rs], position space
+    char *arena = nullptr;
+    BInst *d_inst = nullptr;
+    int *d_sched = nullptr;  // cta_group | group_start | group_size | job_off | jobs
+    unsigned long long *d_bar = nullptr;
+    int *d_err = nullptr;
+    int ngroups = 0;
+    std::vector<int> cta_group, group_start, group_size, job_off, jobs;
+    // staging of one run shape (series lengths + whether states are kept)
+    std::vector<long long> T;
+    int want_phi = -1;
+    size_t u_total = 0, ras_total = 0, v_total = 0, phi_total = 0;
+    double *d_u = nullptr, *h_u = nullptr;
+    unsigned *d_ras = nullptr, *d_ras_nat = nullptr, *h_ras = nullptr;
+    double *d_vnat = nullptr, *h_vnat = nullptr;
+    double *d_phi = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_ok = 0;  // 1 captured, -1 capture refused (direct launches), 0 not tried
+    long long runs = 0;
+};
+
+#define BK(x)                                                                      \
+    do {                                                                           \
+        cudaError_t e_ = (x);                                                      \
+        if (e_ != cudaSuccess) {                                                   \
+            sp_dev_note_error(#x, e_);                                             \
+            return (e_ == cudaErrorMemoryAllocation) ? SP_EALLOC : SP_EINTERNAL;   \
+        }                                                                          \
+    } while (0)
+
+static void batch_free_run(sp_batch *b)
+{
+    if (b->graph)
+        cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_ok = 0;
+    void *dv[] = {b->d_u, b->d_ras, b->d_ras_nat, b->d_vnat, b->d_phi};
+    for (void *p : dv)
+        if (p)
+            cudaFree(p);
+    void *hv[] = {b->h_u, b->h_ras, b->h_vnat};
+    for (void *p : hv)
+        if (p)
+            cudaFreeHost(p);
+    b->d_u = b->h_u = b->d_vnat = b->h_vnat = b->d_phi = nullptr;
+    b->d_ras = b->d_ras_nat = b->h_ras = nullptr;
+    b->T.clear();
+    b->want_phi = -1;
+}
+
+extern "C" void sp_batch_destroy(sp_batch *b)
+{
+    if (!b)
+        return;
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    batch_free_run(b);
+    void *d[] = {b->arena, b->d_inst, b->d_sched, b->d_bar, b->d_err};
+    for (void *p : d)
+        if (p)
+            cudaFree(p);
+    for (auto &m : b->models)
+        sp_model_free(&m);
+    if (b->stream)
+        cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+static int min_ctas(const BInst &I) { return (I.nw + kBatchThreads / 32 - 1) / (kBatchThreads / 32); }
+
+// Estimated seconds for one instance on g CTAs: the larger of a per-step
+// latency floor (the history chunks wait for memory one after another) and the
+// instance's share of the CTAs' streaming rate.
+static double est_time(const BInst &I, long long T, int g)
+{
+    const double cta_bw = 20e9;  // bytes/s one CTA streams
+    const double steps = (double)T * I.micro;
+    if (I.ntype == SP_FLIF_GL) {
+        const double floor_s = 2e-6 + 0.4e-6 * ((I.L + kHistChunk - 1) / kHistChunk);
+        const double mem = 8.0 * I.n * (double)I.L / (g * cta_bw);
+        return steps * std::max(floor_s, mem);
+    }
+    return steps * std::max(2e-6, 64.0 * I.n / (g * cta_bw));
+}
+
+// Static schedule: instances in the given order go to the existing group
+// (wide enough) that finishes them first, or to a new group of their minimum
+// width while CTAs are free. Returns false when an instance found no group.
+static bool plan_order(sp_batch *b, const std::vector<int> &order, const std::vector<long long> &T)
+{
+    struct G {
+        int start, size;
+        double busy;
+        std::vector<int> jobs;
+    };
+    std::vector<G> groups;
+    int used = 0;
+    for (int k : order) {
+        const BInst &I = b->inst[k];
+        const int gmin = min_ctas(I);
+        int best = -1;
+        double best_fin = 1e300;
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+            if (groups[gi].size < gmin)
+                continue;
+            const double fin = groups[gi].busy + est_time(I, T[k], groups[gi].size);
+            if (fin < best_fin) {
+                best_fin = fin;
+                best = (int)gi;
+            }
+        }
+        if (used + gmin <= b->P) {
+            const double fin = est_time(I, T[k], gmin);
+            if (best < 0 || fin < best_fin) {
+                groups.push_back(G{used, gmin, 0.0, {}});
+                used += gmin;
+                best = (int)groups.size() - 1;
+                best_fin = fin;
+            }
+        }
+        if (best < 0)
+            return false;
+        groups[best].busy = best_fin;
+        groups[best].jobs.push_back(k);
+    }
+    b->ngroups = (int)groups.size();
+    b->cta_group.assign(b->P, -1);
+    b->group_start.clear();
+    b->group_size.clear();
+    b->job_off.assign(1, 0);
+    b->jobs.clear();
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        for (int c = 0; c < groups[gi].size; ++c)
+            b->cta_group[groups[gi].start + c] = (int)gi;
+        b->group_start.push_back(groups[gi].start);
+        b->group_size.push_back(groups[gi].size);
+        for (int k : groups[gi].jobs)
+            b->jobs.push_back(k);
+        b->job_off.push_back((int)b->jobs.size());
+    }
+    return true;
+}
+
+// Heaviest first (longest-processing-time list scheduling); if a wide
+// instance then finds every CTA taken by narrower groups, plan again widest
+// first, which always succeeds because every instance fits the grid.
+static void plan(sp_batch *b, const std::vector<long long> &T)
+{
+    const size_t cnt = b->inst.size();
+    std::vector<int> order(cnt);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<double> solo(cnt);
+    for (size_t k = 0; k < cnt; ++k)
+        solo[k] = est_time(b->inst[k], T[k], min_ctas(b->inst[k]));
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return solo[x] > solo[y]; });
+    if (plan_order(b, order, T))
+        return;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const int gx = min_ctas(b->inst[x]), gy = min_ctas(b->inst[y]);
+        return gx != gy ? gx > gy : solo[x] > solo[y];
+    });
+    plan_order(b, order, T);
+}
+
+extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **out)
+{
+    *out = nullptr;
+    if (count == 0 || count > 65535)
+        return SP_EINVAL;
+    for (size_t k = 0; k < count; ++k) {
+        const sp_host_model &m = models[k];
+        if ((m.neuron_type != SP_LIF_DISCRETE && m.neuron_type != SP_FLIF_GL) ||
+            m.syn_type != SP_SYN_SIMPLE || m.n == 0 || m.dout > 16)
+            return SP_EINVAL;
+    }
+    sp_batch *b = new sp_batch();
+    if (cudaGetDevice(&b->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return SP_EINTERNAL;
+    }
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->models.assign(models, models + count);
+    memset(models, 0, count * sizeof(sp_host_model)); /* the batch owns the buffers now */
+
+    size_t total = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = total;
+        total += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    b->inst.resize(count);
+    b->w_pos.resize(count);
+    struct Off {
+        size_t V, tp, ring, spk, rp, col, w, win, coef, nid, pos, wout;
+    };
+    std::vector<Off> off(count);
+    std::vector<std::vector<int>> pos(count), nid(count);
+    size_t max_nw = 1;
+    for (size_t k = 0; k < count; ++k) {
+        const sp_host_model &m = b->models[k];
+        BInst &I = b->inst[k];
+        memset(&I, 0, sizeof(I));
+        I.n = (int)m.n;
+        I.nw = (int)((m.n + 31) / 32);
+        I.rs = I.nw * 32;
+        I.din = (int)m.din;
+        I.L = m.neuron_type == SP_FLIF_GL ? m.nc.L : 1;
+        I.ntype = m.neuron_type;
+        I.micro = m.micro_steps;
+        I.a = m.nc.a;
+        I.b = m.nc.b;
+        I.c = m.nc.c;
+        I.d = m.nc.d;
+        I.e = m.nc.e;
+        I.f = m.nc.f;
+        I.g = m.nc.g;
+        I.dt = m.dt;
+        I.gamma = m.input_strength;
+        I.v_init = m.nc.v_init;
+        I.tprev_init = m.nc.tprev_init;
+        max_nw = std::max(max_nw, (size_t)I.nw);
+        if (I.ntype == SP_FLIF_GL)
+            b->lmax = std::max(b->lmax, I.L);
+        const size_t rs = I.rs;
+        Off &o = off[k];
+        o.V = take(rs * 8);
+        o.tp = take(rs * 8);
+        o.ring = take(I.ntype == SP_FLIF_GL ? rs * (size_t)I.L * 8 : 8);
+        o.spk = take(2 * (size_t)I.nw * 4);
+        o.rp = take((rs + 1) * 8);
+        o.col = take((m.nnz ? m.nnz : 1) * 4);
+        o.w = take((m.nnz ? m.nnz : 1) * 8);
+        o.win = take(rs * (m.din ? m.din : 1) * 8);
+        o.coef = take((size_t)I.L * 8);
+        o.nid = take(rs * 4);
+        o.pos = take(m.n * 4);
+        o.wout = take(rs * (m.dout ? m.dout : 1) * 8);
+    }
+    b->smem = (size_t)b->lmax * 8 + max_nw * 4;
+    int rc = SP_OK;
+    int per_sm = 0;
+    if (b->smem > 200 * 1024)
+        rc = SP_EINVAL;
+    if (!rc && b->smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)b->smem) != cudaSuccess)
+        rc = SP_EINVAL;
+    if (!rc) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads, b->smem);
+        per_sm = std::min(per_sm, 2);
+        if (per_sm < 1)
+            rc = SP_EINVAL;
+        b->P = per_sm * b->num_sms;
+    }
+    for (size_t k = 0; !rc && k < count; ++k)
+        if (min_ctas(b->inst[k]) > b->P)
+            rc = SP_EINVAL;  // wider than the whole grid
+    if (!rc && cudaMalloc(&b->arena, total) != cudaSuccess)
+        rc = SP_EALLOC;
+    if (rc) {
+        cudaGetLastError();
+        sp_batch_destroy(b);
+        return rc;
+    }
+    for (size_t k = 0; k < count; ++k) {
+        const sp_host_model &m = b->models[k];
+        BInst &I = b->inst[k];
+        const Off &o = off[k];
+        char *A = b->arena;
+        const size_t rs = I.rs;
+        sp_make_layout(&m, I.nw, pos[k], nid[k]);
+        // CSR in position order, as the single-reservoir path lays it out
+        std::vector<long long> rp(rs + 1, 0);
+        std::vector<int> col(m.nnz ? m.nnz : 1);
+        std::vector<double> w(m.nnz ? m.nnz : 1), win(rs * (m.din ? m.din : 1), 0.0),
+            wout(rs * (m.dout ? m.dout : 1), 0.0);
+        size_t e = 0;
+        for (size_t q = 0; q < rs; ++q) {
+            rp[q] = (long long)e;
+            const int i = nid[k][q];
+            if (i < 0)
+                continue;
+            for (int64_t kk = m.row_ptr[i]; kk < m.row_ptr[i + 1]; ++kk, ++e) {
+                col[e] = pos[k][m.col[kk]];
+                w[e] = m.w[kk];
+            }
+            for (size_t j = 0; j < m.din; ++j)
+                win[q * m.din + j] = m.W_in[(size_t)i * m.din + j];
+            for (size_t oo = 0; oo < m.dout; ++oo)
+                wout[oo * rs + q] = m.W_out[oo * m.n + i];
+        }
+        rp[rs] = (long long)e;
+        I.V = (double *)(A + o.V);
+        I.tprev = (double *)(A + o.tp);
+        I.ring = (double *)(A + o.ring);
+        I.spk = (unsigned *)(A + o.spk);
+        I.row_ptr = (const long long *)(A + o.rp);
+        I.col = (const int *)(A + o.col);
+        I.w = (const double *)(A + o.w);
+        I.W_in = (const double *)(A + o.win);
+        I.coef = (const double *)(A + o.coef);
+        I.nid_of = (const int *)(A + o.nid);
+        I.pos_of = (const int *)(A + o.pos);
+        b->w_pos[k] = (double *)(A + o.wout);
+        // synchronous copies: the staging vectors die at the end of this iteration
+        bool ok = cudaMemcpy(A + o.rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(A + o.col, col.data(), col.size() * 4, cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(A + o.w, w.data(), w.size() * 8, cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(A + o.win, win.data(), win.size() * 8, cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(A + o.wout, wout.data(), wout.size() * 8, cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(A + o.nid, nid[k].data(), rs * 4, cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(A + o.pos, pos[k].data(), m.n * 4, cudaMemcpyHostToDevice) ==
+                      cudaSuccess;
+        if (ok && I.ntype == SP_FLIF_GL)
+            ok = cudaMemcpy(A + o.coef, m.coef, (size_t)I.L * 8, cudaMemcpyHostToDevice) ==
+                 cudaSuccess;
+        if (!ok) {
+            sp_batch_destroy(b);
+            return SP_EINTERNAL;
+        }
+    }
+    if (cudaMalloc(&b->d_bar, (size_t)b->P * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&b->d_err, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_inst, count * sizeof(BInst)) != cudaSuccess ||
+        cudaMemset(b->d_err, 0, 4 * sizeof(int)) != cudaSuccess) {
+        sp_batch_destroy(b);
+        return SP_EALLOC;
+    }
+    *out = b;
+    return SP_OK;
+}
+
+// Staging buffers and schedule for series lengths T (re-planned only when T
+// or the need for states changes).
+static int batch_prepare(sp_batch *b, const size_t *T, int want_phi)
+{
+    const size_t cnt = b->inst.size();
+    bool same = b->T.size() == cnt && b->want_phi == want_phi;
+    for (size_t k = 0; same && k < cnt; ++k)
+        same = b->T[k] == (long long)T[k];
+    if (same)
+        return SP_OK;
+    batch_free_run(b);
+    b->T.assign(T, T + cnt);
+    b->want_phi = want_phi;
+    size_t u_total = 0, ras_total = 0, v_total = 0, phi_total = 0;
+    for (size_t k = 0; k < cnt; ++k) {
+        u_total += T[k] * b->inst[k].din;
+        ras_total += T[k] * b->inst[k].nw;
+        v_total += b->inst[k].n;
+        phi_total += want_phi ? T[k] * b->inst[k].rs : 0;
+    }
+    b->u_total = u_total;
+    b->ras_total = ras_total;
+    b->v_total = v_total;
+    b->phi_total = phi_total;
+    BK(cudaMalloc(&b->d_u, (u_total ? u_total : 1) * 8));
+    BK(cudaMalloc(&b->d_ras, (ras_total ? ras_total : 1) * 4));
+    BK(cudaMalloc(&b->d_ras_nat, (ras_total ? ras_total : 1) * 4));
+    BK(cudaMalloc(&b->d_vnat, v_total * 8));
+    if (want_phi)
+        BK(cudaMalloc(&b->d_phi, (phi_total ? phi_total : 1) * 8));
+    BK(cudaMallocHost(&b->h_u, (u_total ? u_total : 1) * 8));
+    BK(cudaMallocHost(&b->h_ras, (ras_total ? ras_total : 1) * 4));
+    BK(cudaMallocHost(&b->h_vnat, v_total * 8));
+    size_t uo = 0, ro = 0, vo = 0, po = 0;
+    for (size_t k = 0; k < cnt; ++k) {
+        BInst &I = b->inst[k];
+        I.T = (long long)T[k];
+        I.u = b->d_u + uo;
+        I.raster = b->d_ras + ro;
+        I.raster_nat = b->d_ras_nat + ro;
+        I.V_nat = b->d_vnat + vo;
+        I.phi = want_phi ? b->d_phi + po : nullptr;
+        uo += T[k] * I.din;
+        ro += T[k] * I.nw;
+        vo += I.n;
+        po += want_phi ? T[k] * I.rs : 0;
+    }
+    plan(b, b->T);
+    std::vector<int> sched;
+    sched.insert(sched.end(), b->cta_group.begin(), b->cta_group.end());
+    sched.insert(sched.end(), b->group_start.begin(), b->group_start.end());
+    sched.insert(sched.end(), b->group_size.begin(), b->group_size.end());
+    sched.insert(sched.end(), b->job_off.begin(), b->job_off.end());
+    sched.insert(sched.end(), b->jobs.begin(), b->jobs.end());
+    if (b->d_sched)
+        cudaFree(b->d_sched);
+    b->d_sched = nullptr;
+    BK(cudaMalloc(&b->d_sched, sched.size() * sizeof(int)));
+    BK(cudaMemcpy(b->d_sched, sched.data(), sched.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->d_inst, b->inst.data(), cnt * sizeof(BInst), cudaMemcpyHostToDevice));
+    return SP_OK;
+}
+
+// Device work of one run on b->stream (the sequence the graph captures).
+static int batch_enqueue(sp_batch *b)
+{
+    const unsigned cnt = (unsigned)b->inst.size();
+    BK(cudaMemcpyAsync(b->d_u, b->h_u, (b->u_total ? b->u_total : 1) * 8, cudaMemcpyHostToDevice,
+                       b->stream));
+    const dim3 rg(64, cnt);
+    k_batch_reset<<<rg, 256, 0, b->stream>>>(b->d_inst);
+    BK(cudaGetLastError());
+    BK(cudaMemsetAsync(b->d_bar, 0, (size_t)b->P * sizeof(unsigned long long), b->stream));
+    BParams p;
+    const int P = b->P, G = b->ngroups;
+    p.inst = b->d_inst;
+    p.cta_group = b->d_sched;
+    p.group_start = b->d_sched + P;
+    p.group_size = b->d_sched + P + G;
+    p.job_off = b->d_sched + P + 2 * G;
+    p.jobs = b->d_sched + P + 3 * G + 1;
+    p.bar = b->d_bar;
+    p.err = b->d_err;
+    p.lmax = b->lmax;
+    void *args[] = {&p};
+    BK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(P), dim3(kBatchThreads), args,
+                                   b->smem, b->stream));
+    k_batch_gather<<<rg, 256, 0, b->stream>>>(b->d_inst);
+    BK(cudaGetLastError());
+    BK(cudaMemcpyAsync(b->h_ras, b->d_ras_nat, (b->ras_total ? b->ras_total : 1) * 4,
+                       cudaMemcpyDeviceToHost, b->stream));
+    BK(cudaMemcpyAsync(b->h_vnat, b->d_vnat, b->v_total * 8, cudaMemcpyDeviceToHost, b->stream));
+    return SP_OK;
+}
+
+// Stage inputs, replay (or capture) the graph, wait, check the error flag.
+static int batch_simulate(sp_batch *b, const double *const *u, float *ms)
+{
+    const size_t cnt = b->inst.size();
+    size_t uo = 0;
+    for (size_t k = 0; k < cnt; ++k) {
+        const size_t len = (size_t)b->T[k] * b->inst[k].din;
+        if (u && u[k])
+            memcpy(b->h_u + uo, u[k], len * 8);
+        else
+            memset(b->h_u + uo, 0, len * 8);
+        uo += len;
+    }
+    if (b->graph_ok == 0) {
+        cudaGraph_t g = nullptr;
+        bool ok = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            const int r2 = batch_enqueue(b);
+            ok = cudaStreamEndCapture(b->stream, &g) == cudaSuccess && r2 == SP_OK;
+        }
+        if (ok)
+            ok = cudaGraphInstantiate(&b->graph, g, 0) == cudaSuccess;
+        if (g)
+            cudaGraphDestroy(g);
+        cudaGetLastError();
+        b->graph_ok = ok ? 1 : -1;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BK(cudaEventCreate(&e0));
+    BK(cudaEventCreate(&e1));
+    BK(cudaEventRecord(e0, b->stream));
+    int rc = SP_OK;
+    if (b->graph_ok == 1) {
+        if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess)
+            rc = SP_EINTERNAL;
+    } else {
+        rc = batch_enqueue(b);
+    }
+    cudaEventRecord(e1, b->stream);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+        rc = SP_EINTERNAL;
+    if (!rc && ms)
+        cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc)
+        return rc;
+    b->runs++;
+    int herr[2] = {0, 0};
+    BK(cudaMemcpy(herr, b->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
+    if (herr[0] != 0) {
+        fprintf(stderr, "spires: batch kernel error %d at micro-step %d\n", herr[0], herr[1]);
+        cudaMemset(b->d_err, 0, 4 * sizeof(int));
+        return SP_EINTERNAL;
+    }
+    return SP_OK;
+}
+
+extern "C" int sp_batch_run(sp_batch *b, const double *const *u, const size_t *T,
+                            uint32_t *const *raster, double *const *final_state,
+                            double *elapsed_ms)
+{
+    int rc = batch_prepare(b, T, 0);
+    if (rc)
+        return rc;
+    float ms = 0.f;
+    rc = batch_simulate(b, u, &ms);
+    if (rc)
+        return rc;
+    if (elapsed_ms)
+        *elapsed_ms = ms;
+    size_t ro = 0, vo = 0;
+    for (size_t k = 0; k < b->inst.size(); ++k) {
+        const size_t len = (size_t)b->T[k] * b->inst[k].nw;
+        if (raster && raster[k])
+            memcpy(raster[k], b->h_ras + ro, len * 4);
+        if (final_state && final_state[k])
+            memcpy(final_state[k], b->h_vnat + vo, (size_t)b->inst[k].n * 8);
+        ro += len;
+        vo += b->inst[k].n;
+    }
+    return SP_OK;
+}
+
+// Ridge readouts of every instance from one batched simulation: states of
+// all instances recorded in one launch, then per instance the FP64 ridge of
+// the single-reservoir path (Gram + Cholesky + refinement) on its states.
+extern "C" int sp_batch_train_ridge(sp_batch *b, const double *const *u, const double *const *y,
+                                    const size_t *T, const double *lambda,
+                                    const sp_ridge_opts *o, double *const *w_out,
+                                    double *elapsed_ms)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = batch_prepare(b, T, 1);
+    if (rc)
+        return rc;
+    rc = batch_simulate(b, u, nullptr);
+    if (rc)
+        return rc;
+    size_t max_tn = 1, max_ty = 1, max_wn = 1;
+    for (size_t k = 0; k < b->inst.size(); ++k) {
+        max_tn = std::max(max_tn, T[k] * (size_t)b->inst[k].n);
+        max_ty = std::max(max_ty, T[k] * b->models[k].dout);
+        max_wn = std::max(max_wn, (size_t)b->inst[k].n * b->models[k].dout);
+    }
+    double *nat = nullptr, *Y = nullptr, *W = nullptr;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(b->stream);
+        if (nat)
+            cudaFree(nat);
+        if (Y)
+            cudaFree(Y);
+        if (W)
+            cudaFree(W);
+    };
+    if (cudaMalloc(&nat, max_tn * 8) != cudaSuccess || cudaMalloc(&Y, max_ty * 8) != cudaSuccess ||
+        cudaMalloc(&W, max_wn * 8) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return SP_EALLOC;
+    }
+    size_t po = 0;
+    for (size_t k = 0; k < b->inst.size() && !rc; ++k) {
+        const BInst &I = b->inst[k];
+        const int dout = (int)b->models[k].dout;
+        const double *phi = b->d_phi + po;
+        po += T[k] * I.rs;
+        if (dout == 0)
+            continue;
+        if (cudaMemcpyAsync(Y, y[k], T[k] * dout * 8, cudaMemcpyHostToDevice, b->stream) !=
+            cudaSuccess) {
+            rc = SP_EINTERNAL;
+            break;
+        }
+        rc = sp_launch_gather_rows(b->stream, phi, I.rs, I.pos_of, I.n, T[k], nat);
+        if (rc)
+            break;
+        sp_ridge_report rep;
+        memset(&rep, 0, sizeof(rep));
+        rc = sp_ridge_phi(b->stream, nat, I.n, T[k], Y, dout, lambda[k], o, &rep, W);
+        if (rc == SP_RIDGE_SINGULAR) {
+            // singular: W_out of this instance stays as it was (dgesv failure)
+            rc = SP_OK;
+            if (w_out && w_out[k]) {
+                rc = sp_launch_gather_rows(b->stream, b->w_pos[k], I.rs, I.pos_of, I.n,
+                                           (size_t)dout, W);
+                if (!rc && cudaMemcpy(w_out[k], W, (size_t)dout * I.n * 8,
+                                      cudaMemcpyDeviceToHost) != cudaSuccess)
+                    rc = SP_EINTERNAL;
+            }
+            continue;
+        }
+        if (rc)
+            break;
+        rc = sp_launch_wout_to_pos(b->stream, W, I.nid_of, I.n, I.rs, dout, b->w_pos[k]);
+        if (!rc && w_out && w_out[k] &&
+            cudaMemcpyAsync(w_out[k], W, (size_t)dout * I.n * 8, cudaMemcpyDeviceToHost,
+                            b->stream) != cudaSuccess)
+            rc = SP_EINTERNAL;
+        if (!rc && cudaStreamSynchronize(b->stream) != cudaSuccess)
+            rc = SP_EINTERNAL;
+    }
+    cleanup();
+    if (elapsed_ms)
+        *elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+// Readouts of every instance over its series from reset, with its current
+// W_out: y[k] is T[k] x dout, the same arithmetic as spires_run.
+extern "C" int sp_batch_predict(sp_batch *b, const double *const *u, const size_t *T,
+                                double *const *y, double *elapsed_ms)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = batch_prepare(b, T, 1);
+    if (rc)
+        return rc;
+    rc = batch_simulate(b, u, nullptr);
+    if (rc)
+        return rc;
+    size_t max_ty = 1;
+    for (size_t k = 0; k < b->inst.size(); ++k)
+        max_ty = std::max(max_ty, T[k] * b->models[k].dout);
+    double *Y = nullptr;
+    BK(cudaMalloc(&Y, max_ty * 8));
+    size_t po = 0;
+    for (size_t k = 0; k < b->inst.size() && !rc; ++k) {
+        const BInst &I = b->inst[k];
+        const int dout = (int)b->models[k].dout;
+        const double *phi = b->d_phi + po;
+        po += T[k] * I.rs;
+        if (dout == 0 || !y || !y[k])
+            continue;
+        rc = sp_launch_readout(b->stream, b->w_pos[k], phi, I.rs, T[k], dout, Y);
+        if (!rc && cudaMemcpyAsync(y[k], Y, T[k] * dout * 8, cudaMemcpyDeviceToHost, b->stream) !=
+                       cudaSuccess)
+            rc = SP_EINTERNAL;
+        if (!rc && cudaStreamSynchronize(b->stream) != cudaSuccess)
+            rc = SP_EINTERNAL;
+    }
+    cudaStreamSynchronize(b->stream);
+    cudaFree(Y);
+    if (elapsed_ms)
+        *elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+extern "C" int sp_batch_info(const sp_batch *b, int *ctas, int *groups, int *graph)
+{
+    if (ctas)
+        *ctas = b->P;
+    if (groups)
+        *groups = b->ngroups;
+    if (graph)
+        *graph = b->graph_ok;
+    return SP_OK;
+}

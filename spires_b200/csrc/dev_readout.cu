@@ -647,30 +647,24 @@ static double device_norm(cudaStream_t s, const double *x, size_t cnt, double *d
     return sqrt(h);
 }
 
-extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,
-                                  const double *h_y, size_t T, double lambda,
-                                  const sp_ridge_opts *o, sp_ridge_report *rep, double *h_W_out)
+// Ridge on states already on the device: Phi [T x n] row-major (neuron order),
+// Y [T x dout]; rows [washout, T) enter the Gram. On success d_W_out [dout x n]
+// holds the solution; SP_RIDGE_SINGULAR leaves it untouched (dgesv failure in
+// the reference leaves W_out as it was). Work buffers are allocated per call.
+extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
+                            const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                            sp_ridge_report *rep, double *d_W_out)
 {
     int rc = SP_OK;
-    const int n = d->n, dout = d->dout;
-    cudaStream_t s = d->stream;
-    double *Phi = nullptr, *Y = nullptr, *A = nullptr, *Aw = nullptr, *B = nullptr, *W = nullptr,
-           *R = nullptr, *E = nullptr, *part = nullptr, *tmp = nullptr;
+    double *A = nullptr, *Aw = nullptr, *B = nullptr, *W = nullptr, *R = nullptr, *E = nullptr,
+           *part = nullptr, *tmp = nullptr;
     int *info = nullptr, *piv = nullptr;
     const int parts = 64;
     const size_t w0 = o->washout;
-    memset(rep, 0, sizeof(*rep));
     if (dout == 0)
         return SP_OK;
     if (dout > 16)
         return SP_EINVAL; /* per-thread accumulators below hold up to 16 outputs */
-    auto tstart = std::chrono::steady_clock::now();
-
-    rc = sp_dev_reset_neurons(d, m);
-    if (rc)
-        return rc;
-    RK(cudaMalloc(&Phi, (T ? T : 1) * (size_t)n * sizeof(double)));
-    RK(cudaMalloc(&Y, (T ? T : 1) * (size_t)dout * sizeof(double)));
     RK(cudaMalloc(&A, (size_t)n * n * sizeof(double)));
     RK(cudaMalloc(&B, (size_t)n * dout * sizeof(double)));
     RK(cudaMalloc(&W, (size_t)n * dout * sizeof(double)));
@@ -681,19 +675,6 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
     RK(cudaMalloc(&info, sizeof(int)));
     RK(cudaMalloc(&piv, (size_t)n * sizeof(int)));
     RK(cudaMemsetAsync(info, 0, sizeof(int), s));
-    RK(cudaMemcpyAsync(Y, h_y, T * dout * sizeof(double), cudaMemcpyHostToDevice, s));
-    {
-        sp_run_args a;
-        memset(&a, 0, sizeof(a));
-        a.u = h_u;
-        a.T = T;
-        a.d_phi = Phi;
-        a.sync = 1;
-        rc = sp_dev_run(d, &a);
-        if (rc)
-            goto out;
-    }
-    rep->collect_ms = ms_since(tstart);
 
     {
         auto tg = std::chrono::steady_clock::now();
@@ -739,9 +720,7 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
             k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, lambda);
             int lbad = lu_factor_solve(s, A, n, piv, info, W, dout);
             if (lbad) {
-                // singular: the reference leaves W_out unchanged and warns
-                fprintf(stderr, "Warning: Ridge regression failed (singular system).\n");
-                rc = SP_OK;
+                rc = SP_RIDGE_SINGULAR;
                 goto out;
             }
         } else {
@@ -768,8 +747,6 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
             const size_t tot = (size_t)n * dout;
             k_axpy<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, R, tot);
             ++it;
-            if (rep->gram_mode_used == 0 && it >= 2)
-                ; /* FP64 Gram: refinement converges in one or two sweeps */
         }
         rep->refine_iters = it;
         rep->rel_residual = rel;
@@ -778,18 +755,72 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
 
     {
         const size_t tot = (size_t)n * dout;
-        // W (n x dout) -> W_out (dout x n) in R, host mirror, position-space copy
-        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, R);
-        RK(cudaMemcpyAsync(h_W_out, R, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
-        rc = sp_dev_w_out_from_nat(d, R);
-        if (rc)
-            goto out;
+        // W (n x dout) -> W_out (dout x n)
+        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, d_W_out);
         RK(cudaStreamSynchronize(s));
         RK(cudaGetLastError());
     }
 out:
     cudaStreamSynchronize(s);
-    void *bufs[] = {Phi, Y, A, Aw, B, W, R, E, part, tmp, info, piv};
+    void *bufs[] = {A, Aw, B, W, R, E, part, tmp, info, piv};
+    for (void *b : bufs)
+        if (b)
+            cudaFree(b);
+    return rc;
+}
+
+extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,
+                                  const double *h_y, size_t T, double lambda,
+                                  const sp_ridge_opts *o, sp_ridge_report *rep, double *h_W_out)
+{
+    int rc = SP_OK;
+    const int n = d->n, dout = d->dout;
+    cudaStream_t s = d->stream;
+    double *Phi = nullptr, *Y = nullptr, *Wt = nullptr;
+    memset(rep, 0, sizeof(*rep));
+    if (dout == 0)
+        return SP_OK;
+    if (dout > 16)
+        return SP_EINVAL;
+    auto tstart = std::chrono::steady_clock::now();
+
+    rc = sp_dev_reset_neurons(d, m);
+    if (rc)
+        return rc;
+    RK(cudaMalloc(&Phi, (T ? T : 1) * (size_t)n * sizeof(double)));
+    RK(cudaMalloc(&Y, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(cudaMalloc(&Wt, (size_t)n * dout * sizeof(double)));
+    RK(cudaMemcpyAsync(Y, h_y, T * dout * sizeof(double), cudaMemcpyHostToDevice, s));
+    {
+        sp_run_args a;
+        memset(&a, 0, sizeof(a));
+        a.u = h_u;
+        a.T = T;
+        a.d_phi = Phi;
+        a.sync = 1;
+        rc = sp_dev_run(d, &a);
+        if (rc)
+            goto out;
+    }
+    rep->collect_ms = ms_since(tstart);
+    rc = sp_ridge_phi(s, Phi, n, T, Y, dout, lambda, o, rep, Wt);
+    if (rc == SP_RIDGE_SINGULAR) {
+        // singular: the reference leaves W_out unchanged and warns
+        fprintf(stderr, "Warning: Ridge regression failed (singular system).\n");
+        rc = SP_OK;
+        goto out;
+    }
+    if (rc)
+        goto out;
+    RK(cudaMemcpyAsync(h_W_out, Wt, (size_t)n * dout * sizeof(double), cudaMemcpyDeviceToHost, s));
+    rc = sp_dev_w_out_from_nat(d, Wt);
+    if (rc)
+        goto out;
+    RK(cudaStreamSynchronize(s));
+    RK(cudaGetLastError());
+out:
+    cudaStreamSynchronize(s);
+    void *bufs[] = {Phi, Y, Wt};
     for (void *b : bufs)
         if (b)
             cudaFree(b);

@@ -359,8 +359,8 @@ static void default_launch(sp_dev *d)
 // (longest-processing-time assignment), lanes filled from 0. Every warp, and
 // so every CTA, ends up with about the same number of edges to walk.
 // pos_of[i] = position of neuron i, nid_of[q] = neuron at position q or -1.
-static void make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
-                        std::vector<int> &nid_of)
+void sp_make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
+                    std::vector<int> &nid_of)
 {
     const int n = (int)m->n;
     std::vector<int> order(n);
@@ -440,7 +440,7 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         const size_t n = m->n, rs = (size_t)d->rs, din = m->din, dout = m->dout;
         cudaStream_t s = d->stream;
         std::vector<int> pos_of, nid_of;
-        make_layout(m, d->nw, pos_of, nid_of);
+        sp_make_layout(m, d->nw, pos_of, nid_of);
         // CSR in position order: row q = neuron nid_of[q], edges in their original
         // order, column index mapped to the presynaptic neuron's position
         std::vector<long long> rp(rs + 1, 0);
@@ -685,6 +685,40 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     return SP_OK;
 }
 
+
+// Stream-level launchers of the layout kernels for callers that hold raw
+// device pointers (the batched path).
+extern "C" int sp_launch_readout(cudaStream_t s, const double *W_pos, const double *X, int rs,
+                                 size_t T, int dout, double *Y)
+{
+    if (T == 0 || dout == 0)
+        return SP_OK;
+    dim3 grid((unsigned)T, (unsigned)dout);
+    k_readout<<<grid, 256, 0, s>>>(W_pos, X, rs, dout, Y);
+    SP_CK(cudaGetLastError());
+    return SP_OK;
+}
+
+extern "C" int sp_launch_gather_rows(cudaStream_t s, const double *pos_rows, int rs,
+                                     const int *pos_of, int n, size_t T, double *nat_rows)
+{
+    if (T == 0 || n == 0)
+        return SP_OK;
+    k_gather_rows<<<gather_blocks(T * n), 256, 0, s>>>(pos_rows, rs, pos_of, n, T, nat_rows);
+    SP_CK(cudaGetLastError());
+    return SP_OK;
+}
+
+extern "C" int sp_launch_wout_to_pos(cudaStream_t s, const double *w_nat, const int *nid_of, int n,
+                                     int rs, int dout, double *w_pos)
+{
+    if (dout == 0)
+        return SP_OK;
+    k_wout_to_pos<<<gather_blocks((size_t)dout * rs), 256, 0, s>>>(w_nat, nid_of, n, rs, dout,
+                                                                    w_pos);
+    SP_CK(cudaGetLastError());
+    return SP_OK;
+}
 
 extern "C" int sp_dev_readout(sp_dev *d, const double *X, size_t T, double *Y)
 {

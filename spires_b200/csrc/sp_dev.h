@@ -98,6 +98,21 @@ int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double *h_u,
 int sp_dev_train_online(sp_dev *d, const double *h_target, double lr,
                         double *h_W_out);
 
+/* Batched multi-reservoir path (dev_batch.cu): LIF_DISCRETE / FLIF_GL with
+ * SIMPLE synapses. sp_batch_create takes over the models' buffers (the array
+ * is zeroed). Every run starts all instances from their reset state. */
+typedef struct sp_batch sp_batch;
+int  sp_batch_create(sp_host_model *models, size_t count, sp_batch **out);
+void sp_batch_destroy(sp_batch *b);
+int  sp_batch_run(sp_batch *b, const double *const *u, const size_t *T,
+                  uint32_t *const *raster, double *const *final_state, double *elapsed_ms);
+int  sp_batch_train_ridge(sp_batch *b, const double *const *u, const double *const *y,
+                          const size_t *T, const double *lambda, const sp_ridge_opts *o,
+                          double *const *w_out, double *elapsed_ms);
+int  sp_batch_predict(sp_batch *b, const double *const *u, const size_t *T,
+                      double *const *y, double *elapsed_ms);
+int  sp_batch_info(const sp_batch *b, int *ctas, int *groups, int *graph);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,7 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <vector>
 #include "sp_dev.h"
 
 struct sp_dev {
@@ -74,3 +75,21 @@ extern "C" void sp_dev_note_error(const char *what, int code);
 extern "C" int sp_dev_gather_rows(sp_dev *d, const double *pos_rows, size_t T, double *nat_rows);
 extern "C" int sp_dev_w_out_from_nat(sp_dev *d, const double *dev_w_nat);
 extern "C" int sp_dev_w_out_to_nat(sp_dev *d, double *dev_w_nat);
+
+// Position layout shared by the single and batched paths (dev_reservoir.cu).
+void sp_make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
+                    std::vector<int> &nid_of);
+
+// Ridge on a device Phi [T x n] (neuron order) and targets Y [T x dout];
+// writes d_W_out [dout x n] or returns SP_RIDGE_SINGULAR (dev_readout.cu).
+extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
+                            const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                            sp_ridge_report *rep, double *d_W_out);
+
+// Layout kernels on raw device pointers (dev_reservoir.cu).
+extern "C" int sp_launch_readout(cudaStream_t s, const double *W_pos, const double *X, int rs,
+                                 size_t T, int dout, double *Y);
+extern "C" int sp_launch_gather_rows(cudaStream_t s, const double *pos_rows, int rs,
+                                     const int *pos_of, int n, size_t T, double *nat_rows);
+extern "C" int sp_launch_wout_to_pos(cudaStream_t s, const double *w_nat, const int *nid_of, int n,
+                                     int rs, int dout, double *w_pos);

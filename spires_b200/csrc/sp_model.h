@@ -93,7 +93,7 @@ typedef struct sp_host_model {
 } sp_host_model;
 
 /* status codes mirror spires_status */
-enum { SP_OK = 0, SP_EINVAL = 1, SP_EALLOC = 2, SP_EINTERNAL = 3 };
+enum { SP_OK = 0, SP_EINVAL = 1, SP_EALLOC = 2, SP_EINTERNAL = 3, SP_RIDGE_SINGULAR = 100 };
 
 /* construct.c */
 int  sp_validate_config(size_t n, size_t din, size_t dout, double dt, int conn_type,
