@@ -89,6 +89,15 @@ spires_status spires_ext_autotune(spires_reservoir *r, size_t steps);
  * stream derived from seed and i). Takes effect at the next reset. */
 spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed);
 
+/* ---- spectral radius ------------------------------------------------------
+ * The max-abs normalised power iteration that scales the recurrent weights at
+ * create time (reference src/sparse.c:93-127) on an n x n CSR matrix with
+ * ascending columns: on the current CUDA device (on_device = 1) or on the
+ * host (0). Both give the same bits; spires_reservoir_create uses the device
+ * for matrices with at least 2^18 edges unless SPIRES_HOST_SPECTRAL_RADIUS=1. */
+spires_status spires_ext_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
+                                         const double *w, int on_device, double *out);
+
 /* ---- ridge readout with options ------------------------------------------ */
 typedef enum {
     SPIRES_EXT_GRAM_FP64 = 0,      /* FP64 Gram (CUDA cores) */

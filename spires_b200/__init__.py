@@ -163,6 +163,7 @@ EXT_SIGNATURES = {
                                             C.POINTER(AgileOpts), _dp, C.POINTER(AgileReport)]),
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
                                                  C.c_size_t, C.c_double, _VP, _VP]),
+    "spires_ext_spectral_radius": (C.c_int, [C.c_size_t, _i64p, _i32p, _dp, C.c_int, _dp]),
     "spires_ext_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_uint), C.c_size_t,
                                           C.POINTER(_VP)]),
     "spires_ext_batch_destroy": (None, [_VP]),

@@ -321,6 +321,7 @@ SPIRES_EXPORT spires_status spires_ext_model_build(const spires_reservoir_config
     if (!h)
         return SPIRES_ERR_ALLOC;
     int rc = model_from_config(cfg, &h->m);
+    h->m.host_only = 1; /* inspection builds never touch a GPU */
     if (!rc)
         rc = sp_model_build(&h->m);
     if (rc) {
@@ -667,4 +668,16 @@ SPIRES_EXPORT spires_status spires_ext_batch_info(const spires_ext_batch *b, int
     if (!b)
         return SPIRES_ERR_INVALID_ARG;
     return to_status(sp_batch_info(b->b, ctas, groups, graph));
+}
+
+SPIRES_EXPORT spires_status spires_ext_spectral_radius(size_t n, const int64_t *row_ptr,
+                                                       const int32_t *col, const double *w,
+                                                       int on_device, double *out)
+{
+    if (!row_ptr || !out || (row_ptr[n] > 0 && (!col || !w)))
+        return SPIRES_ERR_INVALID_ARG;
+    if (on_device)
+        return to_status(sp_dev_spectral_radius(n, row_ptr, col, w, out));
+    *out = sp_csr_spectral_radius(n, row_ptr, col, w);
+    return SPIRES_OK;
 }

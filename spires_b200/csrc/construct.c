@@ -273,11 +273,14 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
     int32_t *eu = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
     int32_t *ev = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
     int32_t *picks = malloc((size_t)mm * sizeof(int32_t));
+    int64_t *stamp = malloc(n * sizeof(int64_t)); /* stamp[u] = last v that picked u */
     int64_t *adj_off = NULL;
     int32_t *adj = NULL;
     size_t ne = 0;
-    if (!deg || !fw.t || !eu || !ev || !picks)
+    if (!deg || !fw.t || !eu || !ev || !picks || !stamp)
         goto done;
+    for (size_t u = 0; u < n; u++)
+        stamp[u] = -1;
 
     /* seed clique on m0 nodes */
     for (int u = 0; u < m0; u++)
@@ -311,11 +314,9 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
                 size_t u = fw_lower_bound(&fw, (int64_t)cr);
                 pick = (u < v) ? u : 0; /* no u satisfies: pick stays 0 */
             }
-            int dup = 0;
-            for (int a = 0; a < added; a++)
-                if (picks[a] == (int32_t)pick)
-                    dup = 1;
+            const int dup = stamp[pick] == (int64_t)v; /* already picked for v */
             if (pick != v && !dup) {
+                stamp[pick] = (int64_t)v;
                 picks[added++] = (int32_t)pick;
                 deg[v]++;
                 deg[pick]++;
@@ -328,11 +329,9 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
             size_t pick = (size_t)(urand01() * (double)v);
             if (pick >= v)
                 pick = v - 1;
-            int dup = 0;
-            for (int a = 0; a < added; a++)
-                if (picks[a] == (int32_t)pick)
-                    dup = 1;
+            const int dup = stamp[pick] == (int64_t)v; /* already picked for v */
             if (pick != v && !dup) {
+                stamp[pick] = (int64_t)v;
                 picks[added++] = (int32_t)pick;
                 deg[v]++;
                 deg[pick]++;
@@ -396,6 +395,7 @@ done:
     free(eu);
     free(ev);
     free(picks);
+    free(stamp);
     free(adj_off);
     free(adj);
     return rc;
@@ -405,6 +405,9 @@ done:
 
 /* csr_spectral_radius, src/sparse.c:93-127 (max-abs normalised power
  * iteration, tol 1e-6, at most 1000 iterations, x0 = 1). */
+/* edge count from which the power iteration runs on the device */
+#define SP_DEVICE_SR_MIN_NNZ ((size_t)1 << 18)
+
 double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
                               const double *w)
 {
@@ -420,7 +423,12 @@ double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *c
     for (size_t i = 0; i < n; i++)
         x[i] = 1.0;
     double lambda_old = 0.0, lambda_new = 0.0;
+    /* Rows are independent and each row sums in ascending edge order, and the
+     * maximum is exact in any order, so splitting the rows over threads gives
+     * the same bits as the serial loop. */
+    const int par = row_ptr[n] > 65536;
     for (unsigned int it = 0; it < max_iter; it++) {
+#pragma omp parallel for schedule(static) if (par)
         for (size_t i = 0; i < n; i++) {
             double s = 0.0;
             for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++)
@@ -433,6 +441,7 @@ double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *c
             if (a > lambda_new)
                 lambda_new = a;
         }
+#pragma omp parallel for schedule(static) if (par)
         for (size_t i = 0; i < n; i++)
             x[i] = y[i] / lambda_new;
         if (fabs(lambda_new - lambda_old) < tol)
@@ -808,7 +817,12 @@ int sp_model_build(sp_host_model *m)
         return rc;
 
     /* rescale_weights, src/reservoir.c:548-557 */
-    double sr = sp_csr_spectral_radius(n, m->row_ptr, m->col, m->w);
+    /* large matrices: the device runs the same iteration bit for bit */
+    double sr = 0.0;
+    const char *host_env = getenv("SPIRES_HOST_SPECTRAL_RADIUS");
+    if (m->host_only || m->nnz < SP_DEVICE_SR_MIN_NNZ || (host_env && host_env[0] == '1') ||
+        sp_dev_spectral_radius(n, m->row_ptr, m->col, m->w, &sr) != SP_OK)
+        sr = sp_csr_spectral_radius(n, m->row_ptr, m->col, m->w);
     m->spectral_radius_before = sr;
     if (sr > 1e-9) {
         double f = m->spectral_radius / sr;

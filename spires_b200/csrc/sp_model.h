@@ -90,6 +90,9 @@ typedef struct sp_host_model {
     /* diagnostics from construction */
     double spectral_radius_before;  /* power-iteration estimate before rescale */
     uint64_t diffusive_seed;        /* FLIF_DIFFUSIVE per-reservoir seed */
+
+    /* construction policy: 1 = never use the GPU (spires_ext_model_build) */
+    int host_only;
 } sp_host_model;
 
 /* status codes mirror spires_status */
@@ -102,6 +105,10 @@ int  sp_validate_config(size_t n, size_t din, size_t dout, double dt, int conn_t
 int  sp_model_build(sp_host_model *m);          /* fills weights, consumes rand() */
 int  sp_model_derive_neuron(sp_host_model *m);  /* re-reads neuron_params (create and reset) */
 void sp_model_free(sp_host_model *m);
+/* The same power iteration on the current CUDA device, bit-identical to
+ * sp_csr_spectral_radius (dev_construct.cu); non-zero status = not done. */
+int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
+                           const double *w, double *out);
 double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
                               const double *w);
 int  sp_model_build_synapse(sp_host_model *m, const double *dense_or_null);
