@@ -36,6 +36,11 @@ typedef struct {
 
 spires_status spires_ext_model_build(const spires_reservoir_config *cfg,
                                      spires_ext_model **out);
+/* As spires_ext_model_build after srand(seed), but drawing from a private
+ * generator with the same sequence as glibc's srand(seed) + rand(): the global
+ * rand() state is left alone and several threads may build at once. */
+spires_status spires_ext_model_build_seeded(const spires_reservoir_config *cfg, unsigned seed,
+                                            spires_ext_model **out);
 void          spires_ext_model_free(spires_ext_model *m);
 spires_status spires_ext_model_info_get(const spires_ext_model *m,
                                         spires_ext_model_info *info);
@@ -182,7 +187,10 @@ spires_status spires_ext_ridge_solve_noalloc(const double *d_states, const doubl
  * holds `count` reservoirs of uneven size, ring length, series length and
  * model; instance k is built exactly as spires_reservoir_create builds it
  * after srand(seeds[k]), so its weights, and its spike rasters and states from
- * reset, are bit-identical to those of a separately created reservoir.
+ * reset, are bit-identical to those of a separately created reservoir. With
+ * seeds, the instances are built on all host threads from private generators
+ * with glibc's srand/rand sequence and the global rand() state is untouched;
+ * seeds = NULL draws every instance from the global rand() in turn.
  * Supported: SPIRES_NEURON_LIF_DISCRETE and SPIRES_NEURON_FLIF_GL with
  * SPIRES_SYNAPSE_SIMPLE, num_outputs <= 16; anything else returns
  * SPIRES_ERR_INVALID_ARG. Every call starts all instances from their reset

@@ -139,6 +139,7 @@ SIGNATURES = {
 }
 EXT_SIGNATURES = {
     "spires_ext_model_build": (C.c_int, [C.POINTER(Config), C.POINTER(_VP)]),
+    "spires_ext_model_build_seeded": (C.c_int, [C.POINTER(Config), C.c_uint, C.POINTER(_VP)]),
     "spires_ext_model_free": (None, [_VP]),
     "spires_ext_model_info_get": (C.c_int, [_VP, C.POINTER(ModelInfo)]),
     "spires_ext_model_csr": (C.c_int, [_VP, _i64p, _i32p, _dp]),
@@ -353,12 +354,19 @@ class Reservoir:
 class HostModel:
     """spires_ext_model: construction only, no GPU."""
 
-    def __init__(self, cfg: Config, seed: int | None = None, lib: C.CDLL | None = None):
+    def __init__(self, cfg: Config, seed: int | None = None, lib: C.CDLL | None = None,
+                 private: bool = False):
+        """private=True draws from a private generator with the srand(seed) +
+        rand() sequence instead of seeding the global one."""
         self.lib = lib or load()
-        if seed is not None:
-            libc.srand(seed)
         h = C.c_void_p()
-        st = self.lib.spires_ext_model_build(C.byref(cfg), C.byref(h))
+        if private:
+            st = self.lib.spires_ext_model_build_seeded(C.byref(cfg), int(seed or 0) & 0xFFFFFFFF,
+                                                        C.byref(h))
+        else:
+            if seed is not None:
+                libc.srand(seed)
+            st = self.lib.spires_ext_model_build(C.byref(cfg), C.byref(h))
         if st != SPIRES_OK:
             raise RuntimeError(f"spires_ext_model_build failed: {st}")
         self.h = h

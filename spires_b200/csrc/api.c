@@ -576,21 +576,32 @@ SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_confi
         return SPIRES_ERR_ALLOC;
     }
     int rc = SP_OK;
-    size_t built = 0;
-    for (; built < count && !rc; ++built) {
-        const spires_reservoir_config *c = &cfgs[built];
-        if (!dt_ok(c->dt)) {
-            rc = SP_EINVAL;
-            break;
+    if (seeds) {
+        /* independent private generators: instances build on all host threads */
+        const int dev = sp_dev_current_device();
+        int *rcs = calloc(count, sizeof(int));
+        if (!rcs) {
+            free(ms);
+            free(h);
+            return SPIRES_ERR_ALLOC;
         }
-        if (seeds)
-            srand(seeds[built]);
-        rc = model_from_config(c, &ms[built]);
-        if (!rc)
-            rc = sp_model_build(&ms[built]);
-        if (rc) {
-            sp_model_free(&ms[built]);
-            break;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t k = 0; k < count; ++k) {
+            sp_dev_use_device(dev);
+            int r = model_from_config(&cfgs[k], &ms[k]);
+            if (!r)
+                r = sp_model_build_seeded(&ms[k], seeds[k]);
+            rcs[k] = r;
+        }
+        for (size_t k = 0; k < count && !rc; ++k)
+            rc = rcs[k];
+        free(rcs);
+    } else {
+        /* one global rand() sequence, as count consecutive creates */
+        for (size_t k = 0; k < count && !rc; ++k) {
+            rc = model_from_config(&cfgs[k], &ms[k]);
+            if (!rc)
+                rc = sp_model_build(&ms[k]);
         }
     }
     if (!rc)
@@ -679,5 +690,26 @@ SPIRES_EXPORT spires_status spires_ext_spectral_radius(size_t n, const int64_t *
     if (on_device)
         return to_status(sp_dev_spectral_radius(n, row_ptr, col, w, out));
     *out = sp_csr_spectral_radius(n, row_ptr, col, w);
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_model_build_seeded(const spires_reservoir_config *cfg,
+                                                          unsigned seed, spires_ext_model **out)
+{
+    if (!cfg || !out)
+        return SPIRES_ERR_INVALID_ARG;
+    spires_ext_model *h = calloc(1, sizeof(*h));
+    if (!h)
+        return SPIRES_ERR_ALLOC;
+    int rc = model_from_config(cfg, &h->m);
+    h->m.host_only = 1;
+    if (!rc)
+        rc = sp_model_build_seeded(&h->m, seed);
+    if (rc) {
+        sp_model_free(&h->m);
+        free(h);
+        return to_status(rc);
+    }
+    *out = h;
     return SPIRES_OK;
 }

@@ -29,14 +29,55 @@
 
 /* ---------------------------------------------------------------- draws -- */
 
+/* Private generator with the sequence of glibc's srand(seed) + rand():
+ * the additive lagged-Fibonacci generator of glibc's random_r (TYPE_3,
+ * degree 31, separation 3): r[0] = seed (0 becomes 1), r[i] = 16807 r[i-1]
+ * mod (2^31 - 1) for i < 31 (Schrage's decomposition, on signed 32-bit words
+ * as glibc keeps them), then r[f] += r[b] modulo 2^32 with the front index
+ * three ahead of the back one, output r[f] >> 1, and the first 310 outputs
+ * discarded. It lets worker threads build independently seeded reservoirs at
+ * the same time, each drawing what srand(seed) + rand() would give it. */
+void sp_rand_seed(sp_rand_state *s, unsigned seed)
+{
+    int32_t word = (int32_t)(seed == 0 ? 1u : seed);
+    s->r[0] = word;
+    for (int i = 1; i < 31; i++) {
+        const long hi = word / 127773, lo = word % 127773; /* 127773 = m / 16807 */
+        long v = 16807 * lo - 2836 * hi;                   /* 2836 = m % 16807 */
+        if (v < 0)
+            v += 2147483647;
+        word = (int32_t)v;
+        s->r[i] = word;
+    }
+    s->f = 3;
+    s->b = 0;
+    for (int i = 0; i < 310; i++)
+        (void)sp_rand_next(s);
+}
+
+int sp_rand_next(sp_rand_state *s)
+{
+    const uint32_t v = (uint32_t)s->r[s->f] + (uint32_t)s->r[s->b];
+    s->r[s->f] = (int32_t)v;
+    s->f = s->f == 30 ? 0 : s->f + 1;
+    s->b = s->b == 30 ? 0 : s->b + 1;
+    return (int)(v >> 1);
+}
+
+/* The draw source of the current thread's build: the C library's rand()
+ * (the reference behaviour) unless sp_model_build_seeded installed a private
+ * generator. */
+static __thread sp_rand_state *tl_rng;
+static int draw_int(void) { return tl_rng ? sp_rand_next(tl_rng) : rand(); }
+
 /* (double)rand()/RAND_MAX, src/reservoir.c:330-333 */
-static double urand01(void) { return (double)rand() / (double)RAND_MAX; }
+static double urand01(void) { return (double)draw_int() / (double)RAND_MAX; }
 
 /* magnitude first, then the sign draw; src/reservoir.c:308-317 */
 static double draw_weight(double ei_ratio)
 {
-    double magnitude = (double)rand() / RAND_MAX;
-    if (((double)rand() / RAND_MAX) < ei_ratio)
+    double magnitude = (double)draw_int() / RAND_MAX;
+    if (((double)draw_int() / RAND_MAX) < ei_ratio)
         return magnitude;
     return -magnitude;
 }
@@ -900,4 +941,15 @@ int sp_model_set_dense_weights(sp_host_model *m, const double *dense)
     m->row_ptr[n] = (int64_t)idx;
     m->nnz = nnz;
     return sp_model_build_synapse(m, NULL);
+}
+
+int sp_model_build_seeded(sp_host_model *m, unsigned seed)
+{
+    sp_rand_state st;
+    sp_rand_seed(&st, seed);
+    sp_rand_state *prev = tl_rng;
+    tl_rng = &st;
+    const int rc = sp_model_build(m);
+    tl_rng = prev;
+    return rc;
 }

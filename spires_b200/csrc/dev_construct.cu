@@ -189,3 +189,20 @@ extern "C" int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const in
     cudaStreamDestroy(s);
     return rc;
 }
+
+// Device selection for host worker threads (a new thread starts on device 0).
+extern "C" int sp_dev_current_device(void)
+{
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return d;
+}
+
+extern "C" void sp_dev_use_device(int d)
+{
+    if (d >= 0 && cudaSetDevice(d) != cudaSuccess)
+        cudaGetLastError();
+}

@@ -98,6 +98,11 @@ int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double *h_u,
 int sp_dev_train_online(sp_dev *d, const double *h_target, double lr,
                         double *h_W_out);
 
+/* Current CUDA device of the calling thread (-1 = none) and selection of it
+ * on a worker thread. */
+int  sp_dev_current_device(void);
+void sp_dev_use_device(int d);
+
 /* Batched multi-reservoir path (dev_batch.cu): LIF_DISCRETE / FLIF_GL with
  * SIMPLE synapses. sp_batch_create takes over the models' buffers (the array
  * is zeroed). Every run starts all instances from their reset state. */

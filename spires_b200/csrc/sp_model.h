@@ -105,6 +105,19 @@ int  sp_validate_config(size_t n, size_t din, size_t dout, double dt, int conn_t
 int  sp_model_build(sp_host_model *m);          /* fills weights, consumes rand() */
 int  sp_model_derive_neuron(sp_host_model *m);  /* re-reads neuron_params (create and reset) */
 void sp_model_free(sp_host_model *m);
+/* Private generator with glibc's srand(seed) + rand() sequence (construct.c). */
+typedef struct {
+    int32_t r[31];
+    int f, b;
+} sp_rand_state;
+void sp_rand_seed(sp_rand_state *s, unsigned seed);
+int  sp_rand_next(sp_rand_state *s);
+
+/* sp_model_build drawing from a private generator seeded with `seed` instead
+ * of the global rand(): the same model as srand(seed) + sp_model_build, and
+ * safe to run on several threads at once. */
+int sp_model_build_seeded(sp_host_model *m, unsigned seed);
+
 /* The same power iteration on the current CUDA device, bit-identical to
  * sp_csr_spectral_radius (dev_construct.cu); non-zero status = not done. */
 int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,

@@ -74,3 +74,26 @@ def test_invalid_configs_rejected():
         cfg = sp.make_config(10, **kw)
         assert lib.spires_ext_model_build(C.byref(cfg), C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
     assert lib.spires_reservoir_create(None, C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
+
+
+# ---- private generator with the srand/rand sequence (parallel batch builds)
+@pytest.mark.parametrize("seed", [0, 1, 42, 2**31 - 1, 2**31 + 5, 2**32 - 1])
+@pytest.mark.parametrize("topo", [sp.CONN_RANDOM, sp.CONN_SMALL_WORLD, sp.CONN_SCALE_FREE])
+def test_private_generator_matches_global_rand(seed, topo):
+    cfg = sp.make_config(150, 2, 3, rho=1.1, ei=0.6, conn=0.07, topo=topo, neuron=sp.FLIF_GL,
+                         nparams=(1.0, 0.0, 0.0, 20.0, 0.7, 32.0, 0.1, 2.0))
+    a = sp.HostModel(cfg, seed=seed)
+    b = sp.HostModel(cfg, seed=seed, private=True)
+    for x, y in zip(a.csr(), b.csr()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.w_in(), b.w_in())
+    assert np.array_equal(a.w_out(), b.w_out())
+
+
+def test_private_generator_leaves_global_rand_alone():
+    sp.libc.srand(7)
+    first = sp.libc.rand()
+    sp.libc.srand(7)
+    cfg = sp.make_config(64, 1, 1, conn=0.1)
+    sp.HostModel(cfg, seed=99, private=True)
+    assert sp.libc.rand() == first
