@@ -233,6 +233,36 @@ spires_status spires_ext_batch_predict(spires_ext_batch *b, const double *const 
 spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas, int *groups,
                                     int *graph);
 
+/* ---- surrogate network of the hyper-parameter search ----------------------
+ * No counterpart in the reference. An MLP 10 -> 128 -> 128 -> 2 (GELU) that
+ * predicts the mean and log-variance of a candidate's full-fidelity
+ * log-NRMSE from 10 features (hyper-parameters and its low-fidelity loss),
+ * trained on the GPU by hand-written forward, backward and Adam kernels on the
+ * Gaussian negative log-likelihood 0.5 (v + (y - m)^2 exp(-v)) averaged over
+ * the rows. FP32 parameters (layout: W1[128][10], b1[128], W2[128][128],
+ * b2[128], W3[2][128], b3[2]); X is row-major n x 10; host arrays throughout. */
+typedef struct spires_ext_mlp spires_ext_mlp;
+
+size_t        spires_ext_mlp_num_params(void);
+spires_status spires_ext_mlp_create(uint64_t seed, spires_ext_mlp **out);
+void          spires_ext_mlp_destroy(spires_ext_mlp *m);
+spires_status spires_ext_mlp_get_params(spires_ext_mlp *m, float *params);
+/* also clears the Adam moments */
+spires_status spires_ext_mlp_set_params(spires_ext_mlp *m, const float *params);
+/* NLL over the n rows and its gradient (grad may be NULL); parameters unchanged */
+spires_status spires_ext_mlp_loss_grad(spires_ext_mlp *m, const float *X, const float *y,
+                                       size_t n, float *loss, float *grad);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) over `epochs` seeded shuffles in
+ * minibatches of `batch` rows; final_loss = NLL of the last minibatch */
+spires_status spires_ext_mlp_train(spires_ext_mlp *m, const float *X, const float *y, size_t n,
+                                   int epochs, int batch, float lr, uint64_t seed,
+                                   float *final_loss);
+/* mean / logvar per row (either may be NULL); bf16 = 1: BF16 weights and
+ * activations with FP32 accumulation */
+spires_status spires_ext_mlp_predict(spires_ext_mlp *m, const float *X, size_t n, int bf16,
+                                     float *mean, float *logvar);
+long long     spires_ext_mlp_kernel_launches(const spires_ext_mlp *m);
+
 #ifdef __cplusplus
 }
 #endif

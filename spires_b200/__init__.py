@@ -27,6 +27,7 @@ BACKEND_SPARSE, BACKEND_DENSE = range(2)
 _dp = C.POINTER(C.c_double)
 _u32p = C.POINTER(C.c_uint32)
 _i64p = C.POINTER(C.c_int64)
+_fp = C.POINTER(C.c_float)
 _i32p = C.POINTER(C.c_int32)
 
 
@@ -165,6 +166,16 @@ EXT_SIGNATURES = {
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
                                                  C.c_size_t, C.c_double, _VP, _VP]),
     "spires_ext_spectral_radius": (C.c_int, [C.c_size_t, _i64p, _i32p, _dp, C.c_int, _dp]),
+    "spires_ext_mlp_num_params": (C.c_size_t, []),
+    "spires_ext_mlp_create": (C.c_int, [C.c_uint64, C.POINTER(_VP)]),
+    "spires_ext_mlp_destroy": (None, [_VP]),
+    "spires_ext_mlp_get_params": (C.c_int, [_VP, _fp]),
+    "spires_ext_mlp_set_params": (C.c_int, [_VP, _fp]),
+    "spires_ext_mlp_loss_grad": (C.c_int, [_VP, _fp, _fp, C.c_size_t, _fp, _fp]),
+    "spires_ext_mlp_train": (C.c_int, [_VP, _fp, _fp, C.c_size_t, C.c_int, C.c_int, C.c_float,
+                                       C.c_uint64, _fp]),
+    "spires_ext_mlp_predict": (C.c_int, [_VP, _fp, C.c_size_t, C.c_int, _fp, _fp]),
+    "spires_ext_mlp_kernel_launches": (C.c_longlong, [_VP]),
     "spires_ext_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_uint), C.c_size_t,
                                           C.POINTER(_VP)]),
     "spires_ext_batch_destroy": (None, [_VP]),
@@ -509,6 +520,74 @@ class Batch:
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         self.lib.spires_ext_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c))
         return {"ctas": a.value, "groups": b.value, "graph": c.value}
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_fp)
+
+
+class Surrogate:
+    """spires_ext_mlp: the 10 -> 128 -> 128 -> 2 surrogate on the GPU."""
+
+    IN = 10
+
+    def __init__(self, seed: int = 0, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+        h = C.c_void_p()
+        st = self.lib.spires_ext_mlp_create(seed, C.byref(h))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_mlp_create failed: {st}")
+        self.h = h
+        self.num_params = int(self.lib.spires_ext_mlp_num_params())
+
+    def close(self):
+        if self.h:
+            self.lib.spires_ext_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        p = np.empty(self.num_params, np.float32)
+        assert self.lib.spires_ext_mlp_get_params(self.h, fptr(p)) == SPIRES_OK
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert self.lib.spires_ext_mlp_set_params(self.h, fptr(p)) == SPIRES_OK
+
+    def loss_grad(self, X, y):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.empty(self.num_params, np.float32)
+        st = self.lib.spires_ext_mlp_loss_grad(self.h, fptr(X), fptr(y), X.shape[0], fptr(loss),
+                                               fptr(g))
+        assert st == SPIRES_OK, st
+        return float(loss[0]), g
+
+    def train(self, X, y, epochs=50, batch=256, lr=1e-3, seed=0):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = np.zeros(1, np.float32)
+        st = self.lib.spires_ext_mlp_train(self.h, fptr(X), fptr(y), X.shape[0], epochs, batch,
+                                           lr, seed, fptr(loss))
+        assert st == SPIRES_OK, st
+        return float(loss[0])
+
+    def predict(self, X, bf16=True):
+        X = np.ascontiguousarray(X, np.float32)
+        m = np.empty(X.shape[0], np.float32)
+        v = np.empty(X.shape[0], np.float32)
+        st = self.lib.spires_ext_mlp_predict(self.h, fptr(X), X.shape[0], int(bf16), fptr(m),
+                                             fptr(v))
+        assert st == SPIRES_OK, st
+        return m, v
 
 
 def unpack_raster(R: np.ndarray, n: int) -> np.ndarray:

@@ -713,3 +713,80 @@ SPIRES_EXPORT spires_status spires_ext_model_build_seeded(const spires_reservoir
     *out = h;
     return SPIRES_OK;
 }
+
+/* ---- surrogate MLP ---------------------------------------------------------- */
+struct spires_ext_mlp {
+    sp_mlp *m;
+};
+
+SPIRES_EXPORT size_t spires_ext_mlp_num_params(void) { return (size_t)sp_mlp_num_params(); }
+
+SPIRES_EXPORT spires_status spires_ext_mlp_create(uint64_t seed, spires_ext_mlp **out)
+{
+    if (!out)
+        return SPIRES_ERR_INVALID_ARG;
+    *out = NULL;
+    spires_ext_mlp *h = calloc(1, sizeof(*h));
+    if (!h)
+        return SPIRES_ERR_ALLOC;
+    int rc = sp_mlp_create(seed, &h->m);
+    if (rc) {
+        free(h);
+        return to_status(rc);
+    }
+    *out = h;
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT void spires_ext_mlp_destroy(spires_ext_mlp *m)
+{
+    if (!m)
+        return;
+    sp_mlp_destroy(m->m);
+    free(m);
+}
+
+SPIRES_EXPORT spires_status spires_ext_mlp_get_params(spires_ext_mlp *m, float *params)
+{
+    if (!m || !params)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_mlp_get_params(m->m, params));
+}
+
+SPIRES_EXPORT spires_status spires_ext_mlp_set_params(spires_ext_mlp *m, const float *params)
+{
+    if (!m || !params)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_mlp_set_params(m->m, params));
+}
+
+SPIRES_EXPORT spires_status spires_ext_mlp_loss_grad(spires_ext_mlp *m, const float *X,
+                                                     const float *y, size_t n, float *loss,
+                                                     float *grad)
+{
+    if (!m || !X || !y || !loss || n == 0 || n > 1u << 24)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_mlp_loss_grad(m->m, X, y, (int)n, loss, grad));
+}
+
+SPIRES_EXPORT spires_status spires_ext_mlp_train(spires_ext_mlp *m, const float *X, const float *y,
+                                                 size_t n, int epochs, int batch, float lr,
+                                                 uint64_t seed, float *final_loss)
+{
+    if (!m || !X || !y || n == 0 || n > 1u << 24)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_mlp_train(m->m, X, y, (int)n, epochs, batch, lr, seed, final_loss));
+}
+
+SPIRES_EXPORT spires_status spires_ext_mlp_predict(spires_ext_mlp *m, const float *X, size_t n,
+                                                   int bf16, float *mean, float *logvar)
+{
+    if (!m || !X || n == 0 || n > 1u << 24)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_mlp_predict(m->m, X, (int)n, bf16, mean, logvar));
+}
+
+SPIRES_EXPORT long long spires_ext_mlp_kernel_launches(const spires_ext_mlp *m)
+{
+    return m ? sp_mlp_launches(m->m) : 0;
+}

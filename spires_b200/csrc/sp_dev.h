@@ -98,6 +98,20 @@ int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double *h_u,
 int sp_dev_train_online(sp_dev *d, const double *h_target, double lr,
                         double *h_W_out);
 
+/* Surrogate MLP 10 -> 128 -> 128 -> 2 (dev_surrogate.cu). */
+typedef struct sp_mlp sp_mlp;
+int  sp_mlp_num_params(void);
+int  sp_mlp_create(uint64_t seed, sp_mlp **out);
+void sp_mlp_destroy(sp_mlp *m);
+int  sp_mlp_get_params(sp_mlp *m, float *h);
+int  sp_mlp_set_params(sp_mlp *m, const float *h);
+int  sp_mlp_loss_grad(sp_mlp *m, const float *X, const float *y, int n, float *loss,
+                      float *grad);
+int  sp_mlp_train(sp_mlp *m, const float *X, const float *y, int n, int epochs, int batch,
+                  float lr, uint64_t seed, float *final_loss);
+int  sp_mlp_predict(sp_mlp *m, const float *X, int n, int bf16, float *mean, float *logvar);
+long long sp_mlp_launches(const sp_mlp *m);
+
 /* Current CUDA device of the calling thread (-1 = none) and selection of it
  * on a worker thread. */
 int  sp_dev_current_device(void);
