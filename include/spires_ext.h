@@ -159,6 +159,26 @@ spires_status spires_ext_agile_minimize(const double *theta0, const double *lowe
                                         const spires_ext_agile_opts *opts, double *theta_best,
                                         spires_ext_agile_report *report);
 
+/* AGILE in ask/tell form for batched evaluation: `chains` independent
+ * chains (start points theta0[chains][dim], one seed each, or opts->seed for
+ * all when seeds is NULL) advanced in lockstep. ask writes the points every
+ * live chain needs next (at most 2 * chains rows of dim, chain index of each
+ * row in owner) and returns their count, 0 when every chain has finished;
+ * tell takes their losses in the same order. Each chain visits exactly the
+ * points spires_ext_agile_minimize visits with the same options and seed. */
+typedef struct spires_ext_agile_batch spires_ext_agile_batch;
+
+spires_status spires_ext_agile_batch_create(int chains, int dim, const double *theta0,
+                                            const double *lower, const double *upper,
+                                            const spires_ext_agile_opts *opts,
+                                            const uint64_t *seeds,
+                                            spires_ext_agile_batch **out);
+void          spires_ext_agile_batch_destroy(spires_ext_agile_batch *b);
+int           spires_ext_agile_batch_ask(spires_ext_agile_batch *b, double *points, int *owner);
+spires_status spires_ext_agile_batch_tell(spires_ext_agile_batch *b, const double *losses);
+spires_status spires_ext_agile_batch_best(const spires_ext_agile_batch *b, int chain,
+                                          double *theta, spires_ext_agile_report *report);
+
 /* ---- ridge readout without device allocation -----------------------------
  * No counterpart in the reference. For callers that cannot allocate device
  * memory themselves -- a host framework that owns every device buffer through

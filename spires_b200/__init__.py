@@ -166,6 +166,13 @@ EXT_SIGNATURES = {
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
                                                  C.c_size_t, C.c_double, _VP, _VP]),
     "spires_ext_spectral_radius": (C.c_int, [C.c_size_t, _i64p, _i32p, _dp, C.c_int, _dp]),
+    "spires_ext_agile_batch_create": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp,
+                                                C.POINTER(AgileOpts), C.POINTER(C.c_uint64),
+                                                C.POINTER(_VP)]),
+    "spires_ext_agile_batch_destroy": (None, [_VP]),
+    "spires_ext_agile_batch_ask": (C.c_int, [_VP, _dp, C.POINTER(C.c_int)]),
+    "spires_ext_agile_batch_tell": (C.c_int, [_VP, _dp]),
+    "spires_ext_agile_batch_best": (C.c_int, [_VP, C.c_int, _dp, C.POINTER(AgileReport)]),
     "spires_ext_mlp_num_params": (C.c_size_t, []),
     "spires_ext_mlp_create": (C.c_int, [C.c_uint64, C.POINTER(_VP)]),
     "spires_ext_mlp_destroy": (None, [_VP]),

@@ -482,6 +482,326 @@ SPIRES_EXPORT spires_status spires_ext_agile_minimize(const double *theta0, cons
     return SPIRES_OK;
 }
 
+/* ---- AGILE in ask/tell form: many chains advanced in lockstep ---------------
+ * agile_run above drives one chain through a callback. Here each chain is a
+ * state machine with the same arithmetic and the same PCG32 draws in the same
+ * order; a caller asks every live chain for the points it needs next (two for
+ * an SPSA gradient, one for a candidate or refinement step), evaluates them
+ * all together (one batched simulation) and tells the losses back. A chain
+ * driven this way visits exactly the points agile_run visits with the same
+ * options and seed. */
+enum { CH_INIT, CH_EXP_A, CH_EXP_B, CH_REF_A, CH_REF_B, CH_DONE };
+
+typedef struct {
+    int d, state;
+    agile_opts o;
+    double lo[64], hi[64];
+    double th[64], cand[64], g[64], dir[64], tp[64], tm[64], delta[64], best_theta[64];
+    double loss, best, patience, refine_step;
+    int since, iters, evals, best_iter, refined, no_imp, k;
+    uint64_t rng;
+} agile_chain;
+
+/* draws of spsa() before its two evaluations */
+static void chain_spsa_points(agile_chain *c)
+{
+    for (int i = 0; i < c->d; i++) {
+        c->delta[i] = (pcg32_next(&c->rng) & 1) ? 1.0 : -1.0;
+        c->tp[i] = clampd(c->th[i] + c->o.spsa_eps * c->delta[i], c->lo[i], c->hi[i]);
+        c->tm[i] = clampd(c->th[i] - c->o.spsa_eps * c->delta[i], c->lo[i], c->hi[i]);
+    }
+}
+
+/* rest of spsa() after its evaluations */
+static void chain_spsa_grad(agile_chain *c, double fp, double fm)
+{
+    double scale = (fp - fm) / (2.0 * c->o.spsa_eps);
+    for (int i = 0; i < c->d; i++)
+        c->g[i] = scale * c->delta[i];
+}
+
+static void chain_enter_refine(agile_chain *c)
+{
+    c->refined = 1;
+    memcpy(c->th, c->best_theta, (size_t)c->d * sizeof(double));
+    c->loss = c->best;
+    c->no_imp = 0;
+    c->k = 0;
+    if (c->o.refine_max_iters > 0) {
+        c->iters++;
+        chain_spsa_points(c);
+        c->state = CH_REF_A;
+    } else {
+        c->state = CH_DONE;
+    }
+}
+
+static void chain_init(agile_chain *c, const double *theta0, const double *lo, const double *hi,
+                       int d, const agile_opts *o)
+{
+    memset(c, 0, sizeof(*c));
+    c->d = d;
+    c->o = *o;
+    memcpy(c->lo, lo, (size_t)d * sizeof(double));
+    memcpy(c->hi, hi, (size_t)d * sizeof(double));
+    c->refine_step = o->refine_step > 0.0 ? o->refine_step : o->eta_min;
+    c->rng = o->seed ? o->seed : 0xA57B17E5ULL;
+    memcpy(c->th, theta0, (size_t)d * sizeof(double));
+    project(c->th, lo, hi, d, o->reflect);
+    c->patience = o->patience0;
+    c->state = CH_INIT;
+}
+
+/* points the chain needs evaluated now (0, 1 or 2), written to pts */
+static int chain_ask(const agile_chain *c, double *pts)
+{
+    const size_t b = (size_t)c->d * sizeof(double);
+    switch (c->state) {
+    case CH_INIT:
+        memcpy(pts, c->th, b);
+        return 1;
+    case CH_EXP_A:
+    case CH_REF_A:
+        memcpy(pts, c->tp, b);
+        memcpy(pts + c->d, c->tm, b);
+        return 2;
+    case CH_EXP_B:
+        memcpy(pts, c->cand, b);
+        return 1;
+    case CH_REF_B:
+        memcpy(pts, c->th, b);
+        return 1;
+    default:
+        return 0;
+    }
+}
+
+static void chain_tell(agile_chain *c, const double *f)
+{
+    const int d = c->d;
+    switch (c->state) {
+    case CH_INIT:
+        c->loss = f[0];
+        c->best = f[0];
+        memcpy(c->best_theta, c->th, (size_t)d * sizeof(double));
+        c->evals = 1;
+        c->iters++;
+        chain_spsa_points(c);
+        c->state = CH_EXP_A;
+        break;
+    case CH_EXP_A: {
+        chain_spsa_grad(c, f[0], f[1]);
+        c->evals += 2;
+        double s = 0.0;
+        for (int i = 0; i < d; i++)
+            s += c->g[i] * c->g[i];
+        double gn = sqrt(s);
+        if (gn > 1e-18) {
+            for (int i = 0; i < d; i++)
+                c->dir[i] = (-1.0 / gn) * c->g[i];
+        } else {
+            double ss = 0.0;
+            for (int i = 0; i < d; i++) {
+                double z = pcg_uniform(&c->rng) * 2.0 - 1.0;
+                c->dir[i] = z;
+                ss += z * z;
+            }
+            double nn = sqrt(ss) + 1e-18;
+            for (int i = 0; i < d; i++)
+                c->dir[i] /= nn;
+        }
+        double eta = levy_step(c->o.mu, c->o.eta_min, c->o.eta_max, &c->rng);
+        for (int i = 0; i < d; i++)
+            c->cand[i] = c->th[i] + eta * c->dir[i];
+        project(c->cand, c->lo, c->hi, d, c->o.reflect);
+        c->state = CH_EXP_B;
+        break;
+    }
+    case CH_EXP_B: {
+        double cl = f[0];
+        c->evals++;
+        if (cl < c->loss) {
+            memcpy(c->th, c->cand, (size_t)d * sizeof(double));
+            c->loss = cl;
+            c->since = 0;
+            c->patience *= c->o.patience_decay;
+            if (c->patience < 1.0)
+                c->patience = 1.0;
+            if (c->loss < c->best) {
+                c->best = c->loss;
+                c->best_iter = c->iters;
+                memcpy(c->best_theta, c->th, (size_t)d * sizeof(double));
+            }
+        } else {
+            c->since++;
+        }
+        if (c->since >= (int)ceil(c->patience)) {
+            chain_enter_refine(c);
+        } else if (c->iters > 1000000) {
+            c->state = CH_DONE;
+        } else {
+            c->iters++;
+            chain_spsa_points(c);
+            c->state = CH_EXP_A;
+        }
+        break;
+    }
+    case CH_REF_A:
+        chain_spsa_grad(c, f[0], f[1]);
+        c->evals += 2;
+        for (int i = 0; i < d; i++)
+            c->th[i] += -c->refine_step * c->g[i];
+        project(c->th, c->lo, c->hi, d, c->o.reflect);
+        c->state = CH_REF_B;
+        break;
+    case CH_REF_B: {
+        double nl = f[0];
+        c->evals++;
+        if (nl < c->loss - 1e-12) {
+            c->loss = nl;
+            if (c->loss < c->best) {
+                c->best = c->loss;
+                c->best_iter = c->iters;
+                memcpy(c->best_theta, c->th, (size_t)d * sizeof(double));
+            }
+            c->no_imp = 0;
+        } else {
+            c->no_imp++;
+        }
+        c->k++;
+        if (c->no_imp >= c->o.refine_no_improve || c->k >= c->o.refine_max_iters) {
+            c->state = CH_DONE;
+        } else {
+            c->iters++;
+            chain_spsa_points(c);
+            c->state = CH_REF_A;
+        }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+struct spires_ext_agile_batch {
+    int chains, dim;
+    agile_chain *c;
+    int *asked; /* points each chain was asked for in the last ask */
+};
+
+static void opts_from_public(agile_opts *o, const spires_ext_agile_opts *p)
+{
+    agile_opts def = {1.3, 1e-3, 5e-1, 100.0, 0.9, 0.0, 200, 30, 1e-3, 1, 0xC0FFEEULL};
+    *o = def;
+    if (p) {
+        o->mu = p->mu;
+        o->eta_min = p->eta_min;
+        o->eta_max = p->eta_max;
+        o->patience0 = p->patience0;
+        o->patience_decay = p->patience_decay;
+        o->refine_step = p->refine_step;
+        o->refine_max_iters = p->refine_max_iters;
+        o->refine_no_improve = p->refine_no_improve;
+        o->spsa_eps = p->spsa_eps;
+        o->reflect = p->reflect_at_bounds;
+        o->seed = p->seed;
+    }
+}
+
+SPIRES_EXPORT spires_status spires_ext_agile_batch_create(int chains, int dim,
+                                                          const double *theta0,
+                                                          const double *lower,
+                                                          const double *upper,
+                                                          const spires_ext_agile_opts *opts,
+                                                          const uint64_t *seeds,
+                                                          spires_ext_agile_batch **out)
+{
+    if (!out || chains <= 0 || dim <= 0 || dim > 64 || !theta0 || !lower || !upper)
+        return SPIRES_ERR_INVALID_ARG;
+    spires_ext_agile_batch *b = calloc(1, sizeof(*b));
+    if (!b)
+        return SPIRES_ERR_ALLOC;
+    b->chains = chains;
+    b->dim = dim;
+    b->c = calloc((size_t)chains, sizeof(agile_chain));
+    b->asked = calloc((size_t)chains, sizeof(int));
+    if (!b->c || !b->asked) {
+        free(b->c);
+        free(b->asked);
+        free(b);
+        return SPIRES_ERR_ALLOC;
+    }
+    for (int k = 0; k < chains; k++) {
+        agile_opts o;
+        opts_from_public(&o, opts);
+        if (seeds)
+            o.seed = seeds[k];
+        chain_init(&b->c[k], theta0 + (size_t)k * dim, lower, upper, dim, &o);
+    }
+    *out = b;
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT void spires_ext_agile_batch_destroy(spires_ext_agile_batch *b)
+{
+    if (!b)
+        return;
+    free(b->c);
+    free(b->asked);
+    free(b);
+}
+
+SPIRES_EXPORT int spires_ext_agile_batch_ask(spires_ext_agile_batch *b, double *points,
+                                             int *owner)
+{
+    if (!b || !points)
+        return -1;
+    int n = 0;
+    for (int k = 0; k < b->chains; k++) {
+        const int m = chain_ask(&b->c[k], points + (size_t)n * b->dim);
+        b->asked[k] = m;
+        for (int j = 0; j < m; j++)
+            if (owner)
+                owner[n + j] = k;
+        n += m;
+    }
+    return n;
+}
+
+SPIRES_EXPORT spires_status spires_ext_agile_batch_tell(spires_ext_agile_batch *b,
+                                                        const double *losses)
+{
+    if (!b || !losses)
+        return SPIRES_ERR_INVALID_ARG;
+    int n = 0;
+    for (int k = 0; k < b->chains; k++) {
+        if (b->asked[k] > 0)
+            chain_tell(&b->c[k], losses + n);
+        n += b->asked[k];
+        b->asked[k] = 0;
+    }
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_agile_batch_best(const spires_ext_agile_batch *b, int chain,
+                                                        double *theta,
+                                                        spires_ext_agile_report *report)
+{
+    if (!b || chain < 0 || chain >= b->chains)
+        return SPIRES_ERR_INVALID_ARG;
+    const agile_chain *c = &b->c[chain];
+    if (theta)
+        memcpy(theta, c->best_theta, (size_t)c->d * sizeof(double));
+    if (report) {
+        report->best_loss = c->best;
+        report->best_iter = c->best_iter;
+        report->total_evals = c->evals;
+        report->total_iters = c->iters;
+        report->exited_refinement = c->refined;
+    }
+    return SPIRES_OK;
+}
+
 int sp_default_gram_mode(void)
 {
     const char *e = getenv("SPIRES_RIDGE_GRAM");
