@@ -248,6 +248,18 @@ spires_status spires_ext_batch_predict(spires_ext_batch *b, const double *const 
                                        const size_t *T, double *const *y,
                                        double *elapsed_ms);
 
+/* Fit and score from one simulation: every instance runs T[k] steps of u[k]
+ * from reset with its states recorded, its ridge readout is fitted on rows
+ * [washout, T_fit[k]) against y[k] (T_fit[k] x num_outputs_k needed) and the
+ * fitted W_out, kept for later calls and copied to w_out[k] when given, is
+ * applied to all T[k] rows: y_out[k] is T[k] x num_outputs_k. */
+spires_status spires_ext_batch_fit_predict(spires_ext_batch *b, const double *const *u,
+                                           const double *const *y, const size_t *T,
+                                           const size_t *T_fit, const double *lambda,
+                                           const spires_ext_ridge_opts *opts,
+                                           double *const *y_out, double *const *w_out,
+                                           double *elapsed_ms);
+
 /* Schedule of the last run: CTAs of the grid, CTA groups, and whether the
  * launch sequence runs as a CUDA graph (1) or as direct launches (-1). */
 spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas, int *groups,

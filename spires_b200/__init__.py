@@ -193,6 +193,10 @@ EXT_SIGNATURES = {
                                                C.POINTER(RidgeOpts), C.POINTER(_dp), _dp]),
     "spires_ext_batch_predict": (C.c_int, [_VP, C.POINTER(_dp), C.POINTER(C.c_size_t),
                                            C.POINTER(_dp), _dp]),
+    "spires_ext_batch_fit_predict": (C.c_int, [_VP, C.POINTER(_dp), C.POINTER(_dp),
+                                               C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), _dp,
+                                               C.POINTER(RidgeOpts), C.POINTER(_dp),
+                                               C.POINTER(_dp), _dp]),
     "spires_ext_batch_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                         C.POINTER(C.c_int)]),
 }
@@ -521,6 +525,25 @@ class Batch:
         st = self.lib.spires_ext_batch_predict(self.h, up, Ts, yp, C.byref(ms))
         if st != SPIRES_OK:
             raise RuntimeError(f"spires_ext_batch_predict failed: {st}")
+        return Y, ms.value
+
+    def fit_predict(self, us, ys, T_fit, lam, washout=0, gram_mode=0):
+        """One simulation of every full series: ridge on rows [washout, T_fit[k]),
+        readouts of all rows returned (list of [T_k, dout_k])."""
+        up, T, keep = self._inputs(us, None)
+        ykeep = [np.ascontiguousarray(y, dtype=np.float64) for y in ys]
+        yp = (_dp * self.count)(*[dptr(y) for y in ykeep])
+        Ts = (C.c_size_t * self.count)(*T)
+        Tf = (C.c_size_t * self.count)(*[int(t) for t in T_fit])
+        lams = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, np.float64), (self.count,)))
+        Y = [np.empty((T[k], max(self.dout[k], 1))) for k in range(self.count)]
+        op = (_dp * self.count)(*[dptr(v) for v in Y])
+        o = RidgeOpts(gram_mode, 30, 1e-13, washout)
+        ms = C.c_double(0.0)
+        st = self.lib.spires_ext_batch_fit_predict(self.h, up, yp, Ts, Tf, dptr(lams), C.byref(o),
+                                                   op, None, C.byref(ms))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_batch_fit_predict failed: {st}")
         return Y, ms.value
 
     def info(self):

@@ -673,6 +673,31 @@ SPIRES_EXPORT spires_status spires_ext_batch_predict(spires_ext_batch *b, const 
     return to_status(sp_batch_predict(b->b, u, T, y, elapsed_ms));
 }
 
+SPIRES_EXPORT spires_status spires_ext_batch_fit_predict(
+    spires_ext_batch *b, const double *const *u, const double *const *y, const size_t *T,
+    const size_t *T_fit, const double *lambda, const spires_ext_ridge_opts *opts,
+    double *const *y_out, double *const *w_out, double *elapsed_ms)
+{
+    if (!b || !T || !T_fit || !y || !lambda)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_opts o;
+    memset(&o, 0, sizeof(o));
+    o.gram_mode = SPIRES_EXT_GRAM_FP64;
+    o.max_refine = 30;
+    o.refine_tol = 1e-13;
+    if (opts) {
+        o.gram_mode = opts->gram_mode;
+        o.max_refine = opts->max_refine;
+        o.refine_tol = opts->refine_tol;
+        o.washout = opts->washout;
+    }
+    for (size_t k = 0; k < b->count; ++k)
+        if (!y[k] || T_fit[k] > T[k] || o.washout >= T_fit[k])
+            return SPIRES_ERR_INVALID_ARG;
+    return to_status(
+        sp_batch_fit_predict(b->b, u, y, T, T_fit, lambda, &o, y_out, w_out, elapsed_ms));
+}
+
 SPIRES_EXPORT spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas,
                                                   int *groups, int *graph)
 {

@@ -107,6 +107,61 @@ __device__ __forceinline__ double batch_history(double hist, const double *s_coe
     return hist;
 }
 
+// SIMPLE-synapse row pass of one warp (rows [row0, row0 + 32), lane r owns
+// row row0 + r) for long rows: the warp's contiguous edge range is scanned in
+// blocks of 32 * U edges whose column indices and weights are loaded one block
+// ahead, so U loads per lane are in flight instead of one. Within a block the
+// sub-chunks are taken in ascending edge order and each spiking edge's weight
+// is added by the owner lane of its row: exactly the non-zero terms of
+// csr_row_dot (src/sparse.c:68-76) in order, as in the one-chunk row pass.
+template <int U>
+__device__ __forceinline__ double rowpass_simple_warp_deep(const long long *__restrict__ row_ptr,
+                                                           const int *__restrict__ col,
+                                                           const double *__restrict__ w,
+                                                           const unsigned *s_spk, int row0,
+                                                           int lane)
+{
+    const long long e0 = __ldg(row_ptr + row0);
+    const long long e1 = __ldg(row_ptr + row0 + 32);
+    const long long my_end = __ldg(row_ptr + row0 + lane + 1);
+    double acc = 0.0;
+    int cn[U];
+    double wn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const long long k = e0 + 32 * u + lane;
+        cn[u] = k < e1 ? __ldg(col + k) : -1;
+        wn[u] = k < e1 ? __ldg(w + k) : 0.0;
+    }
+    for (long long base = e0; base < e1; base += 32 * U) {
+        int c[U];
+        double wv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            c[u] = cn[u];
+            wv[u] = wn[u];
+            const long long k = base + 32 * (U + u) + lane;
+            cn[u] = k < e1 ? __ldg(col + k) : -1;
+            wn[u] = k < e1 ? __ldg(w + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool sp = c[u] >= 0 && ((s_spk[c[u] >> 5] >> (c[u] & 31)) & 1u);
+            unsigned m = __ballot_sync(kFull, sp);
+            while (m) {
+                const int bpos = __ffs(m) - 1;
+                m &= m - 1;
+                const long long eb = base + 32 * u + bpos;
+                const double wb = __shfl_sync(kFull, wv[u], bpos);
+                const unsigned owner = __ballot_sync(kFull, my_end > eb);
+                if (lane == __ffs(owner) - 1)
+                    acc = add(acc, wb);
+            }
+        }
+    }
+    return acc;
+}
+
 // One persistent cooperative launch over the whole batch. CTA c belongs to
 // group cta_group[c] (or to none, then it returns at once); a group runs its
 // job list in order, splitting each instance's warps evenly over its CTAs,
@@ -228,8 +283,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
                 s_spk[wi] = __ldcg(I.spk + (size_t)cur * nw + wi);
             __syncthreads();
             double rec = 0.0;
-            if (wact)
-                rec = rowpass_simple_warp(I.row_ptr, I.col, I.w, s_spk, gw * 32, 32, lane);
+            if (wact) {
+                // warp-uniform choice: long edge ranges take the deep pipeline
+                const long long span = __ldg(I.row_ptr + gw * 32 + 32) - __ldg(I.row_ptr + gw * 32);
+                rec = span > 256 ? rowpass_simple_warp_deep<8>(I.row_ptr, I.col, I.w, s_spk,
+                                                                gw * 32, lane)
+                                 : rowpass_simple_warp(I.row_ptr, I.col, I.w, s_spk, gw * 32, 32,
+                                                       lane);
+            }
             bool fired = false;
             if (act) {
                 const double in = add(ext, rec);
@@ -969,6 +1030,85 @@ extern "C" int sp_batch_predict(sp_batch *b, const double *const *u, const size_
     }
     cudaStreamSynchronize(b->stream);
     cudaFree(Y);
+    if (elapsed_ms)
+        *elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+// One simulation per instance serves both the fit and the score: states of
+// T[k] steps are recorded, the ridge uses rows [washout, T_fit[k]) and the
+// fitted readout is applied to every row, y_out[k] being T[k] x dout.
+extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const double *const *y,
+                                    const size_t *T, const size_t *T_fit, const double *lambda,
+                                    const sp_ridge_opts *o, double *const *y_out,
+                                    double *const *w_out, double *elapsed_ms)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = batch_prepare(b, T, 1);
+    if (rc)
+        return rc;
+    rc = batch_simulate(b, u, nullptr);
+    if (rc)
+        return rc;
+    size_t max_tn = 1, max_ty = 1, max_wn = 1;
+    for (size_t k = 0; k < b->inst.size(); ++k) {
+        max_tn = std::max(max_tn, T_fit[k] * (size_t)b->inst[k].n);
+        max_ty = std::max(max_ty, T[k] * b->models[k].dout);
+        max_wn = std::max(max_wn, (size_t)b->inst[k].n * b->models[k].dout);
+    }
+    double *nat = nullptr, *Y = nullptr, *W = nullptr;
+    if (cudaMalloc(&nat, max_tn * 8) != cudaSuccess || cudaMalloc(&Y, max_ty * 8) != cudaSuccess ||
+        cudaMalloc(&W, max_wn * 8) != cudaSuccess) {
+        cudaGetLastError();
+        if (nat)
+            cudaFree(nat);
+        if (Y)
+            cudaFree(Y);
+        return SP_EALLOC;
+    }
+    size_t po = 0;
+    for (size_t k = 0; k < b->inst.size() && !rc; ++k) {
+        const BInst &I = b->inst[k];
+        const int dout = (int)b->models[k].dout;
+        const double *phi = b->d_phi + po;
+        po += T[k] * I.rs;
+        if (dout == 0)
+            continue;
+        if (cudaMemcpyAsync(Y, y[k], T_fit[k] * dout * 8, cudaMemcpyHostToDevice, b->stream) !=
+            cudaSuccess) {
+            rc = SP_EINTERNAL;
+            break;
+        }
+        rc = sp_launch_gather_rows(b->stream, phi, I.rs, I.pos_of, I.n, T_fit[k], nat);
+        if (rc)
+            break;
+        sp_ridge_report rep;
+        memset(&rep, 0, sizeof(rep));
+        rc = sp_ridge_phi(b->stream, nat, I.n, T_fit[k], Y, dout, lambda[k], o, &rep, W);
+        if (rc == SP_RIDGE_SINGULAR) {
+            rc = SP_OK; /* this instance keeps its previous W_out */
+        } else if (!rc) {
+            rc = sp_launch_wout_to_pos(b->stream, W, I.nid_of, I.n, I.rs, dout, b->w_pos[k]);
+            if (!rc && w_out && w_out[k] &&
+                cudaMemcpyAsync(w_out[k], W, (size_t)dout * I.n * 8, cudaMemcpyDeviceToHost,
+                                b->stream) != cudaSuccess)
+                rc = SP_EINTERNAL;
+        }
+        if (rc)
+            break;
+        rc = sp_launch_readout(b->stream, b->w_pos[k], phi, I.rs, T[k], dout, Y);
+        if (!rc && y_out && y_out[k] &&
+            cudaMemcpyAsync(y_out[k], Y, T[k] * dout * 8, cudaMemcpyDeviceToHost, b->stream) !=
+                cudaSuccess)
+            rc = SP_EINTERNAL;
+        if (!rc && cudaStreamSynchronize(b->stream) != cudaSuccess)
+            rc = SP_EINTERNAL;
+    }
+    cudaStreamSynchronize(b->stream);
+    cudaFree(nat);
+    cudaFree(Y);
+    cudaFree(W);
     if (elapsed_ms)
         *elapsed_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -130,6 +130,10 @@ int  sp_batch_train_ridge(sp_batch *b, const double *const *u, const double *con
                           double *const *w_out, double *elapsed_ms);
 int  sp_batch_predict(sp_batch *b, const double *const *u, const size_t *T,
                       double *const *y, double *elapsed_ms);
+int  sp_batch_fit_predict(sp_batch *b, const double *const *u, const double *const *y,
+                          const size_t *T, const size_t *T_fit, const double *lambda,
+                          const sp_ridge_opts *o, double *const *y_out, double *const *w_out,
+                          double *elapsed_ms);
 int  sp_batch_info(const sp_batch *b, int *ctas, int *groups, int *graph);
 
 #ifdef __cplusplus

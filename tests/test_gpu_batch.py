@@ -153,3 +153,18 @@ def test_batch_rejects_unsupported_models():
                           sparams=(5.0,))
     with pytest.raises(RuntimeError):
         sp.Batch([cfg2], [1])
+
+
+def test_fit_predict_equals_train_then_predict():
+    cfgs, seeds, us = mixed_batch(4, seed=41, n_hi=600, t_lo=200, t_hi=300)
+    rng = np.random.default_rng(2)
+    ys = [rng.standard_normal((u.shape[0], 2)) for u in us]
+    T_fit = [int(0.7 * u.shape[0]) for u in us]
+    b = sp.Batch(cfgs, seeds)
+    Y, _ = b.fit_predict(us, ys, T_fit, 1e-3, washout=10)
+    b2 = sp.Batch(cfgs, seeds)
+    b2.train_ridge([u[:t] for u, t in zip(us, T_fit)], [y[:t] for y, t in zip(ys, T_fit)], 1e-3,
+                   washout=10)
+    Y2, _ = b2.predict(us)
+    for k in range(len(cfgs)):
+        assert same_bits(Y[k][:, :2], Y2[k][:, :2]), f"instance {k}"
