@@ -124,6 +124,8 @@ typedef struct {
     double collect_ms, gram_ms, factor_ms, refine_ms;
     int    factor_failed;
     int    lu_fallback;
+    int    dual;             /* 1: fewer fitted rows than N/2, solved as
+                                W = Phi^T (Phi Phi^T + lambda I)^-1 Y */
 } spires_ext_ridge_report;
 
 spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_series,

@@ -92,7 +92,7 @@ class RidgeReport(C.Structure):
                 ("rel_residual", C.c_double), ("collect_ms", C.c_double),
                 ("gram_ms", C.c_double), ("factor_ms", C.c_double),
                 ("refine_ms", C.c_double), ("factor_failed", C.c_int),
-                ("lu_fallback", C.c_int)]
+                ("lu_fallback", C.c_int), ("dual", C.c_int)]
 
 
 class AgileOpts(C.Structure):

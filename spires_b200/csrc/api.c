@@ -551,6 +551,7 @@ SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
         report->refine_ms = rep.refine_ms;
         report->factor_failed = rep.factor_failed;
         report->lu_fallback = rep.lu_fallback;
+        report->dual = rep.dual;
     }
     return to_status(rc);
 }

@@ -124,11 +124,48 @@ static int trip_cmp(const void *a, const void *b)
 /* Triplets (unique (r,c), any order) -> CSR with ascending columns, dropping
  * entries equal to zero exactly as csr_build_from_dense does
  * (src/sparse.c:7-42: `dense[k] != 0.0`). */
+/* Stable counting sort of the triplets by row; rows whose columns are then
+ * not ascending (none, for the generators here) are sorted on their own. */
+static int trips_sort_rows(size_t n, tripbuf *b)
+{
+    int64_t *off = calloc(n + 1, sizeof(int64_t));
+    trip *t = malloc((b->n ? b->n : 1) * sizeof(trip));
+    if (!off || !t) {
+        free(off);
+        free(t);
+        return SP_EALLOC;
+    }
+    for (size_t k = 0; k < b->n; k++)
+        off[b->t[k].r + 1]++;
+    for (size_t i = 0; i < n; i++)
+        off[i + 1] += off[i];
+    for (size_t k = 0; k < b->n; k++)
+        t[off[b->t[k].r]++] = b->t[k];
+    /* off[i] now holds the end of row i */
+    int64_t start = 0;
+    for (size_t i = 0; i < n; i++) {
+        for (int64_t k = start + 1; k < off[i]; k++)
+            if (t[k].c < t[k - 1].c) {
+                qsort(t + start, (size_t)(off[i] - start), sizeof(trip), trip_cmp);
+                break;
+            }
+        start = off[i];
+    }
+    free(off);
+    free(b->t);
+    b->t = t;
+    b->cap = b->n ? b->n : 1;
+    return SP_OK;
+}
+
 static int csr_from_trips(sp_host_model *m, tripbuf *b, int sorted)
 {
     size_t n = m->n;
-    if (!sorted)
-        qsort(b->t, b->n, sizeof(trip), trip_cmp);
+    if (!sorted) {
+        int rc = trips_sort_rows(n, b);
+        if (rc)
+            return rc;
+    }
     size_t nnz = 0;
     for (size_t k = 0; k < b->n; k++)
         if (b->t[k].v != 0.0)
@@ -390,14 +427,18 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
         degsum += deg[v];
     }
 
-    /* undirected adjacency lists, sorted */
+    /* Neighbours above each node, ascending: the edges (a, b), a < b, are
+     * bucketed by a. They were generated in nondecreasing order of b (the seed
+     * clique row by row, then node by node), so a stable bucket fill leaves
+     * every bucket ascending -- the same lists a sort of the full undirected
+     * adjacency would give for the j > i part the orientation pass reads. */
     adj_off = calloc(n + 1, sizeof(int64_t));
-    adj = malloc(((2) * (ne) > 0 ? (2) * (ne) : 1) * sizeof(int32_t));
+    adj = malloc((ne > 0 ? ne : 1) * sizeof(int32_t));
     if (!adj_off || !adj)
         goto done;
     for (size_t e = 0; e < ne; e++) {
-        adj_off[eu[e] + 1]++;
-        adj_off[ev[e] + 1]++;
+        const int32_t lo = eu[e] < ev[e] ? eu[e] : ev[e];
+        adj_off[lo + 1]++;
     }
     for (size_t u = 0; u < n; u++)
         adj_off[u + 1] += adj_off[u];
@@ -407,13 +448,19 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
             goto done;
         memcpy(fill, adj_off, n * sizeof(int64_t));
         for (size_t e = 0; e < ne; e++) {
-            adj[fill[eu[e]]++] = ev[e];
-            adj[fill[ev[e]]++] = eu[e];
+            const int32_t lo = eu[e] < ev[e] ? eu[e] : ev[e];
+            const int32_t hi = eu[e] < ev[e] ? ev[e] : eu[e];
+            adj[fill[lo]++] = hi;
         }
         free(fill);
     }
-    for (size_t u = 0; u < n; u++)
-        qsort(adj + adj_off[u], (size_t)(adj_off[u + 1] - adj_off[u]), sizeof(int32_t), cmp_i32);
+    for (size_t u = 0; u < n; u++) /* guard: keep the ascending order exact */
+        for (int64_t k = adj_off[u] + 1; k < adj_off[u + 1]; k++)
+            if (adj[k] < adj[k - 1]) {
+                qsort(adj + adj_off[u], (size_t)(adj_off[u + 1] - adj_off[u]), sizeof(int32_t),
+                      cmp_i32);
+                break;
+            }
 
     /* orientation pass in row-major order over i < j */
     for (size_t i = 0; i < n; i++)

@@ -658,7 +658,14 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         sp_batch_destroy(b);
         return rc;
     }
+    // Layouts, position-order CSR and uploads of the instances on all host
+    // threads (each worker thread selects the batch's device first).
+    int failed = 0;
+#pragma omp parallel for schedule(dynamic, 1)
     for (size_t k = 0; k < count; ++k) {
+        if (failed)
+            continue;
+        cudaSetDevice(b->device);
         const sp_host_model &m = b->models[k];
         BInst &I = b->inst[k];
         const Off &o = off[k];
@@ -717,9 +724,14 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
             ok = cudaMemcpy(A + o.coef, m.coef, (size_t)I.L * 8, cudaMemcpyHostToDevice) ==
                  cudaSuccess;
         if (!ok) {
-            sp_batch_destroy(b);
-            return SP_EINTERNAL;
+#pragma omp atomic write
+            failed = 1;
         }
+    }
+    if (failed) {
+        cudaGetLastError();
+        sp_batch_destroy(b);
+        return SP_EINTERNAL;
     }
     if (cudaMalloc(&b->d_bar, (size_t)b->P * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&b->d_err, 4 * sizeof(int)) != cudaSuccess ||

@@ -141,8 +141,10 @@ extern "C" int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const in
                  o_x = o_w + ((nnz ? nnz : 1) * 8 + 255) / 256 * 256,
                  o_y = o_x + ((n ? n : 1) * 8 + 255) / 256 * 256,
                  o_small = o_y + ((n ? n : 1) * 8 + 255) / 256 * 256, total = o_small + 256;
+    // stream-ordered allocation: no device-wide synchronisation, so several
+    // host threads building reservoirs at once do not serialise here
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&buf, total) != cudaSuccess) {
+        cudaMallocAsync(&buf, total, s) != cudaSuccess) {
         cudaGetLastError();
         if (s)
             cudaStreamDestroy(s);
@@ -185,7 +187,8 @@ extern "C" int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const in
     } else {
         *out = h_out[0];
     }
-    cudaFree(buf);
+    cudaFreeAsync(buf, s);
+    cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     return rc;
 }

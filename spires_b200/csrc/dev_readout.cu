@@ -156,6 +156,26 @@ __global__ void k_resid_rows(const double *__restrict__ X, int n, size_t t0, siz
     }
 }
 
+// Pt[k][t - t0] = X[t][k] for rows [t0, t1) of X (T x n): 32 x 32 tiles
+// through shared memory, both sides coalesced.
+__global__ void k_rows_to_cols(const double *__restrict__ X, int n, size_t t0, size_t t1,
+                               double *__restrict__ Pt)
+{
+    __shared__ double tile[32][33];
+    const size_t tw = t1 - t0;
+    const size_t tb = (size_t)blockIdx.y * 32, kb = (size_t)blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const size_t t = tb + r, k = kb + threadIdx.x;
+        tile[r][threadIdx.x] = (t < tw && k < (size_t)n) ? X[(t0 + t) * n + k] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const size_t k = kb + r, t = tb + threadIdx.x;
+        if (k < (size_t)n && t < tw)
+            Pt[k * tw + t] = tile[threadIdx.x][r];
+    }
+}
+
 __global__ void k_add_diag(double *A, int n, int lda, double lam)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -647,6 +667,70 @@ static double device_norm(cudaStream_t s, const double *x, size_t cnt, double *d
     return sqrt(h);
 }
 
+// Dual-form ridge for T - w0 < n: K = Phi_w Phi_w^T + lambda I (FP64 Gram of
+// the transposed rows), Cholesky (pivoted LU if it fails, as dgesv would),
+// alpha = K^-1 Y_w, W = Phi_w^T alpha; B = Phi_w^T Y_w for the residual check.
+// E (T x dout) is used as the right-hand side and holds alpha in rows w0..T-1.
+static int ridge_dual(cudaStream_t s, const double *Phi, int n, size_t T, size_t w0,
+                      const double *Y, int dout, double lambda, sp_ridge_report *rep, double *W,
+                      double *B, double *E, double *part, int parts, int *info, int *piv)
+{
+    int rc = SP_OK;
+    const size_t tw = T - w0;
+    const int m = (int)tw;
+    double *Pt = nullptr, *K = nullptr;
+    const size_t tot = (size_t)n * dout;
+    const dim3 gp((n + 127) / 128, parts);
+    auto tg = std::chrono::steady_clock::now();
+    RK(cudaMalloc(&Pt, (size_t)n * tw * sizeof(double)));
+    RK(cudaMalloc(&K, tw * tw * sizeof(double)));
+    {
+        dim3 g((n + 31) / 32, (unsigned)((tw + 31) / 32));
+        k_rows_to_cols<<<g, dim3(32, 8), 0, s>>>(Phi, n, w0, T, Pt);
+        const int nt = (m + 63) / 64;
+        k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(Pt, m, 0, (size_t)n, K, m);
+        k_add_diag<<<(m + 255) / 256, 256, 0, s>>>(K, m, m, lambda);
+        k_xt_e_part<<<gp, 128, 0, s>>>(Phi, n, w0, T, Y, dout, parts, part);
+        k_reduce_parts<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, parts, n, dout, nullptr,
+                                                                     0.0, B);
+        RK(cudaMemcpyAsync(E, Y, T * dout * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+        rep->gram_ms = ms_since(tg);
+    }
+    {
+        auto tf = std::chrono::steady_clock::now();
+        double *Z = E + w0 * dout;
+        if (cholesky_inplace(s, K, m, info)) {
+            rep->factor_failed = 1;
+            rep->lu_fallback = 1;
+            RK(cudaMemsetAsync(info, 0, sizeof(int), s));
+            const int nt = (m + 63) / 64;
+            k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(Pt, m, 0, (size_t)n, K, m);
+            k_add_diag<<<(m + 255) / 256, 256, 0, s>>>(K, m, m, lambda);
+            if (lu_factor_solve(s, K, m, piv, info, Z, dout)) {
+                rc = SP_RIDGE_SINGULAR;
+                goto out;
+            }
+        } else {
+            chol_solve(s, K, m, Z, dout);
+        }
+        k_xt_e_part<<<gp, 128, 0, s>>>(Phi, n, w0, T, E, dout, parts, part);
+        k_reduce_parts<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, parts, n, dout, nullptr,
+                                                                     0.0, W);
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+        rep->factor_ms = ms_since(tf);
+    }
+out:
+    cudaStreamSynchronize(s);
+    if (Pt)
+        cudaFree(Pt);
+    if (K)
+        cudaFree(K);
+    return rc;
+}
+
 // Ridge on states already on the device: Phi [T x n] row-major (neuron order),
 // Y [T x dout]; rows [washout, T) enter the Gram. On success d_W_out [dout x n]
 // holds the solution; SP_RIDGE_SINGULAR leaves it untouched (dgesv failure in
@@ -675,6 +759,28 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
     RK(cudaMalloc(&info, sizeof(int)));
     RK(cudaMalloc(&piv, (size_t)n * sizeof(int)));
     RK(cudaMemsetAsync(info, 0, sizeof(int), s));
+
+    if (lambda > 0.0 && 2 * (T - w0) <= (size_t)n) {
+        // Fewer fitted rows than half the neurons: the dual form
+        // W = Phi_w^T (Phi_w Phi_w^T + lambda I)^-1 Y_w, algebraically the same
+        // solution, factors a (T - w0)^2 matrix instead of n^2. (lambda = 0
+        // keeps the primal system, singular here, so that the call fails and
+        // leaves W_out as the reference's dgesv does.)
+        rc = ridge_dual(s, Phi, n, T, w0, Y, dout, lambda, rep, W, B, E, part, parts, info, piv);
+        if (rc)
+            goto out;
+        rep->dual = 1;
+        rep->gram_mode_used = 0;
+        const double bnorm = device_norm(s, B, (size_t)n * dout, tmp);
+        ridge_residual(s, Phi, n, w0, T, Y, W, dout, lambda, E, part, parts, R);
+        rep->rel_residual = device_norm(s, R, (size_t)n * dout, tmp) / (bnorm > 0 ? bnorm : 1.0);
+        rep->refine_iters = 0;
+        const size_t tot = (size_t)n * dout;
+        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, d_W_out);
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+        goto out;
+    }
 
     {
         auto tg = std::chrono::steady_clock::now();

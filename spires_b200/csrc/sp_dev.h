@@ -86,6 +86,7 @@ typedef struct {
     double gram_ms, factor_ms, refine_ms, collect_ms;
     int factor_failed;        /* Cholesky met a non-positive pivot */
     int lu_fallback;          /* solved by pivoted LU instead */
+    int dual;                 /* solved in the dual form (fewer rows than n / 2) */
 } sp_ridge_report;
 
 int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,

@@ -208,3 +208,24 @@ def test_coarse_grain_matches_restatement():
         r.lib.spires_step(h, sp.dptr(np.ascontiguousarray(u[t])))
     r.lib.spires_reservoir_destroy(h)
     r.close()
+
+
+@pytest.mark.parametrize("lam", [1e-2, 1e-5])
+def test_ridge_dual_form_when_rows_are_few(lam):
+    """Fewer fitted rows than N/2: the dual form solves the same ridge."""
+    cfg = cfg_gl(n=700, conn=0.02)
+    u, y = data(300, 2, 3, seed=9)
+    r = sp.Reservoir(cfg, seed=5)
+    opts = sp.RidgeOpts(0, 30, 1e-13, 20)
+    rep = sp.RidgeReport()
+    assert r.lib.spires_ext_train_ridge(r.h, sp.dptr(u), sp.dptr(y), 300, lam, C.byref(opts),
+                                        C.byref(rep)) == sp.SPIRES_OK
+    W = r.readout()
+    r.close()
+    assert rep.dual == 1
+    orc = O.Oracle(cfg, sp.HostModel(cfg, seed=5))
+    phi, _, _ = orc.run(u)
+    Wo = O.oracle_ridge(phi, y, lam, washout=20)
+    assert rel(phi[20:] @ W.T, phi[20:] @ Wo.T) < 1e-8
+    assert rel(W, Wo) < (1e-6 if lam >= 1e-2 else 1e-3)
+    assert rep.rel_residual < 1e-8
