@@ -106,8 +106,9 @@ spires_status spires_ext_spectral_radius(size_t n, const int64_t *row_ptr, const
 /* ---- ridge readout with options ------------------------------------------ */
 typedef enum {
     SPIRES_EXT_GRAM_FP64 = 0,      /* FP64 Gram (CUDA cores) */
-    SPIRES_EXT_GRAM_BF16X3 = 1     /* BF16 hi/lo split on tensor cores, FP32
-                                      accumulate, FP64 refinement */
+    SPIRES_EXT_GRAM_BF16X3 = 1,    /* BF16 hi/lo split on tensor cores, FP32
+                                      accumulate, FP64 Cholesky + refinement */
+    SPIRES_EXT_GRAM_TF32X3 = 2     /* the same with TF32 hi/lo */
 } spires_ext_gram_mode;
 
 typedef struct {

@@ -587,6 +587,57 @@ double ms_since(std::chrono::steady_clock::time_point t)
 
 }  // namespace
 
+// per-column dot products out[o] = sum_i X[i][o] Y[i][o] (n x dout arrays),
+// one block per column, fixed-order reduction
+static __global__ void k_coldot(const double *__restrict__ X, const double *__restrict__ Y, int n,
+                         int dout, double *__restrict__ out)
+{
+    __shared__ double s[256];
+    const int o = blockIdx.x;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < n; i += 256)
+        a = fma(X[(size_t)i * dout + o], Y[(size_t)i * dout + o], a);
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int st = 128; st; st >>= 1) {
+        if ((int)threadIdx.x < st)
+            s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        out[o] = s[0];
+}
+
+// Y[i][o] += c[o] X[i][o]  (xpby = 0)  or  Y[i][o] = X[i][o] + c[o] Y[i][o]  (xpby = 1)
+static __global__ void k_col_update(double *__restrict__ Y, const double *__restrict__ X,
+                             const double *__restrict__ c, int n, int dout, int xpby)
+{
+    const size_t total = (size_t)n * dout;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int o = (int)(k % dout);
+        Y[k] = xpby ? fma(c[o], Y[k], X[k]) : fma(c[o], X[k], Y[k]);
+    }
+}
+
+// largest diagonal entry (non-negative doubles compare like their bits)
+static __global__ void k_diag_max(const double *__restrict__ A, int n, unsigned long long *out)
+{
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = A[(size_t)i * n + i];
+        if (v > m)
+            m = v;
+    }
+    for (int off = 16; off; off >>= 1) {
+        const double o = __shfl_xor_sync(kFull, m, off);
+        if (o > m)
+            m = o;
+    }
+    if ((threadIdx.x & 31) == 0 && m > 0.0)
+        atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
 // ------------------------------------------------------------ factor + solve
 // Factor A (n x n) in place; returns 0 or the 1-based failing pivot.
 static int cholesky_inplace(cudaStream_t s, double *A, int n, int *d_info)
@@ -731,6 +782,117 @@ out:
     return rc;
 }
 
+// Mixed-precision solve of (Phi_w^T Phi_w + lambda I) W = B given A = G + lambda I
+// with G the split tensor-core Gram. The rounding error of G can exceed
+// lambda, so A itself may be indefinite: the preconditioner is the FP64
+// Cholesky factor of A + delta I, delta = eps * max diag (raised tenfold until
+// the factorisation succeeds), and the system is solved by preconditioned
+// conjugate gradients per output column whose operator p -> Phi^T (Phi p) +
+// lambda p is applied in FP64 from the states themselves. So the answer is
+// the FP64 ridge solution to the stated residual; the Gram's precision only
+// sets how many iterations that takes.
+static int ridge_mixed(cudaStream_t s, const double *Phi, int n, size_t T, size_t w0,
+                       const double *Y, int dout, double lambda, int mode,
+                       const sp_ridge_opts *o, sp_ridge_report *rep, double *A, double *B,
+                       double *W, double *R, double *E, double *part, int parts, double *tmp,
+                       int *info)
+{
+    int rc = SP_OK;
+    const size_t nn = (size_t)n * n, tot = (size_t)n * dout;
+    const unsigned gb = (unsigned)((tot + 255) / 256 < 4096 ? (tot + 255) / 256 : 4096);
+    double *A0 = nullptr, *Z = nullptr, *P = nullptr, *Q = nullptr, *Yz = nullptr, *c = nullptr,
+           *dots = nullptr;
+    double h_rz[16], h_pq[16], h_c[16];
+    auto tf = std::chrono::steady_clock::now();
+    RK(cudaMalloc(&A0, nn * sizeof(double)));
+    RK(cudaMalloc(&Z, tot * sizeof(double)));
+    RK(cudaMalloc(&P, tot * sizeof(double)));
+    RK(cudaMalloc(&Q, tot * sizeof(double)));
+    RK(cudaMalloc(&Yz, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(cudaMalloc(&c, 16 * sizeof(double)));
+    RK(cudaMalloc(&dots, 16 * sizeof(double)));
+    RK(cudaMemsetAsync(Yz, 0, (T ? T : 1) * (size_t)dout * sizeof(double), s));
+    RK(cudaMemcpyAsync(A0, A, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    {
+        RK(cudaMemsetAsync(tmp, 0, sizeof(double), s));
+        k_diag_max<<<(n + 255) / 256, 256, 0, s>>>(A, n, (unsigned long long *)tmp);
+        double dmax = 0.0;
+        RK(cudaMemcpyAsync(&dmax, tmp, sizeof(double), cudaMemcpyDeviceToHost, s));
+        RK(cudaStreamSynchronize(s));
+        double delta = (mode == 1 ? 1e-4 : 1e-5) * dmax;
+        int ok = 0;
+        for (int attempt = 0; attempt < 6 && !ok; ++attempt, delta *= 10.0) {
+            if (attempt > 0) {
+                rep->factor_failed = 1;
+                RK(cudaMemcpyAsync(A, A0, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                RK(cudaMemsetAsync(info, 0, sizeof(int), s));
+            }
+            k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, delta);
+            ok = cholesky_inplace(s, A, n, info) == 0;
+        }
+        if (!ok) {
+            rc = SP_RIDGE_SINGULAR;
+            goto out;
+        }
+        rep->factor_ms = ms_since(tf);
+    }
+    {
+        auto tr = std::chrono::steady_clock::now();
+        const double bnorm = device_norm(s, B, tot, tmp);
+        const double bden = bnorm > 0 ? bnorm : 1.0;
+        // W = M^-1 B, R = B - A W (FP64 from Phi), Z = M^-1 R, P = Z
+        RK(cudaMemcpyAsync(W, B, tot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        chol_solve(s, A, n, W, dout);
+        ridge_residual(s, Phi, n, w0, T, Y, W, dout, lambda, E, part, parts, R);
+        RK(cudaMemcpyAsync(Z, R, tot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        chol_solve(s, A, n, Z, dout);
+        RK(cudaMemcpyAsync(P, Z, tot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        k_coldot<<<dout, 256, 0, s>>>(R, Z, n, dout, dots);
+        RK(cudaMemcpyAsync(h_rz, dots, dout * sizeof(double), cudaMemcpyDeviceToHost, s));
+        int it = 0;
+        double rel = device_norm(s, R, tot, tmp) / bden;
+        while (rel > o->refine_tol && it < o->max_refine) {
+            // Q = -(A P): the residual form with zero targets
+            ridge_residual(s, Phi, n, w0, T, Yz, P, dout, lambda, E, part, parts, Q);
+            k_coldot<<<dout, 256, 0, s>>>(P, Q, n, dout, dots);
+            RK(cudaMemcpyAsync(h_pq, dots, dout * sizeof(double), cudaMemcpyDeviceToHost, s));
+            RK(cudaStreamSynchronize(s));
+            for (int k = 0; k < dout; ++k)
+                h_c[k] = (h_pq[k] != 0.0) ? h_rz[k] / -h_pq[k] : 0.0;  // alpha
+            RK(cudaMemcpyAsync(c, h_c, dout * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_col_update<<<gb, 256, 0, s>>>(W, P, c, n, dout, 0);  // W += alpha P
+            k_col_update<<<gb, 256, 0, s>>>(R, Q, c, n, dout, 0);  // R -= alpha A P
+            RK(cudaMemcpyAsync(Z, R, tot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            chol_solve(s, A, n, Z, dout);
+            k_coldot<<<dout, 256, 0, s>>>(R, Z, n, dout, dots);
+            double h_rz2[16];
+            RK(cudaMemcpyAsync(h_rz2, dots, dout * sizeof(double), cudaMemcpyDeviceToHost, s));
+            RK(cudaStreamSynchronize(s));
+            for (int k = 0; k < dout; ++k) {
+                h_c[k] = (h_rz[k] != 0.0) ? h_rz2[k] / h_rz[k] : 0.0;  // beta
+                h_rz[k] = h_rz2[k];
+            }
+            RK(cudaMemcpyAsync(c, h_c, dout * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_col_update<<<gb, 256, 0, s>>>(P, Z, c, n, dout, 1);  // P = Z + beta P
+            ++it;
+            rel = device_norm(s, R, tot, tmp) / bden;
+        }
+        // the reported residual is recomputed from Phi, not the recurrence
+        ridge_residual(s, Phi, n, w0, T, Y, W, dout, lambda, E, part, parts, R);
+        rep->rel_residual = device_norm(s, R, tot, tmp) / bden;
+        rep->refine_iters = it;
+        rep->refine_ms = ms_since(tr);
+        RK(cudaGetLastError());
+    }
+out:
+    cudaStreamSynchronize(s);
+    void *bufs[] = {A0, Z, P, Q, Yz, c, dots};
+    for (void *b : bufs)
+        if (b)
+            cudaFree(b);
+    return rc;
+}
+
 // Ridge on states already on the device: Phi [T x n] row-major (neuron order),
 // Y [T x dout]; rows [washout, T) enter the Gram. On success d_W_out [dout x n]
 // holds the solution; SP_RIDGE_SINGULAR leaves it untouched (dgesv failure in
@@ -785,8 +947,8 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
     {
         auto tg = std::chrono::steady_clock::now();
         int mode = o->gram_mode;
-        if (mode == 1 && sp_gram_bf16x3_available()) {
-            rc = sp_gram_bf16x3(s, Phi, n, w0, T, A, n);
+        if ((mode == 1 || mode == 2) && sp_gram_bf16x3_available()) {
+            rc = sp_gram_split(s, mode, Phi, n, w0, T, A, n);
             if (rc)
                 goto out;
         } else {
@@ -806,6 +968,18 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
         rep->gram_ms = ms_since(tg);
     }
 
+    if (rep->gram_mode_used != 0) {
+        rc = ridge_mixed(s, Phi, n, T, w0, Y, dout, lambda, rep->gram_mode_used, o, rep, A, B, W,
+                         R, E, part, parts, tmp, info);
+        if (rc)
+            goto out;
+        const size_t tot = (size_t)n * dout;
+        k_transpose_w<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(W, n, dout, d_W_out);
+        RK(cudaStreamSynchronize(s));
+        RK(cudaGetLastError());
+        goto out;
+    }
+
     {
         auto tf = std::chrono::steady_clock::now();
         RK(cudaMemcpyAsync(W, B, (size_t)n * dout * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -815,8 +989,8 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
             rep->factor_failed = 1;
             rep->lu_fallback = 1;
             RK(cudaMemsetAsync(info, 0, sizeof(int), s));
-            if (rep->gram_mode_used == 1) {
-                rc = sp_gram_bf16x3(s, Phi, n, w0, T, A, n);
+            if (rep->gram_mode_used != 0) {
+                rc = sp_gram_split(s, rep->gram_mode_used, Phi, n, w0, T, A, n);
                 if (rc)
                     goto out;
             } else {

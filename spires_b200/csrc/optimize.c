@@ -807,5 +807,7 @@ int sp_default_gram_mode(void)
     const char *e = getenv("SPIRES_RIDGE_GRAM");
     if (e && (!strcmp(e, "bf16x3") || !strcmp(e, "1")))
         return 1;
+    if (e && (!strcmp(e, "tf32x3") || !strcmp(e, "2")))
+        return 2;
     return 0;
 }
