@@ -356,6 +356,161 @@ def run_profile_case(args):
     print("profile case done")
 
 
+# ------------------------------------------------- additional workloads --
+# Printed only when asked for with --workload; the default line above is the
+# headline measurement.
+
+def bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def run_sweep_workload(args):
+    """256 uneven reservoirs (LIF_DISCRETE / FLIF_GL, N log-uniform in
+    [500, 8000], own Mackey-Glass series of 2000..10000 steps) in one batched
+    launch; all ridge readouts from one batched simulation."""
+    import numpy as np
+
+    import spires_b200 as sp
+    from spires_b200 import sweep
+
+    insts = sweep.sweep_space(args.sweep_count, seed=2024)
+    t0 = time.perf_counter()
+    b = sp.Batch([i.cfg for i in insts], [i.seed for i in insts])
+    build_s = time.perf_counter() - t0
+    us, ys = sweep.series_for(insts)
+    ns = float(sum(i.n * i.T for i in insts))
+    b.run(us, rasters=False, states=False)  # warm-up (plans, captures the graph)
+    times = [b.run(us, rasters=False, states=False)[2] for _ in range(max(1, args.steps // 10))]
+    ms = float(np.median(times))
+    res = sweep.run_sweep(insts, batch=b)
+    # the same instances one at a time through the single-reservoir path
+    k = min(8, len(insts))
+    solo_ms, solo_ns = 0.0, 0.0
+    for inst, u in list(zip(insts, us))[:k]:
+        r = sp.Reservoir(inst.cfg, seed=inst.seed)
+        t = time.perf_counter()
+        r.run_record(u, phi=False)
+        solo_ms += (time.perf_counter() - t) * 1e3
+        solo_ns += inst.n * inst.T
+        r.close()
+    line = {"metric": "batched sweep neuron-steps/s", "value": ns / (ms * 1e-3),
+            "unit": "neuron-steps/s", "n_gpus": 1, "ms_per_run": ms, "instances": len(insts),
+            "neuron_steps_per_run": ns, "build_s": build_s, "ridge_all_s": res["train_s"],
+            "predict_all_s": res["predict_s"], "nrmse_median": float(np.median(res["nrmse"])),
+            "nrmse_min": float(np.min(res["nrmse"])), "schedule": b.info(),
+            "single_path_sample": {"instances": k, "value": solo_ns / (solo_ms * 1e-3)},
+            "dtype": "f64", "data": "synthetic (seeded Mackey-Glass per instance)",
+            "config": {"workload": "sweep of uneven reservoirs", "count": len(insts)}}
+    print(json.dumps(line))
+
+
+def run_search_workload(args):
+    """Surrogate-guided multi-fidelity AGILE against plain AGILE (lockstep
+    chains, every point at full fidelity), same start points and seeds."""
+    import math
+
+    from spires_b200 import search as S
+
+    if args.search_scale == "full":
+        space, task = S.Space(), S.Task(length=16000, val=1000, washout=200)
+        rungs, points, chains = (1000, 4000, 16000), 4096, 64
+    else:
+        space, task = S.Space(), S.Task(length=8000, val=1000, washout=200)
+        rungs, points, chains = (500, 2000, 8000), 1024, 32
+    out = {}
+    for name in ("plain", "surrogate", "no_surrogate"):
+        ev = S.Evaluator(space, task, seed=1)
+        if name == "plain":
+            r = S.plain_agile(ev, chains=chains, T=rungs[-1], seed=0, max_points=points)
+        else:
+            r = S.surrogate_agile(ev, chains=chains, rungs=rungs, max_points=points, waves=4,
+                                  seed=0, use_surrogate=(name == "surrogate"))
+        out[name] = (r, ev.stats)
+    plain = out["plain"][0]
+    target = plain.best_loss + math.log(1.02)
+    line = {"metric": "AGILE wall-clock to plain AGILE's best NRMSE (within 2%)",
+            "unit": "s", "higher_is_better": False,
+            "value": out["surrogate"][0].time_to(target),
+            "plain_wall_s": plain.wall_s, "plain_best_nrmse": plain.best_nrmse,
+            "plain_time_to_best_s": plain.time_to(plain.best_loss)}
+    for name in ("surrogate", "no_surrogate"):
+        r, st = out[name]
+        line[name] = {"best_nrmse": r.best_nrmse, "wall_s": r.wall_s,
+                      "time_to_target_s": r.time_to(target), "evals": r.evals,
+                      "neuron_steps": st.neuron_steps, "build_s": st.build_s,
+                      "surrogate_rmse_logNRMSE": r.extra.get("surrogate_rmse"),
+                      "low_fidelity_rmse_logNRMSE": r.extra.get("low_fidelity_rmse")}
+    line["plain_neuron_steps"] = out["plain"][1].neuron_steps
+    line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
+                      "rungs": list(rungs), "points": points, "chains": chains}
+    line["data"] = "synthetic (seeded Mackey-Glass)"
+    print(json.dumps(line))
+
+
+def run_classify_workload(args):
+    """FLIF_GL N=20000 L=1024 BA m=5 reservoir, 500 bursty-sinusoid sequences
+    of 20..100 frames, reset between sequences, 10-way ridge classifier on
+    the time-averaged states."""
+    from spires_b200 import classify
+
+    out = classify.run_classification(n=N_NEURONS, num_seq=500, seed=0)
+    out.update({"metric": "classification accuracy", "value": out["accuracy"], "unit": "fraction",
+                "states_neuron_steps_per_s": out["neuron_steps"] / out["states_s"],
+                "data": "synthetic (seeded bursty sinusoids)",
+                "config": {"workload": "FLIF_GL N=20000 L=1024 sequence classification"}})
+    print(json.dumps(out))
+
+
+def run_ridge_workload(args):
+    """FLIF_GL N=4000 L=512 Watts-Strogatz k=10, Mackey-Glass T=20000,
+    washout 1000: the ridge readout with the FP64 Gram and with the split
+    tensor-core Grams, errors against the FP64 solution on the same states."""
+    import numpy as np
+
+    import spires_b200 as sp
+    from spires_b200.datasets import mackey_glass
+
+    n, T, w, lam = 4000, 20000, 1000, 1e-6
+    cfg = sp.make_config(n, 1, 1, rho=0.95, ei=0.5, gamma=0.5, conn=10.0 / (n - 1),
+                         topo=sp.CONN_SMALL_WORLD, neuron=sp.FLIF_GL,
+                         nparams=(1.0, 0.0, 0.0, 20.0, 0.7, 512.0, 0.1, 2.0))
+    x = mackey_glass(T + 1, seed=0)
+    u, y = np.ascontiguousarray(x[:-1, None]), np.ascontiguousarray(x[1:, None])
+    r = sp.Reservoir(cfg, seed=42)
+    phi, _, _ = r.run_record(u, phi=True, raster=False)
+    r.close()
+    peak, kind = bf16_peak()
+    rows = []
+    W64 = None
+    for mode in (0, 1, 2, 1, 2):
+        W, rep = sp.ridge_fit(phi, y, lam, washout=w, gram_mode=mode, max_refine=300)
+        yhat = phi[w:] @ W.T
+        nr = float(np.sqrt(np.mean((yhat[:, 0] - y[w:, 0]) ** 2)) / y[w:, 0].std())
+        if mode == 0:
+            W64, n64 = W, nr
+        fl = (3 if mode else 1) * 2.0 * (T - w) * n * n
+        rows.append({"gram_mode": mode, "gram_ms": rep.gram_ms,
+                     "gram_tflops": fl / rep.gram_ms / 1e9, "factor_ms": rep.factor_ms,
+                     "refine_ms": rep.refine_ms, "refine_iters": rep.refine_iters,
+                     "rel_residual": rep.rel_residual,
+                     "w_rel_err": float(np.linalg.norm(W - W64) / np.linalg.norm(W64)),
+                     "nrmse": nr, "nrmse_rel_err": abs(nr - n64) / n64})
+    best = min((x for x in rows[3:] if x["gram_mode"] == 1), key=lambda x: x["gram_ms"])
+    line = {"metric": "ridge Gram TFLOP/s (BF16X3 split, issued flops)",
+            "value": best["gram_tflops"], "unit": "TFLOP/s",
+            "roofline": {"bound": "tensor", "achieved": best["gram_tflops"], "peak": peak,
+                         "unit": "TFLOP/s", "frac": best["gram_tflops"] / peak,
+                         "peak_kind": kind},
+            "modes": rows, "lambda": lam, "dtype": "bf16x3 / tf32x3 / f64",
+            "data": "synthetic (seeded Mackey-Glass)",
+            "config": {"workload": "FLIF_GL N=4000 L=512 WS ridge, T=20000 washout 1000"}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,7 +527,16 @@ def main():
                     help="fill the ring, then one launch of --chunk steps (for ncu -s 1 -c 1)")
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
+    ap.add_argument("--workload", default="step",
+                    choices=["step", "sweep", "search", "classify", "ridge"],
+                    help="step (default, the headline line) or an additional workload")
+    ap.add_argument("--sweep-count", type=int, default=256)
+    ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
     args = ap.parse_args()
+    if args.workload != "step":
+        {"sweep": run_sweep_workload, "search": run_search_workload,
+         "classify": run_classify_workload, "ridge": run_ridge_workload}[args.workload](args)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -134,6 +134,17 @@ spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_se
                                      double lambda, const spires_ext_ridge_opts *opts,
                                      spires_ext_ridge_report *report);
 
+/* Ridge on states the caller already holds (host arrays): states [T x n]
+ * row-major, targets [T x dout], rows [washout, T) fitted; w_out [dout x n].
+ * The reservoir readouts' solver, including the dual form when fewer than
+ * n/2 rows are fitted (the classification workload's 500 time-averaged
+ * states against 20000 neurons) and the split-Gram modes. A singular system
+ * returns SPIRES_ERR_INTERNAL. */
+spires_status spires_ext_ridge_fit(const double *states, size_t T, size_t n,
+                                   const double *targets, size_t dout, double lambda,
+                                   const spires_ext_ridge_opts *opts, double *w_out,
+                                   spires_ext_ridge_report *report);
+
 /* ---- AGILE search core ----------------------------------------------------
  * The black-box optimiser behind spires_optimize (reference src/agile.h:21-91,
  * same option and report layouts): Levy-step exploration with SPSA gradients,

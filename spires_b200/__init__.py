@@ -161,6 +161,8 @@ EXT_SIGNATURES = {
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),
     "spires_ext_train_ridge": (C.c_int, [_VP, _dp, _dp, C.c_size_t, C.c_double,
                                          C.POINTER(RidgeOpts), C.POINTER(RidgeReport)]),
+    "spires_ext_ridge_fit": (C.c_int, [_dp, C.c_size_t, C.c_size_t, _dp, C.c_size_t, C.c_double,
+                                       C.POINTER(RidgeOpts), _dp, C.POINTER(RidgeReport)]),
     "spires_ext_agile_minimize": (C.c_int, [_dp, _dp, _dp, C.c_int, LOSS_FN, _VP,
                                             C.POINTER(AgileOpts), _dp, C.POINTER(AgileReport)]),
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
@@ -550,6 +552,23 @@ class Batch:
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         self.lib.spires_ext_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c))
         return {"ctas": a.value, "groups": b.value, "graph": c.value}
+
+
+def ridge_fit(states, targets, lam, washout=0, gram_mode=0, max_refine=30, lib=None):
+    """spires_ext_ridge_fit: W_out [dout, n] from host states/targets, and the report."""
+    lib = lib or load()
+    X = np.ascontiguousarray(states, np.float64)
+    Y = np.ascontiguousarray(targets, np.float64)
+    if Y.ndim == 1:
+        Y = Y[:, None]
+    W = np.empty((Y.shape[1], X.shape[1]))
+    o = RidgeOpts(gram_mode, max_refine, 1e-13, washout)
+    rep = RidgeReport()
+    st = lib.spires_ext_ridge_fit(dptr(X), X.shape[0], X.shape[1], dptr(Y), Y.shape[1], lam,
+                                  C.byref(o), dptr(W), C.byref(rep))
+    if st != SPIRES_OK:
+        raise RuntimeError(f"spires_ext_ridge_fit failed: {st}")
+    return W, rep
 
 
 def fptr(a: np.ndarray):

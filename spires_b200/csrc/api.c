@@ -816,3 +816,44 @@ SPIRES_EXPORT long long spires_ext_mlp_kernel_launches(const spires_ext_mlp *m)
 {
     return m ? sp_mlp_launches(m->m) : 0;
 }
+
+SPIRES_EXPORT spires_status spires_ext_ridge_fit(const double *states, size_t T, size_t n,
+                                                 const double *targets, size_t dout,
+                                                 double lambda,
+                                                 const spires_ext_ridge_opts *opts,
+                                                 double *w_out, spires_ext_ridge_report *report)
+{
+    if (!states || !targets || !w_out || n == 0 || n > (size_t)INT32_MAX || dout == 0 ||
+        dout > 16)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_opts o;
+    memset(&o, 0, sizeof(o));
+    o.gram_mode = sp_default_gram_mode();
+    o.max_refine = 30;
+    o.refine_tol = 1e-13;
+    if (opts) {
+        o.gram_mode = opts->gram_mode;
+        o.max_refine = opts->max_refine;
+        o.refine_tol = opts->refine_tol;
+        o.washout = opts->washout;
+    }
+    if (o.washout >= T)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ridge_report rep;
+    int rc = sp_ridge_host(states, T, (int)n, targets, (int)dout, lambda, &o, &rep, w_out);
+    if (report) {
+        report->gram_mode_used = rep.gram_mode_used;
+        report->refine_iters = rep.refine_iters;
+        report->rel_residual = rep.rel_residual;
+        report->collect_ms = rep.collect_ms;
+        report->gram_ms = rep.gram_ms;
+        report->factor_ms = rep.factor_ms;
+        report->refine_ms = rep.refine_ms;
+        report->factor_failed = rep.factor_failed;
+        report->lu_fallback = rep.lu_fallback;
+        report->dual = rep.dual;
+    }
+    if (rc == SP_RIDGE_SINGULAR)
+        return SPIRES_ERR_INTERNAL;
+    return to_status(rc);
+}

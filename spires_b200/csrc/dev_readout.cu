@@ -1049,6 +1049,45 @@ out:
     return rc;
 }
 
+// Ridge on caller-provided states (host arrays): Phi [T x n], Y [T x dout];
+// writes W_out [dout x n] to the host. Same solver (and dual/split choices) as
+// the reservoir readouts, on the current device and a stream of its own.
+extern "C" int sp_ridge_host(const double *h_phi, size_t T, int n, const double *h_y, int dout,
+                             double lambda, const sp_ridge_opts *o, sp_ridge_report *rep,
+                             double *h_w_out)
+{
+    int rc = SP_OK;
+    cudaStream_t s = nullptr;
+    double *Phi = nullptr, *Y = nullptr, *Wt = nullptr;
+    memset(rep, 0, sizeof(*rep));
+    if (dout <= 0 || dout > 16 || n <= 0 || T == 0 || o->washout >= T)
+        return SP_EINVAL;
+    auto t0 = std::chrono::steady_clock::now();
+    RK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    RK(cudaMalloc(&Phi, T * (size_t)n * sizeof(double)));
+    RK(cudaMalloc(&Y, T * (size_t)dout * sizeof(double)));
+    RK(cudaMalloc(&Wt, (size_t)n * dout * sizeof(double)));
+    RK(cudaMemcpyAsync(Phi, h_phi, T * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
+    RK(cudaMemcpyAsync(Y, h_y, T * (size_t)dout * sizeof(double), cudaMemcpyHostToDevice, s));
+    RK(cudaStreamSynchronize(s));
+    rep->collect_ms = ms_since(t0);
+    rc = sp_ridge_phi(s, Phi, n, T, Y, dout, lambda, o, rep, Wt);
+    if (rc)
+        goto out;
+    RK(cudaMemcpyAsync(h_w_out, Wt, (size_t)n * dout * sizeof(double), cudaMemcpyDeviceToHost, s));
+    RK(cudaStreamSynchronize(s));
+out:
+    if (s)
+        cudaStreamSynchronize(s);
+    void *bufs[] = {Phi, Y, Wt};
+    for (void *b : bufs)
+        if (b)
+            cudaFree(b);
+    if (s)
+        cudaStreamDestroy(s);
+    return rc;
+}
+
 extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,
                                   const double *h_y, size_t T, double lambda,
                                   const sp_ridge_opts *o, sp_ridge_report *rep, double *h_W_out)

@@ -93,6 +93,9 @@ int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const double *h_u,
                        const double *h_y, size_t T, double lambda,
                        const sp_ridge_opts *o, sp_ridge_report *rep,
                        double *h_W_out);
+int sp_ridge_host(const double *h_phi, size_t T, int n, const double *h_y, int dout,
+                  double lambda, const sp_ridge_opts *o, sp_ridge_report *rep,
+                  double *h_w_out);
 int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double *h_u,
                      const double *h_y, size_t T, double delta, double lambda,
                      double *h_W_out);

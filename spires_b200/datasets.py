@@ -48,11 +48,11 @@ def mackey_glass(T: int, seed: int = 0, batch: int | None = None, tau: float = 1
 
 def bursty_sinusoids(num_seq: int = 500, channels: int = 13, classes: int = 10,
                      len_min: int = 20, len_max: int = 100, seed: int = 0,
-                     p_switch: float = 0.1):
+                     p_switch: float = 0.1, offset_span: float = 0.015):
     """Returns (sequences: list of [len, channels] arrays, labels: [num_seq] int)."""
     rng = np.random.default_rng(seed)
     f0 = rng.uniform(0.01, 0.2, size=(channels, 3))
-    offsets = rng.uniform(-0.015, 0.015, size=(classes, channels, 3))
+    offsets = rng.uniform(-offset_span, offset_span, size=(classes, channels, 3))
     labels = rng.integers(0, classes, size=num_seq)
     seqs = []
     for s in range(num_seq):
