@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -40,6 +41,10 @@ constexpr int kBatchThreads = 256;  // 8 warps per CTA
 
 struct BInst {
     int n, nw, rs, din, L, ntype, micro;
+    long long nnz;  // recurrent edges (schedule cost model)
+    int dense;      // recurrent input from column blocks (see rowpass_columns)
+    const uint2 *cmo;   // [n][nw] {row bits, weight offset} per (column, row word)
+    const double *cw;   // [nnz] weights in column order
     long long T;  // macro steps of the current run
     double a, b, c, d, e, f, g, dt, gamma, v_init, tprev_init;
     double *V, *tprev, *ring;
@@ -48,6 +53,9 @@ struct BInst {
     const int *col;
     const double *w, *W_in, *coef;
     const int *nid_of, *pos_of;
+    // layout of W_out and of the readout sums: the single-reservoir path's
+    // (equal to nid_of / pos_of except for column-block instances)
+    const int *nid_ro, *pos_ro;
     const double *u;       // [T][din]
     double *phi;           // [T][rs] position order, or null
     unsigned *raster;      // [T][nw] position order
@@ -61,6 +69,8 @@ struct BParams {
     unsigned long long *bar;  // one arrival counter per group
     int *err;
     int lmax;                 // longest FLIF_GL ring of the batch (coefficients in smem)
+    int max_nw;               // most spike words of an instance
+    int list_cap;             // largest column-block instance (spike list in smem)
 };
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p)
@@ -162,6 +172,87 @@ __device__ __forceinline__ double rowpass_simple_warp_deep(const long long *__re
     return acc;
 }
 
+// SIMPLE-synapse recurrent input from column blocks, for dense matrices.
+// Bits of row word q (rows 32q..32q+31) of column j say which of those rows
+// have an edge from neuron j; the block's weights are stored contiguously in
+// row order from its offset. The lane of row i walks the list of spiking
+// neurons in ascending order and adds w_ij where the bit is set: exactly the
+// non-zero terms of csr_row_dot (src/sparse.c:68-76) in ascending column
+// order, reading 8 bytes per spiking column per 32 rows instead of 12 bytes per
+// stored edge. Blocks are fetched C columns ahead.
+__device__ __forceinline__ double rowpass_columns(const uint2 *__restrict__ cmo,
+                                                  const double *__restrict__ cw,
+                                                  const int *s_list, int cnt, int nw, int q,
+                                                  int lane)
+{
+    constexpr int C = 8;
+    const unsigned below = (1u << lane) - 1u;
+    double acc = 0.0;
+    uint2 cur[C], nxt[C];
+#pragma unroll
+    for (int u = 0; u < C; ++u)
+        cur[u] = u < cnt ? __ldg(cmo + (size_t)s_list[u] * nw + q) : make_uint2(0u, 0u);
+    for (int t = 0; t < cnt; t += C) {
+#pragma unroll
+        for (int u = 0; u < C; ++u)
+            nxt[u] = t + C + u < cnt ? __ldg(cmo + (size_t)s_list[t + C + u] * nw + q)
+                                     : make_uint2(0u, 0u);
+        double wv[C];
+#pragma unroll
+        for (int u = 0; u < C; ++u)
+            wv[u] = ((cur[u].x >> lane) & 1u) ? __ldg(cw + cur[u].y + __popc(cur[u].x & below))
+                                              : 0.0;
+#pragma unroll
+        for (int u = 0; u < C; ++u)
+            if ((cur[u].x >> lane) & 1u)
+                acc = add(acc, wv[u]);
+#pragma unroll
+        for (int u = 0; u < C; ++u)
+            cur[u] = nxt[u];
+    }
+    return acc;
+}
+
+// Ascending list of the spiking positions from the CTA's spike words: each
+// thread takes a contiguous range of words, a block scan of their bit counts
+// gives its write offset. Returns the count (all threads).
+__device__ __forceinline__ int spike_list(const unsigned *s_spk, int nw, int *s_list,
+                                          int *s_warp)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (nw + kBatchThreads - 1) / kBatchThreads;
+    const int w0 = tid * per < nw ? tid * per : nw;
+    const int w1 = w0 + per < nw ? w0 + per : nw;
+    int c = 0;
+    for (int wi = w0; wi < w1; ++wi)
+        c += __popc(s_spk[wi]);
+    int x = c;  // inclusive warp scan
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, off);
+        if (lane >= off)
+            x += y;
+    }
+    if (lane == 31)
+        s_warp[warp] = x;
+    __syncthreads();
+    int base = x - c;
+    for (int k = 0; k < warp; ++k)
+        base += s_warp[k];
+    int total = 0;
+    for (int k = 0; k < kBatchThreads / 32; ++k)
+        total += s_warp[k];
+    for (int wi = w0; wi < w1; ++wi) {
+        unsigned m = s_spk[wi];
+        while (m) {
+            s_list[base++] = wi * 32 + __ffs(m) - 1;
+            m &= m - 1;
+        }
+    }
+    __syncthreads();  // list complete; s_warp free again
+    return total;
+}
+
 // One persistent cooperative launch over the whole batch. CTA c belongs to
 // group cta_group[c] (or to none, then it returns at once); a group runs its
 // job list in order, splitting each instance's warps evenly over its CTAs,
@@ -173,8 +264,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     double *s_coef = (double *)s_dyn;                    // [lmax]
-    unsigned *s_spk = (unsigned *)(s_coef + p.lmax);     // [nw]
+    unsigned *s_spk = (unsigned *)(s_coef + p.lmax);     // [max_nw]
+    int *s_list = (int *)(s_spk + p.max_nw);             // [list_cap]
     __shared__ int s_flag, s_abort;
+    __shared__ int s_warp[kBatchThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int grp = p.cta_group[blockIdx.x];
     if (grp < 0)
@@ -283,7 +376,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
                 s_spk[wi] = __ldcg(I.spk + (size_t)cur * nw + wi);
             __syncthreads();
             double rec = 0.0;
-            if (wact) {
+            if (I.dense) {
+                const int cnt = spike_list(s_spk, nw, s_list, s_warp);
+                if (wact)
+                    rec = rowpass_columns(I.cmo, I.cw, s_list, cnt, nw, gw, lane);
+            } else if (wact) {
                 // warp-uniform choice: long edge ranges take the deep pipeline
                 const long long span = __ldg(I.row_ptr + gw * 32 + 32) - __ldg(I.row_ptr + gw * 32);
                 rec = span > 256 ? rowpass_simple_warp_deep<8>(I.row_ptr, I.col, I.w, s_spk,
@@ -357,6 +454,21 @@ __global__ void k_batch_reset(const BInst *inst)
             I.ring[k] = I.v_init;
 }
 
+// out[t][q] = in[t][nid[q]] (0 at holes): states of a column-block instance
+// (neuron order) in its readout layout.
+__global__ void k_rows_to_layout(const double *__restrict__ in, int rs,
+                                 const int *__restrict__ nid, size_t T, double *__restrict__ out)
+{
+    const size_t total = T * (size_t)rs;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = k / rs;
+        const int q = (int)(k % rs);
+        const int i = nid[q];
+        out[k] = i >= 0 ? in[t * rs + i] : 0.0;
+    }
+}
+
 // Rasters and final states of every instance back in neuron order.
 __global__ void k_batch_gather(const BInst *inst)
 {
@@ -390,6 +502,7 @@ struct sp_batch {
     int device = 0, num_sms = 0, P = 0;
     size_t smem = 0;
     int lmax = 0;
+    int max_nw = 1, list_cap = 0;
     cudaStream_t stream = nullptr;
     std::vector<sp_host_model> models;
     std::vector<BInst> inst;
@@ -464,18 +577,29 @@ extern "C" void sp_batch_destroy(sp_batch *b)
 static int min_ctas(const BInst &I) { return (I.nw + kBatchThreads / 32 - 1) / (kBatchThreads / 32); }
 
 // Estimated seconds for one instance on g CTAs: the larger of a per-step
-// latency floor (the history chunks wait for memory one after another) and the
-// instance's share of the CTAs' streaming rate.
+// latency floor and the instance's share of the CTAs' streaming rate. The
+// floor adds the barrier, the row pass (its warps scan 256 edges per memory
+// round trip on long rows, 32 on short ones) and the FLIF_GL history (16 ring
+// values per round trip); the bytes are the CSR scan (column + weight per
+// edge), the history ring and the neuron state.
 static double est_time(const BInst &I, long long T, int g)
 {
-    const double cta_bw = 20e9;  // bytes/s one CTA streams
+    const double cta_bw = 20e9;   // bytes/s one CTA streams
+    const double trip = 0.35e-6;  // one dependent memory round trip
     const double steps = (double)T * I.micro;
-    if (I.ntype == SP_FLIF_GL) {
-        const double floor_s = 2e-6 + 0.4e-6 * ((I.L + kHistChunk - 1) / kHistChunk);
-        const double mem = 8.0 * I.n * (double)I.L / (g * cta_bw);
-        return steps * std::max(floor_s, mem);
+    const double span = (double)I.nnz / (I.nw > 0 ? I.nw : 1);  // edges per warp
+    double rows = span > 256 ? std::ceil(span / 256.0) : std::ceil(span / 32.0);
+    double bytes = 12.0 * (double)I.nnz + 24.0 * I.n;
+    if (I.dense) {  // column blocks: about a tenth of the columns spike per step
+        rows = std::ceil(0.1 * I.n / 8.0);
+        bytes = 0.8 * I.n * (double)I.nw + 0.8 * (double)I.nnz + 24.0 * I.n;
     }
-    return steps * std::max(2e-6, 64.0 * I.n / (g * cta_bw));
+    double floor_s = 2e-6 + trip * rows;
+    if (I.ntype == SP_FLIF_GL) {
+        floor_s += trip * ((I.L + kHistChunk - 1) / kHistChunk);
+        bytes += 8.0 * I.n * (double)I.L;
+    }
+    return steps * std::max(floor_s, bytes / (g * cta_bw));
 }
 
 // Static schedule: instances in the given order go to the existing group
@@ -539,8 +663,119 @@ static bool plan_order(sp_batch *b, const std::vector<int> &order, const std::ve
 // Heaviest first (longest-processing-time list scheduling); if a wide
 // instance then finds every CTA taken by narrower groups, plan again widest
 // first, which always succeeds because every instance fits the grid.
+// Size-class schedule: every instance runs on a group whose width is its
+// minimum CTA count rounded up to a power of two; each class gets one group,
+// then the free CTAs go one group at a time to the class with the longest
+// estimated time per group (balancing the classes' finish times), and each
+// class's instances are dealt heaviest first to its least busy group.
+// Many narrow groups keep every SM busy with instances that each run at their
+// own per-step latency. Returns false when the classes do not fit the grid.
+static bool plan_classes(sp_batch *b, const std::vector<long long> &T)
+{
+    const int P = b->P;
+    const size_t cnt = b->inst.size();
+    std::vector<int> width(cnt);
+    std::vector<int> classes;
+    for (size_t k = 0; k < cnt; ++k) {
+        int w = 1;
+        while (w < min_ctas(b->inst[k]))
+            w <<= 1;
+        if (w > P)
+            w = min_ctas(b->inst[k]);
+        width[k] = w;
+        if (std::find(classes.begin(), classes.end(), w) == classes.end())
+            classes.push_back(w);
+    }
+    std::sort(classes.begin(), classes.end(), std::greater<int>());
+    std::vector<double> work(classes.size(), 0.0);
+    std::vector<int> members(classes.size(), 0);
+    for (size_t k = 0; k < cnt; ++k) {
+        const size_t c = std::find(classes.begin(), classes.end(), width[k]) - classes.begin();
+        work[c] += est_time(b->inst[k], T[k], width[k]);
+        members[c]++;
+    }
+    int need = 0;
+    for (int w : classes)
+        need += w;
+    if (need > P)
+        return false;
+    double total = 0.0;
+    for (double x : work)
+        total += x;
+    std::vector<int> ngroups(classes.size(), 1);
+    int used = need;
+    // hand out the remaining CTAs one group at a time to the class whose
+    // time per group is longest
+    for (;;) {
+        int bestc = -1;
+        double bestload = 0.0;
+        for (size_t c = 0; c < classes.size(); ++c) {
+            if (used + classes[c] > P || ngroups[c] >= members[c])
+                continue;
+            const double load = work[c] / ngroups[c];
+            if (bestc < 0 || load > bestload) {
+                bestload = load;
+                bestc = (int)c;
+            }
+        }
+        if (bestc < 0)
+            break;
+        ngroups[bestc]++;
+        used += classes[bestc];
+    }
+    (void)total;
+    struct G {
+        int start, size;
+        double busy;
+        std::vector<int> jobs;
+    };
+    std::vector<G> groups;
+    std::vector<int> first(classes.size());
+    int start = 0;
+    for (size_t c = 0; c < classes.size(); ++c) {
+        first[c] = (int)groups.size();
+        for (int q = 0; q < ngroups[c]; ++q) {
+            groups.push_back(G{start, classes[c], 0.0, {}});
+            start += classes[c];
+        }
+    }
+    std::vector<int> order(cnt);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<double> est(cnt);
+    for (size_t k = 0; k < cnt; ++k)
+        est[k] = est_time(b->inst[k], T[k], width[k]);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return est[x] > est[y]; });
+    for (int k : order) {
+        const size_t c = std::find(classes.begin(), classes.end(), width[k]) - classes.begin();
+        int best = first[c];
+        for (int gi = first[c]; gi < first[c] + ngroups[c]; ++gi)
+            if (groups[gi].busy < groups[best].busy)
+                best = gi;
+        groups[best].busy += est[k];
+        groups[best].jobs.push_back(k);
+    }
+    b->ngroups = (int)groups.size();
+    b->cta_group.assign(P, -1);
+    b->group_start.clear();
+    b->group_size.clear();
+    b->job_off.assign(1, 0);
+    b->jobs.clear();
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        for (int q = 0; q < groups[gi].size; ++q)
+            b->cta_group[groups[gi].start + q] = (int)gi;
+        b->group_start.push_back(groups[gi].start);
+        b->group_size.push_back(groups[gi].size);
+        for (int k : groups[gi].jobs)
+            b->jobs.push_back(k);
+        b->job_off.push_back((int)b->jobs.size());
+    }
+    return true;
+}
+
 static void plan(sp_batch *b, const std::vector<long long> &T)
 {
+    if (plan_classes(b, T))
+        return;
     const size_t cnt = b->inst.size();
     std::vector<int> order(cnt);
     std::iota(order.begin(), order.end(), 0);
@@ -587,11 +822,12 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
     b->inst.resize(count);
     b->w_pos.resize(count);
     struct Off {
-        size_t V, tp, ring, spk, rp, col, w, win, coef, nid, pos, wout;
+        size_t V, tp, ring, spk, rp, col, w, win, coef, nid, pos, wout, cmo, cw, nro, pro;
     };
     std::vector<Off> off(count);
     std::vector<std::vector<int>> pos(count), nid(count);
     size_t max_nw = 1;
+    int list_cap = 0;
     for (size_t k = 0; k < count; ++k) {
         const sp_host_model &m = b->models[k];
         BInst &I = b->inst[k];
@@ -603,6 +839,11 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         I.L = m.neuron_type == SP_FLIF_GL ? m.nc.L : 1;
         I.ntype = m.neuron_type;
         I.micro = m.micro_steps;
+        I.nnz = (long long)m.nnz;
+        // column blocks when at least one edge in 256 pairs is present (the
+        // spike list of up to 16384 neurons fits shared memory)
+        I.dense = m.nnz > 0 && (double)m.nnz * 256.0 >= (double)m.n * (double)m.n &&
+                  m.n <= 16384 && m.nnz < 0xFFFFFFFFull;
         I.a = m.nc.a;
         I.b = m.nc.b;
         I.c = m.nc.c;
@@ -624,15 +865,23 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         o.ring = take(I.ntype == SP_FLIF_GL ? rs * (size_t)I.L * 8 : 8);
         o.spk = take(2 * (size_t)I.nw * 4);
         o.rp = take((rs + 1) * 8);
-        o.col = take((m.nnz ? m.nnz : 1) * 4);
-        o.w = take((m.nnz ? m.nnz : 1) * 8);
+        o.col = take((I.dense || !m.nnz ? 1 : m.nnz) * 4);
+        o.w = take((I.dense || !m.nnz ? 1 : m.nnz) * 8);
+        o.cmo = take(I.dense ? (size_t)m.n * I.nw * 8 : 8);
+        o.cw = take(I.dense ? m.nnz * 8 : 8);
+        o.nro = take(I.dense ? rs * 4 : 8);
+        o.pro = take(I.dense ? m.n * 4 : 8);
+        if (I.dense)
+            list_cap = std::max(list_cap, (int)m.n);
         o.win = take(rs * (m.din ? m.din : 1) * 8);
         o.coef = take((size_t)I.L * 8);
         o.nid = take(rs * 4);
         o.pos = take(m.n * 4);
         o.wout = take(rs * (m.dout ? m.dout : 1) * 8);
     }
-    b->smem = (size_t)b->lmax * 8 + max_nw * 4;
+    b->max_nw = (int)max_nw;
+    b->list_cap = list_cap;
+    b->smem = (size_t)b->lmax * 8 + max_nw * 4 + (size_t)list_cap * 4;
     int rc = SP_OK;
     int per_sm = 0;
     if (b->smem > 200 * 1024)
@@ -671,26 +920,70 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         const Off &o = off[k];
         char *A = b->arena;
         const size_t rs = I.rs;
-        sp_make_layout(&m, I.nw, pos[k], nid[k]);
+        std::vector<int> pos_ro, nid_ro;  // readout layout of column-block instances
+        if (I.dense) {
+            // column blocks read spike lists in neuron order: identity layout;
+            // W_out and the readout sums keep the single path's layout
+            sp_make_layout(&m, I.nw, pos_ro, nid_ro);
+            pos[k].resize(m.n);
+            nid[k].assign(rs, -1);
+            for (size_t i = 0; i < m.n; ++i) {
+                pos[k][i] = (int)i;
+                nid[k][i] = (int)i;
+            }
+        } else {
+            sp_make_layout(&m, I.nw, pos[k], nid[k]);
+        }
         // CSR in position order, as the single-reservoir path lays it out
+        // (column-block instances keep only empty rows here)
+        const size_t ecap = (I.dense || !m.nnz) ? 1 : m.nnz;
         std::vector<long long> rp(rs + 1, 0);
-        std::vector<int> col(m.nnz ? m.nnz : 1);
-        std::vector<double> w(m.nnz ? m.nnz : 1), win(rs * (m.din ? m.din : 1), 0.0),
+        std::vector<int> col(ecap);
+        std::vector<double> w(ecap), win(rs * (m.din ? m.din : 1), 0.0),
             wout(rs * (m.dout ? m.dout : 1), 0.0);
+        std::vector<uint2> cmo;
+        std::vector<double> cw;
+        if (I.dense) {
+            // blocks (column j, row word q): row bits and the offset of the
+            // block's weights, stored column by column in row order
+            cmo.assign((size_t)m.n * I.nw, make_uint2(0u, 0u));
+            cw.resize(m.nnz);
+            std::vector<long long> cstart(m.n + 1, 0);
+            for (size_t kk = 0; kk < m.nnz; ++kk)
+                cstart[m.col[kk] + 1]++;
+            for (size_t j = 0; j < m.n; ++j)
+                cstart[j + 1] += cstart[j];
+            std::vector<long long> fill(cstart.begin(), cstart.end() - 1);
+            for (size_t i = 0; i < m.n; ++i)
+                for (int64_t kk = m.row_ptr[i]; kk < m.row_ptr[i + 1]; ++kk) {
+                    const int j = m.col[kk];
+                    cw[fill[j]++] = m.w[kk];
+                    cmo[(size_t)j * I.nw + i / 32].x |= 1u << (i % 32);
+                }
+            for (size_t j = 0; j < m.n; ++j) {
+                long long run = cstart[j];
+                for (int q = 0; q < I.nw; ++q) {
+                    cmo[(size_t)j * I.nw + q].y = (unsigned)run;
+                    run += __builtin_popcount(cmo[(size_t)j * I.nw + q].x);
+                }
+            }
+        }
         size_t e = 0;
         for (size_t q = 0; q < rs; ++q) {
             rp[q] = (long long)e;
             const int i = nid[k][q];
             if (i < 0)
                 continue;
-            for (int64_t kk = m.row_ptr[i]; kk < m.row_ptr[i + 1]; ++kk, ++e) {
-                col[e] = pos[k][m.col[kk]];
-                w[e] = m.w[kk];
-            }
+            if (!I.dense)
+                for (int64_t kk = m.row_ptr[i]; kk < m.row_ptr[i + 1]; ++kk, ++e) {
+                    col[e] = pos[k][m.col[kk]];
+                    w[e] = m.w[kk];
+                }
             for (size_t j = 0; j < m.din; ++j)
                 win[q * m.din + j] = m.W_in[(size_t)i * m.din + j];
-            for (size_t oo = 0; oo < m.dout; ++oo)
-                wout[oo * rs + q] = m.W_out[oo * m.n + i];
+            if (!I.dense)
+                for (size_t oo = 0; oo < m.dout; ++oo)
+                    wout[oo * rs + q] = m.W_out[oo * m.n + i];
         }
         rp[rs] = (long long)e;
         I.V = (double *)(A + o.V);
@@ -705,6 +998,17 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         I.nid_of = (const int *)(A + o.nid);
         I.pos_of = (const int *)(A + o.pos);
         b->w_pos[k] = (double *)(A + o.wout);
+        I.cmo = (const uint2 *)(A + o.cmo);
+        I.cw = (const double *)(A + o.cw);
+        I.nid_ro = I.dense ? (const int *)(A + o.nro) : I.nid_of;
+        I.pos_ro = I.dense ? (const int *)(A + o.pro) : I.pos_of;
+        if (I.dense)
+            for (size_t q = 0; q < rs; ++q) {
+                const int i = nid_ro[q];
+                if (i >= 0)
+                    for (size_t oo = 0; oo < m.dout; ++oo)
+                        wout[oo * rs + q] = m.W_out[oo * m.n + i];
+            }
         // synchronous copies: the staging vectors die at the end of this iteration
         bool ok = cudaMemcpy(A + o.rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice) ==
                       cudaSuccess &&
@@ -720,6 +1024,15 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
                       cudaSuccess &&
                   cudaMemcpy(A + o.pos, pos[k].data(), m.n * 4, cudaMemcpyHostToDevice) ==
                       cudaSuccess;
+        if (ok && I.dense)
+            ok = cudaMemcpy(A + o.nro, nid_ro.data(), rs * 4, cudaMemcpyHostToDevice) ==
+                     cudaSuccess &&
+                 cudaMemcpy(A + o.pro, pos_ro.data(), m.n * 4, cudaMemcpyHostToDevice) ==
+                     cudaSuccess &&
+                 cudaMemcpy(A + o.cmo, cmo.data(), cmo.size() * 8, cudaMemcpyHostToDevice) ==
+                     cudaSuccess &&
+                 cudaMemcpy(A + o.cw, cw.data(), cw.size() * 8, cudaMemcpyHostToDevice) ==
+                     cudaSuccess;
         if (ok && I.ntype == SP_FLIF_GL)
             ok = cudaMemcpy(A + o.coef, m.coef, (size_t)I.L * 8, cudaMemcpyHostToDevice) ==
                  cudaSuccess;
@@ -828,6 +1141,8 @@ static int batch_enqueue(sp_batch *b)
     p.bar = b->d_bar;
     p.err = b->d_err;
     p.lmax = b->lmax;
+    p.max_nw = b->max_nw;
+    p.list_cap = b->list_cap;
     void *args[] = {&p};
     BK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(P), dim3(kBatchThreads), args,
                                    b->smem, b->stream));
@@ -923,6 +1238,30 @@ extern "C" int sp_batch_run(sp_batch *b, const double *const *u, const size_t *T
     return SP_OK;
 }
 
+// Readouts of one instance over its recorded states, with the single path's
+// layout and reduction (so the bits match spires_run): column-block
+// instances first move their states from neuron order to that layout.
+static int batch_readout(sp_batch *b, const BInst &I, const double *phi, size_t T, int dout,
+                         double *Y)
+{
+    if (!I.dense)
+        return sp_launch_readout(b->stream, b->w_pos[&I - b->inst.data()], phi, I.rs, T, dout, Y);
+    double *tmp = nullptr;
+    if (cudaMallocAsync(&tmp, (T ? T : 1) * (size_t)I.rs * sizeof(double), b->stream) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return SP_EALLOC;
+    }
+    const size_t total = T * (size_t)I.rs;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 16384);
+    k_rows_to_layout<<<blocks ? blocks : 1, 256, 0, b->stream>>>(phi, I.rs, I.nid_ro, T, tmp);
+    int rc = cudaGetLastError() == cudaSuccess ? SP_OK : SP_EINTERNAL;
+    if (!rc)
+        rc = sp_launch_readout(b->stream, b->w_pos[&I - b->inst.data()], tmp, I.rs, T, dout, Y);
+    cudaFreeAsync(tmp, b->stream);
+    return rc;
+}
+
 // Ridge readouts of every instance from one batched simulation: states of
 // all instances recorded in one launch, then per instance the FP64 ridge of
 // the single-reservoir path (Gram + Cholesky + refinement) on its states.
@@ -983,7 +1322,7 @@ extern "C" int sp_batch_train_ridge(sp_batch *b, const double *const *u, const d
             // singular: W_out of this instance stays as it was (dgesv failure)
             rc = SP_OK;
             if (w_out && w_out[k]) {
-                rc = sp_launch_gather_rows(b->stream, b->w_pos[k], I.rs, I.pos_of, I.n,
+                rc = sp_launch_gather_rows(b->stream, b->w_pos[k], I.rs, I.pos_ro, I.n,
                                            (size_t)dout, W);
                 if (!rc && cudaMemcpy(w_out[k], W, (size_t)dout * I.n * 8,
                                       cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -993,7 +1332,7 @@ extern "C" int sp_batch_train_ridge(sp_batch *b, const double *const *u, const d
         }
         if (rc)
             break;
-        rc = sp_launch_wout_to_pos(b->stream, W, I.nid_of, I.n, I.rs, dout, b->w_pos[k]);
+        rc = sp_launch_wout_to_pos(b->stream, W, I.nid_ro, I.n, I.rs, dout, b->w_pos[k]);
         if (!rc && w_out && w_out[k] &&
             cudaMemcpyAsync(w_out[k], W, (size_t)dout * I.n * 8, cudaMemcpyDeviceToHost,
                             b->stream) != cudaSuccess)
@@ -1033,7 +1372,7 @@ extern "C" int sp_batch_predict(sp_batch *b, const double *const *u, const size_
         po += T[k] * I.rs;
         if (dout == 0 || !y || !y[k])
             continue;
-        rc = sp_launch_readout(b->stream, b->w_pos[k], phi, I.rs, T[k], dout, Y);
+        rc = batch_readout(b, I, phi, T[k], dout, Y);
         if (!rc && cudaMemcpyAsync(y[k], Y, T[k] * dout * 8, cudaMemcpyDeviceToHost, b->stream) !=
                        cudaSuccess)
             rc = SP_EINTERNAL;
@@ -1101,7 +1440,7 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
         if (rc == SP_RIDGE_SINGULAR) {
             rc = SP_OK; /* this instance keeps its previous W_out */
         } else if (!rc) {
-            rc = sp_launch_wout_to_pos(b->stream, W, I.nid_of, I.n, I.rs, dout, b->w_pos[k]);
+            rc = sp_launch_wout_to_pos(b->stream, W, I.nid_ro, I.n, I.rs, dout, b->w_pos[k]);
             if (!rc && w_out && w_out[k] &&
                 cudaMemcpyAsync(w_out[k], W, (size_t)dout * I.n * 8, cudaMemcpyDeviceToHost,
                                 b->stream) != cudaSuccess)
@@ -1109,7 +1448,7 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
         }
         if (rc)
             break;
-        rc = sp_launch_readout(b->stream, b->w_pos[k], phi, I.rs, T[k], dout, Y);
+        rc = batch_readout(b, I, phi, T[k], dout, Y);
         if (!rc && y_out && y_out[k] &&
             cudaMemcpyAsync(y_out[k], Y, T[k] * dout * 8, cudaMemcpyDeviceToHost, b->stream) !=
                 cudaSuccess)
