@@ -427,7 +427,7 @@ def run_search_workload(args):
         if name == "plain":
             r = S.plain_agile(ev, chains=chains, T=rungs[-1], seed=0, max_points=points)
         else:
-            r = S.surrogate_agile(ev, chains=chains, rungs=rungs, max_points=points, waves=4,
+            r = S.surrogate_agile(ev, chains=chains, rungs=rungs, max_points=points, waves=8,
                                   seed=0, use_surrogate=(name == "surrogate"))
         out[name] = (r, ev.stats)
     plain = out["plain"][0]
@@ -446,7 +446,7 @@ def run_search_workload(args):
                       "low_fidelity_rmse_logNRMSE": r.extra.get("low_fidelity_rmse")}
     line["plain_neuron_steps"] = out["plain"][1].neuron_steps
     line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
-                      "rungs": list(rungs), "points": points, "chains": chains}
+                      "rungs": list(rungs), "points": points, "chains": chains, "waves": 8}
     line["data"] = "synthetic (seeded Mackey-Glass)"
     print(json.dumps(line))
 

@@ -99,7 +99,7 @@ spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed);
  * create time (reference src/sparse.c:93-127) on an n x n CSR matrix with
  * ascending columns: on the current CUDA device (on_device = 1) or on the
  * host (0). Both give the same bits; spires_reservoir_create uses the device
- * for matrices with at least 2^18 edges unless SPIRES_HOST_SPECTRAL_RADIUS=1. */
+ * for matrices with at least 2^15 edges unless SPIRES_HOST_SPECTRAL_RADIUS=1. */
 spires_status spires_ext_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
                                          const double *w, int on_device, double *out);
 
@@ -273,6 +273,12 @@ spires_status spires_ext_batch_fit_predict(spires_ext_batch *b, const double *co
                                            const spires_ext_ridge_opts *opts,
                                            double *const *y_out, double *const *w_out,
                                            double *elapsed_ms);
+
+/* Wall-clock milliseconds of spires_ext_batch_create: host construction of
+ * the instances, and the device set-up (layouts, recurrent-input formats,
+ * uploads). */
+spires_status spires_ext_batch_timing(const spires_ext_batch *b, double *construct_ms,
+                                      double *setup_ms);
 
 /* Schedule of the last run: CTAs of the grid, CTA groups, and whether the
  * launch sequence runs as a CUDA graph (1) or as direct launches (-1). */

@@ -199,6 +199,7 @@ EXT_SIGNATURES = {
                                                C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), _dp,
                                                C.POINTER(RidgeOpts), C.POINTER(_dp),
                                                C.POINTER(_dp), _dp]),
+    "spires_ext_batch_timing": (C.c_int, [_VP, _dp, _dp]),
     "spires_ext_batch_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                         C.POINTER(C.c_int)]),
 }
@@ -547,6 +548,12 @@ class Batch:
         if st != SPIRES_OK:
             raise RuntimeError(f"spires_ext_batch_fit_predict failed: {st}")
         return Y, ms.value
+
+    def timing(self):
+        """(construct_ms, setup_ms) of the batch's creation."""
+        a, b = C.c_double(), C.c_double()
+        self.lib.spires_ext_batch_timing(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def info(self):
         a, b, c = C.c_int(), C.c_int(), C.c_int()

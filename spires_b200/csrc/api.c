@@ -12,6 +12,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include "../../include/spires.h"
 #include "../../include/spires_ext.h"
 #include "sp_model.h"
@@ -560,7 +561,16 @@ SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
 struct spires_ext_batch {
     sp_batch *b;
     size_t count;
+    double construct_ms; /* host construction of every instance */
+    double setup_ms;     /* layouts, recurrent-input formats, device uploads */
 };
+
+static double now_ms(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return 1e3 * (double)t.tv_sec + 1e-6 * (double)t.tv_nsec;
+}
 
 SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_config *cfgs,
                                                     const unsigned *seeds, size_t count,
@@ -577,6 +587,7 @@ SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_confi
         return SPIRES_ERR_ALLOC;
     }
     int rc = SP_OK;
+    const double t0 = now_ms();
     if (seeds) {
         /* independent private generators: instances build on all host threads */
         const int dev = sp_dev_current_device();
@@ -605,8 +616,11 @@ SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_confi
                 rc = sp_model_build(&ms[k]);
         }
     }
+    const double t1 = now_ms();
     if (!rc)
         rc = sp_batch_create(ms, count, &h->b);
+    h->construct_ms = t1 - t0;
+    h->setup_ms = now_ms() - t1;
     if (rc) {
         for (size_t k = 0; k < count; ++k)
             sp_model_free(&ms[k]); /* no-op on zeroed or never-built entries */
@@ -856,4 +870,16 @@ SPIRES_EXPORT spires_status spires_ext_ridge_fit(const double *states, size_t T,
     if (rc == SP_RIDGE_SINGULAR)
         return SPIRES_ERR_INTERNAL;
     return to_status(rc);
+}
+
+SPIRES_EXPORT spires_status spires_ext_batch_timing(const spires_ext_batch *b, double *construct_ms,
+                                                    double *setup_ms)
+{
+    if (!b)
+        return SPIRES_ERR_INVALID_ARG;
+    if (construct_ms)
+        *construct_ms = b->construct_ms;
+    if (setup_ms)
+        *setup_ms = b->setup_ms;
+    return SPIRES_OK;
 }

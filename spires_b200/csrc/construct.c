@@ -494,7 +494,7 @@ done:
 /* csr_spectral_radius, src/sparse.c:93-127 (max-abs normalised power
  * iteration, tol 1e-6, at most 1000 iterations, x0 = 1). */
 /* edge count from which the power iteration runs on the device */
-#define SP_DEVICE_SR_MIN_NNZ ((size_t)1 << 18)
+#define SP_DEVICE_SR_MIN_NNZ ((size_t)1 << 15)
 
 double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
                               const double *w)

@@ -139,12 +139,16 @@ class Evaluator:
         return int((self.seed * 0x9E3779B1 + int(cid) * 0x85EBCA77) & 0x7FFFFFFF) or 1
 
     def evaluate(self, thetas, T, ids):
+        return self.evaluate_rungs(thetas, (T,), ids)[0]
+
+    def evaluate_rungs(self, thetas, rungs, ids):
+        """Losses of the same candidates at several training lengths, each
+        reservoir built once (list of arrays, one per length)."""
         thetas = np.atleast_2d(thetas)
-        out = np.full(len(thetas), FAIL_LOSS)
+        outs = [np.full(len(thetas), FAIL_LOSS) for _ in rungs]
         if len(thetas) == 0:
-            return out
-        u, y = self.task.series(T)
-        total = T + self.task.val
+            return outs
+        total = max(rungs) + self.task.val
         cfgs, decs = zip(*[self.space.config(th) for th in thetas])
         chunks, cur, acc = [], [], 0.0
         for k in range(len(thetas)):
@@ -157,27 +161,31 @@ class Evaluator:
         if cur:
             chunks.append(cur)
         t0 = time.perf_counter()
-        yv = y[T:, 0]
-        sd = yv.std()
         for ch in chunks:
             tb = time.perf_counter()
             batch = Batch([cfgs[k] for k in ch], [self.instance_seed(ids[k]) for k in ch])
             tf = time.perf_counter()
             lams = [decs[k]["lam"] for k in ch]
-            Y, _ = batch.fit_predict([u] * len(ch), [y] * len(ch), [T] * len(ch), lams,
-                                     washout=min(self.task.washout, T // 2))
+            for out, T in zip(outs, rungs):
+                u, y = self.task.series(T)
+                yv = y[T:, 0]
+                sd = yv.std()
+                Y, _ = batch.fit_predict([u] * len(ch), [y] * len(ch), [T] * len(ch), lams,
+                                         washout=min(self.task.washout, T // 2))
+                for j, k in enumerate(ch):
+                    e = Y[j][T:, 0] - yv
+                    nr = math.sqrt(float(np.mean(e * e))) / (sd if sd > 0 else 1.0)
+                    out[k] = (min(math.log(nr), FAIL_LOSS) if np.isfinite(nr) and nr > 0
+                              else FAIL_LOSS)
+                self.stats.neuron_steps += sum(decs[k]["n"] for k in ch) * float(
+                    T + self.task.val)
             batch.close()
             self.stats.build_s += tf - tb
             self.stats.fit_s += time.perf_counter() - tf
-            for j, k in enumerate(ch):
-                e = Y[j][T:, 0] - yv
-                nr = math.sqrt(float(np.mean(e * e))) / (sd if sd > 0 else 1.0)
-                out[k] = min(math.log(nr), FAIL_LOSS) if np.isfinite(nr) and nr > 0 else FAIL_LOSS
-            self.stats.neuron_steps += sum(decs[k]["n"] for k in ch) * float(total)
         self.stats.sim_s += time.perf_counter() - t0
-        self.stats.evals += len(thetas)
+        self.stats.evals += len(thetas) * len(rungs)
         self.stats.calls += 1
-        return out
+        return outs
 
 
 @dataclass
@@ -246,7 +254,7 @@ def plain_agile(ev: Evaluator, chains: int = 16, T: int = 16000, seed: int = 0,
 
 
 def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), keep: float = 0.1,
-                    max_points: int = 4096, waves: int = 4, seed: int = 0,
+                    max_points: int = 4096, waves: int = 8, seed: int = 0,
                     opts: AgileOpts | None = None, use_surrogate: bool = True, epochs: int = 200,
                     calibration: int = 8, kappa: float = 1.0) -> SearchResult:
     """Surrogate-guided multi-fidelity AGILE (see module doc). The chains start
@@ -335,7 +343,7 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
         n = lib.spires_ext_agile_batch_ask(h, dptr(pts), owner)
         if n > 0:
             th = pts[:n].copy()
-            lows = [ev.evaluate(th, T, np.arange(n)) for T in rungs]
+            lows = ev.evaluate_rungs(th, rungs, np.arange(n))
             evals += n * len(rungs)
             asked += n
             full = lows[-1]
