@@ -377,7 +377,8 @@ def run_sweep_workload(args):
     import spires_b200 as sp
     from spires_b200 import sweep
 
-    insts = sweep.sweep_space(args.sweep_count, seed=2024)
+    insts = sweep.sweep_space(args.sweep_count, seed=2024,
+                              t_range=(min(2000, args.sweep_tmax), args.sweep_tmax))
     t0 = time.perf_counter()
     b = sp.Batch([i.cfg for i in insts], [i.seed for i in insts])
     build_s = time.perf_counter() - t0
@@ -404,7 +405,8 @@ def run_sweep_workload(args):
             "nrmse_min": float(np.min(res["nrmse"])), "schedule": b.info(),
             "single_path_sample": {"instances": k, "value": solo_ns / (solo_ms * 1e-3)},
             "dtype": "f64", "data": "synthetic (seeded Mackey-Glass per instance)",
-            "config": {"workload": "sweep of uneven reservoirs", "count": len(insts)}}
+            "config": {"workload": "sweep of uneven reservoirs", "count": len(insts),
+                       "t_max": args.sweep_tmax}}
     print(json.dumps(line))
 
 
@@ -531,6 +533,8 @@ def main():
                     choices=["step", "sweep", "search", "classify", "ridge"],
                     help="step (default, the headline line) or an additional workload")
     ap.add_argument("--sweep-count", type=int, default=256)
+    ap.add_argument("--sweep-tmax", type=int, default=10000,
+                    help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
     args = ap.parse_args()
     if args.workload != "step":
