@@ -78,42 +78,62 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
     return *(const volatile unsigned long long *)p;
 }
 
-constexpr int kHistChunk = 16;  // ring values in flight per thread
+constexpr int kHistChunk = 32;  // ring values in flight per thread (cost model)
 
-// FLIF_GL history of neuron column `ci` for lags k = 2..lim, in ascending k
-// (the order of src/neurons/flif_gl.c:68-72): the next chunk of ring values is
-// loaded while the current one is summed, so the dependent add chain does not
-// wait for memory at every chunk.
-__device__ __forceinline__ double batch_history(double hist, const double *s_coef,
-                                                const double *ci, int rs, int L, int head,
-                                                int lim)
+constexpr int kHistC = 8;  // ring values per cp.async group and thread
+constexpr int kHistS = 4;  // groups in flight per thread
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// FLIF_GL history of column `ci` for lags 2..lim in ascending order, with the
+// ring values copied asynchronously into this thread's own shared-memory
+// slots (s_h[(stage * kHistC + j) * kBatchThreads + tid]) kHistS groups ahead,
+// so kHistS * kHistC loads are in flight while the ordered add chain runs.
+// Only the issuing thread reads its slots, so no block barrier is needed.
+__device__ __forceinline__ double batch_history_async(double hist, const double *s_coef,
+                                                      const double *ci, int rs, int L, int head,
+                                                      int lim, double *s_h, int tid)
 {
     if (lim < 2)
         return hist;
     int r = head - 2;
     if (r < 0)
         r += L;
-    double cur[kHistChunk], nxt[kHistChunk];
+    int kiss = 2;  // next lag to issue
+    auto issue = [&](int stg) {
 #pragma unroll
-    for (int j = 0; j < kHistChunk; ++j) {
-        cur[j] = (2 + j <= lim) ? __ldcg(ci + (size_t)r * rs) : 0.0;
-        r = (r == 0) ? L - 1 : r - 1;
-    }
-#pragma unroll 1
-    for (int k = 2; k <= lim; k += kHistChunk) {
-#pragma unroll
-        for (int j = 0; j < kHistChunk; ++j) {
-            nxt[j] = (k + kHistChunk + j <= lim) ? __ldcg(ci + (size_t)r * rs) : 0.0;
-            r = (r == 0) ? L - 1 : r - 1;
+        for (int j = 0; j < kHistC; ++j) {
+            if (kiss + j <= lim) {
+                cp_async8(s_h + (size_t)(stg * kHistC + j) * kBatchThreads + tid,
+                          ci + (size_t)r * rs);
+                r = (r == 0) ? L - 1 : r - 1;
+            }
         }
+        kiss += kHistC;
+        cp_async_commit();
+    };
 #pragma unroll
-        for (int j = 0; j < kHistChunk; ++j)
+    for (int q = 0; q < kHistS - 1; ++q)
+        issue(q);
+    int stg = 0;
+    for (int k = 2; k <= lim; k += kHistC) {
+        issue((stg + kHistS - 1) % kHistS);  // possibly an empty group
+        cp_async_wait<kHistS - 1>();          // the group of lags k.. has landed
+        const double *src = s_h + (size_t)stg * kHistC * kBatchThreads + tid;
+#pragma unroll
+        for (int j = 0; j < kHistC; ++j)
             if (k + j <= lim)
-                hist = add(hist, mul(s_coef[k + j], cur[j]));
-#pragma unroll
-        for (int j = 0; j < kHistChunk; ++j)
-            cur[j] = nxt[j];
+                hist = add(hist, mul(s_coef[k + j], src[(size_t)j * kBatchThreads]));
+        stg = (stg + 1 == kHistS) ? 0 : stg + 1;
     }
+    cp_async_wait<0>();
     return hist;
 }
 
@@ -266,6 +286,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
     double *s_coef = (double *)s_dyn;                    // [lmax]
     unsigned *s_spk = (unsigned *)(s_coef + p.lmax);     // [max_nw]
     int *s_list = (int *)(s_spk + p.max_nw);             // [list_cap]
+    // per-thread ring staging (FLIF_GL batches), 16-byte aligned
+    double *s_h = (double *)(((uintptr_t)(s_list + p.list_cap) + 15) & ~(uintptr_t)15);
     __shared__ int s_flag, s_abort;
     __shared__ int s_warp[kBatchThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -367,7 +389,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
                 if (act && integ) {
                     if (lim >= 1)
                         hist = add(hist, mul(s_coef[1], vlast));
-                    hist = batch_history(hist, s_coef, I.ring + i, rs, L, head, lim);
+                    hist = batch_history_async(hist, s_coef, I.ring + i, rs, L, head, lim,
+                                               s_h, tid);
                 }
             }
             if (!wait(b))
@@ -881,7 +904,8 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
     }
     b->max_nw = (int)max_nw;
     b->list_cap = list_cap;
-    b->smem = (size_t)b->lmax * 8 + max_nw * 4 + (size_t)list_cap * 4;
+    b->smem = (size_t)b->lmax * 8 + max_nw * 4 + (size_t)list_cap * 4 + 16 +
+              (b->lmax > 0 ? (size_t)kHistS * kHistC * kBatchThreads * 8 : 0);
     int rc = SP_OK;
     int per_sm = 0;
     if (b->smem > 200 * 1024)
