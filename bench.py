@@ -387,7 +387,7 @@ def run_sweep_workload(args):
     b.run(us, rasters=False, states=False)  # warm-up (plans, captures the graph)
     times = [b.run(us, rasters=False, states=False)[2] for _ in range(max(1, args.steps // 10))]
     ms = float(np.median(times))
-    res = sweep.run_sweep(insts, batch=b)
+    res = sweep.run_sweep(insts, batch=b, washout=min(500, args.sweep_tmax // 5))
     # the same instances one at a time through the single-reservoir path
     k = min(8, len(insts))
     solo_ms, solo_ns = 0.0, 0.0
