@@ -216,6 +216,22 @@ def config_dict(chunk):
 
 # ---------------------------------------------------------------- GPU arm --
 
+def max_over_ranks(x, device):
+    """Largest value of x over all ranks of the process group (every rank
+    gets it): the job's elapsed time is that of its slowest replica."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, seconds):
+    """Whole-job throughput: every replica processes units_per_rank."""
+    return world * units_per_rank / seconds
+
+
 def run_gpu_arm(args, rank, world):
     import numpy as np
     import torch
@@ -280,12 +296,8 @@ def run_gpu_arm(args, rank, world):
     per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
     if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * N_NEURONS * S * args.steps / (total_ms * 1e-3)
+        total_ms = max_over_ranks(total_ms, dev)
+    value = job_rate(N_NEURONS * S * args.steps, world, total_ms * 1e-3)
 
     # roofline of the step kernel
     g0 = fill + args.warmup * S
@@ -308,12 +320,9 @@ def run_gpu_arm(args, rank, world):
             sp.libc.free(C.cast(p, C.c_void_p))
         el = time.perf_counter() - t0
         if world > 1:
-            import torch.distributed as dist
-
-            t = torch.tensor([el], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": world * N_NEURONS * S * args.e2e_steps / el, "unit": "neuron-steps/s",
+            el = max_over_ranks(el, dev)
+        e2e = {"value": job_rate(N_NEURONS * S * args.e2e_steps, world, el),
+               "unit": "neuron-steps/s",
                "h2d_bytes_per_step": S * DIN * 8, "d2h_bytes_per_step": S * DOUT * 8,
                "api": "spires_run", "steps": args.e2e_steps}
     r.close()
