@@ -511,12 +511,39 @@ def run_ridge_workload(args):
                      "w_rel_err": float(np.linalg.norm(W - W64) / np.linalg.norm(W64)),
                      "nrmse": nr, "nrmse_rel_err": abs(nr - n64) / n64})
     best = min((x for x in rows[3:] if x["gram_mode"] == 1), key=lambda x: x["gram_ms"])
+    # spires_train_ridge end to end (reset, T steps recording states, ridge),
+    # the library on the GPU against the reference on all host cores
+    r = sp.Reservoir(cfg, seed=42)
+    t0 = time.perf_counter()
+    r.train_ridge(u, y, lam)
+    gpu_s = time.perf_counter() - t0
+    Wg = r.readout()
+    r.close()
+    cpu = None
+    try:
+        from tests import _oracle as O
+
+        threads = os.cpu_count() or 1
+        os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+        rr = sp.Reservoir(cfg, lib=O.ref_lib("openblas"), seed=42)
+        t0 = time.perf_counter()
+        rr.train_ridge(u, y, lam)
+        cpu_s = time.perf_counter() - t0
+        Wr = rr.readout()
+        rr.close()
+        cpu = {"value": cpu_s, "unit": "s", "cores": threads, "kind": "reference",
+               "sample": "reference spires_train_ridge, N=4000 T=20000 (OpenBLAS build)",
+               "w_rel_diff_vs_library": float(np.linalg.norm(Wg - Wr) / np.linalg.norm(Wr))}
+    except Exception as exc:  # the reference build is optional on a GPU host
+        cpu = {"unavailable": str(exc)[:200]}
     line = {"metric": "ridge Gram TFLOP/s (BF16X3 split, issued flops)",
             "value": best["gram_tflops"], "unit": "TFLOP/s",
             "roofline": {"bound": "tensor", "achieved": best["gram_tflops"], "peak": peak,
                          "unit": "TFLOP/s", "frac": best["gram_tflops"] / peak,
                          "peak_kind": kind},
             "modes": rows, "lambda": lam, "dtype": "bf16x3 / tf32x3 / f64",
+            "train_ridge_e2e": {"value": gpu_s, "unit": "s", "api": "spires_train_ridge"},
+            "cpu_baseline": cpu,
             "data": "synthetic (seeded Mackey-Glass)",
             "config": {"workload": "FLIF_GL N=4000 L=512 WS ridge, T=20000 washout 1000"}}
     print(json.dumps(line))
