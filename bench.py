@@ -433,7 +433,9 @@ def run_search_workload(args):
         space, task = S.Space(), S.Task(length=8000, val=1000, washout=200)
         rungs, points, chains = (500, 2000, 8000), 1024, 32
     out = {}
-    for name in ("plain", "surrogate", "no_surrogate"):
+    arms = [a for a in ("plain", "surrogate", "no_surrogate") if a in args.search_arms.split(",")]
+    assert "plain" in arms and "surrogate" in arms, "plain and surrogate arms are required"
+    for name in arms:
         ev = S.Evaluator(space, task, seed=1)
         if name == "plain":
             r = S.plain_agile(ev, chains=chains, T=rungs[-1], seed=0, max_points=points)
@@ -448,7 +450,7 @@ def run_search_workload(args):
             "value": out["surrogate"][0].time_to(target),
             "plain_wall_s": plain.wall_s, "plain_best_nrmse": plain.best_nrmse,
             "plain_time_to_best_s": plain.time_to(plain.best_loss)}
-    for name in ("surrogate", "no_surrogate"):
+    for name in [a for a in ("surrogate", "no_surrogate") if a in out]:
         r, st = out[name]
         line[name] = {"best_nrmse": r.best_nrmse, "wall_s": r.wall_s,
                       "time_to_target_s": r.time_to(target), "evals": r.evals,
@@ -572,6 +574,8 @@ def main():
     ap.add_argument("--sweep-tmax", type=int, default=10000,
                     help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
+    ap.add_argument("--search-arms", default="plain,surrogate,no_surrogate",
+                    help="comma list of plain, surrogate, no_surrogate")
     args = ap.parse_args()
     if args.workload != "step":
         {"sweep": run_sweep_workload, "search": run_search_workload,
