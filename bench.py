@@ -409,8 +409,7 @@ def run_sweep_workload(args):
         r.close()
     line = {"metric": "batched sweep neuron-steps/s", "value": ns / (ms * 1e-3),
             "unit": "neuron-steps/s", "n_gpus": 1, "ms_per_run": ms, "instances": len(insts),
-            "neuron_steps_per_run": ns, "build_s": build_s, "ridge_all_s": res["train_s"],
-            "predict_all_s": res["predict_s"], "nrmse_median": float(np.median(res["nrmse"])),
+            "neuron_steps_per_run": ns, "build_s": build_s, "fit_score_all_s": res["fit_score_s"], "nrmse_median": float(np.median(res["nrmse"])),
             "nrmse_min": float(np.min(res["nrmse"])), "schedule": b.info(),
             "single_path_sample": {"instances": k, "value": solo_ns / (solo_ms * 1e-3)},
             "dtype": "f64", "data": "synthetic (seeded Mackey-Glass per instance)",

@@ -262,15 +262,13 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
 
     Cut r (after rung r) ranks by its own network, an MLP 10 -> 128 -> 128 -> 2
     mapping the 9 hyper-parameter features plus the rung-r loss to the mean
-    and log-variance of the full-fidelity loss. The first wave also carries a
-    seeded random calibration set through every rung, so that the first
-    training tuples are not only the best points: the chains' start points
-    all go through every rung (their full-fidelity losses are what the
-    chains are told for them), and each wave carries `calibration` further
-    random points through every rung.
+    and log-variance of the full-fidelity loss. So that the training tuples
+    are not only the best points, the chains' start points all go through
+    every rung (their full-fidelity losses are what the chains are told for
+    them; the networks train on them before the first wave), and every wave
+    carries `calibration` further seeded random points through every rung.
     Cuts rank by the optimistic score mean - kappa * std, so that points the
-    network is unsure about still get simulated. The first wave is half as
-    long as the others, so the network starts guiding the chains early."""
+    network is unsure about still get simulated."""
     lib, h = _agile_start(chains, seed, opts)
     ncut = len(rungs) - 1
     nets = [Surrogate(seed=seed + r) for r in range(ncut)] if use_surrogate else None
@@ -299,7 +297,7 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
             m = m - kappa * np.exp(0.5 * np.clip(v.astype(np.float64), -20.0, 20.0))
         return m
 
-    def cut_wave(th, l0, pid, first):
+    def cut_wave(th, l0, pid):
         # pid: asked index of every point, the seed of its reservoir at every rung
         nonlocal best, best_th, evals, trained
         n = len(th)
@@ -337,7 +335,6 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
                           batch=min(256, len(ya)), lr=1e-3, seed=seed + 31 * len(hist) + r)
         trained = True
 
-    first = True
     try:
         # the chains' start points: every rung, told their full-fidelity loss
         n = lib.spires_ext_agile_batch_ask(h, dptr(pts), owner)
@@ -374,12 +371,10 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
             pool_id.append(np.arange(asked - n, asked))
             if sum(len(p) for p in pool_th) >= wave_size:
                 cut_wave(np.concatenate(pool_th), np.concatenate(pool_l0),
-                         np.concatenate(pool_id), first)
-                first = False
+                         np.concatenate(pool_id))
                 pool_th, pool_l0, pool_id = [], [], []
         if pool_th:
-            cut_wave(np.concatenate(pool_th), np.concatenate(pool_l0), np.concatenate(pool_id),
-                     first)
+            cut_wave(np.concatenate(pool_th), np.concatenate(pool_l0), np.concatenate(pool_id))
     finally:
         lib.spires_ext_agile_batch_destroy(h)
         if nets is not None:
