@@ -477,6 +477,54 @@ def run_classify_workload(args):
     print(json.dumps(out))
 
 
+def run_small_lif_workload(args):
+    """LIF_DISCRETE N=1000 [V_0=0, V_th=1, leak=0.9, bias=0], Erdos-Renyi 0.1
+    with N(0,1) weights on the present edges rescaled to spectral radius 0.9
+    (injected with spires_ext_set_weights), W_in U[-1, 1], gain 0.5,
+    Mackey-Glass T=5000, washout 500, ridge lambda 1e-6 (FP64)."""
+    import numpy as np
+
+    import spires_b200 as sp
+    from spires_b200.datasets import mackey_glass
+
+    n, T, w, lam = 1000, 5000, 500, 1e-6
+    cfg = sp.make_config(n, 1, 1, rho=0.9, ei=0.5, gamma=0.5, conn=0.1, dt=1.0,
+                         topo=sp.CONN_RANDOM, neuron=sp.LIF_DISCRETE,
+                         nparams=(0.0, 1.0, 0.9, 0.0))
+    rng = np.random.default_rng(SEED)
+    mask = rng.random((n, n)) < 0.1
+    np.fill_diagonal(mask, False)
+    D = np.where(mask, rng.standard_normal((n, n)), 0.0)
+    x = mackey_glass(T + 1, seed=0)
+    u, y = np.ascontiguousarray(x[:-1, None]), np.ascontiguousarray(x[1:, None])
+    r = sp.Reservoir(cfg, seed=SEED)
+    r.set_weights(D, rescale=True)
+    r.run_record(u[:500], phi=False, raster=False)  # warm-up
+    r.reset()
+    t0 = time.perf_counter()
+    _, R, _ = r.run_record(u, phi=False, raster=True)
+    step_s = time.perf_counter() - t0
+    o = sp.RidgeOpts(0, 30, 1e-13, w)
+    rep = sp.RidgeReport()
+    t0 = time.perf_counter()
+    assert r.lib.spires_ext_train_ridge(r.h, sp.dptr(u), sp.dptr(y), T, lam, C.byref(o),
+                                        C.byref(rep)) == sp.SPIRES_OK
+    ridge_s = time.perf_counter() - t0
+    r.reset()
+    yhat = r.run(u)
+    r.close()
+    e = yhat[w:, 0] - y[w:, 0]
+    nr = float(np.sqrt(np.mean(e * e)) / y[w:, 0].std())
+    spikes = int(np.unpackbits(R.view(np.uint8)).sum())
+    line = {"metric": "reservoir neuron-steps/s", "value": n * T / step_s,
+            "unit": "neuron-steps/s", "note": "latency bound at N=1000 (one launch, T steps)",
+            "train_ridge_s": ridge_s, "nrmse": nr, "spikes": spikes,
+            "ridge": {"dual": rep.dual, "rel_residual": rep.rel_residual},
+            "dtype": "f64", "data": "synthetic (seeded Mackey-Glass, N(0,1) weights)",
+            "config": {"workload": "LIF_DISCRETE N=1000 ER 0.1 N(0,1) rho 0.9, T=5000"}}
+    print(json.dumps(line))
+
+
 def run_ridge_workload(args):
     """FLIF_GL N=4000 L=512 Watts-Strogatz k=10, Mackey-Glass T=20000,
     washout 1000: the ridge readout with the FP64 Gram and with the split
@@ -567,7 +615,7 @@ def main():
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
     ap.add_argument("--workload", default="step",
-                    choices=["step", "sweep", "search", "classify", "ridge"],
+                    choices=["step", "sweep", "search", "classify", "ridge", "small"],
                     help="step (default, the headline line) or an additional workload")
     ap.add_argument("--sweep-count", type=int, default=256)
     ap.add_argument("--sweep-tmax", type=int, default=10000,
@@ -578,7 +626,8 @@ def main():
     args = ap.parse_args()
     if args.workload != "step":
         {"sweep": run_sweep_workload, "search": run_search_workload,
-         "classify": run_classify_workload, "ridge": run_ridge_workload}[args.workload](args)
+         "classify": run_classify_workload, "ridge": run_ridge_workload,
+         "small": run_small_lif_workload}[args.workload](args)
         return
 
     rank = int(os.environ.get("RANK", "0"))

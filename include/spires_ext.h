@@ -94,6 +94,16 @@ spires_status spires_ext_autotune(spires_reservoir *r, size_t steps);
  * stream derived from seed and i). Takes effect at the next reset. */
 spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed);
 
+/* ---- recurrent weights from a dense matrix ----------------------------------
+ * Replaces W by dense[N x N] (row-major, zero = no edge) the way the
+ * reference's synapse_build_from_dense builds a synapse matrix (per-edge
+ * synapse quantities drawn again from rand() where the model has them);
+ * with rescale = 1 the weights are scaled to the configured spectral radius by
+ * the construction's power iteration. The reservoir returns to its reset
+ * state; W_in and W_out are kept. For workloads whose weights are not the
+ * generator's (for example N(0,1) weights on an Erdos-Renyi pattern). */
+spires_status spires_ext_set_weights(spires_reservoir *r, const double *dense, int rescale);
+
 /* ---- spectral radius ------------------------------------------------------
  * The max-abs normalised power iteration that scales the recurrent weights at
  * create time (reference src/sparse.c:93-127) on an n x n CSR matrix with

@@ -167,6 +167,7 @@ EXT_SIGNATURES = {
                                             C.POINTER(AgileOpts), _dp, C.POINTER(AgileReport)]),
     "spires_ext_ridge_solve_noalloc": (C.c_int, [_VP, _VP, C.c_size_t, C.c_size_t, C.c_size_t,
                                                  C.c_size_t, C.c_double, _VP, _VP]),
+    "spires_ext_set_weights": (C.c_int, [_VP, _dp, C.c_int]),
     "spires_ext_spectral_radius": (C.c_int, [C.c_size_t, _i64p, _i32p, _dp, C.c_int, _dp]),
     "spires_ext_agile_batch_create": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp,
                                                 C.POINTER(AgileOpts), C.POINTER(C.c_uint64),
@@ -358,6 +359,13 @@ class Reservoir:
             None if R is None else R.ctypes.data_as(_u32p), None if Y is None else dptr(Y))
         assert st == SPIRES_OK, st
         return P, R, Y
+
+    def set_weights(self, dense, rescale=True):
+        """spires_ext_set_weights: dense [n, n] recurrent weights (0 = no edge)."""
+        d = np.ascontiguousarray(dense, np.float64)
+        assert d.shape == (self.n, self.n)
+        st = self.lib.spires_ext_set_weights(self.h, dptr(d), int(rescale))
+        assert st == SPIRES_OK, st
 
     def w_in(self):
         w = np.empty(self.n * self.din)

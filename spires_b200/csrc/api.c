@@ -883,3 +883,48 @@ SPIRES_EXPORT spires_status spires_ext_batch_timing(const spires_ext_batch *b, d
         *setup_ms = b->setup_ms;
     return SPIRES_OK;
 }
+
+/* Replace the recurrent weights by a dense matrix (zeros are no edge), as the
+ * reference's synapse_build_from_dense builds them (per-edge synapse draws
+ * included), optionally rescaled to the configured spectral radius with the
+ * construction's power iteration; the reservoir returns to its reset state. */
+SPIRES_EXPORT spires_status spires_ext_set_weights(spires_reservoir *r, const double *dense,
+                                                   int rescale)
+{
+    if (!r || !r->dev || !dense)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_host_model *m = &r->m;
+    void *old[] = {m->row_ptr, m->col, m->w, m->edge_decay, m->edge_omd, m->edge_tau,
+                   m->syn_coef, m->mexp_decay, m->mexp_omd, m->mexp_c, m->mexp_tau};
+    m->row_ptr = NULL;
+    m->col = NULL;
+    m->w = NULL;
+    m->edge_decay = m->edge_omd = m->edge_tau = m->syn_coef = NULL;
+    m->mexp_decay = m->mexp_omd = m->mexp_c = m->mexp_tau = NULL;
+    for (size_t k = 0; k < sizeof(old) / sizeof(old[0]); ++k)
+        free(old[k]);
+    int rc = sp_model_set_dense_weights(m, dense);
+    if (!rc && rescale) {
+        double sr = 0.0;
+        if (m->nnz < ((size_t)1 << 15) ||
+            sp_dev_spectral_radius(m->n, m->row_ptr, m->col, m->w, &sr) != SP_OK)
+            sr = sp_csr_spectral_radius(m->n, m->row_ptr, m->col, m->w);
+        m->spectral_radius_before = sr;
+        if (sr > 1e-9) {
+            const double f = m->spectral_radius / sr;
+            for (size_t k = 0; k < m->nnz; k++)
+                m->w[k] = f * m->w[k];
+        }
+    }
+    if (!rc)
+        rc = sp_model_derive_neuron(m);
+    if (rc)
+        return to_status(rc);
+    sp_dev *nd = NULL;
+    rc = sp_dev_create(m, &nd);
+    if (rc)
+        return to_status(rc);
+    sp_dev_destroy(r->dev);
+    r->dev = nd;
+    return SPIRES_OK;
+}
