@@ -556,8 +556,13 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                     const bool landed = mbar_wait(&full[cst], (unsigned)cph, &s_abort, p.err);
                     const double *buf = s_stage + (size_t)cst * STAGE + boff;
                     if (landed && act && integ) {
-                        if (cnt == 16) {
-                            hist = stage_sum<16>(hist, cf + k, buf, p.BW);
+                        if ((cnt & 15) == 0) {
+                            // full stages of 16, 32 or 64 rows: 16 lags at a time
+                            // with their loads batched, still in ascending lag
+                            // order (lag k + jr sits at row offset cnt-1-jr)
+                            for (int h = 0; h < cnt; h += 16)
+                                hist = stage_sum<16>(hist, cf + k + h,
+                                                     buf + (size_t)(cnt - 16 - h) * p.BW, p.BW);
                         } else if (cnt == 8) {
                             hist = stage_sum<8>(hist, cf + k, buf, p.BW);
                         } else {
