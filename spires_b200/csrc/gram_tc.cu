@@ -106,7 +106,7 @@ extern "C" int sp_gram_bf16x3_available(void) { return handle_for_current_device
 extern "C" int sp_gram_split(cudaStream_t s, int mode, const double *X, int n, size_t t0,
                              size_t t1, double *C, int ldc)
 {
-    if (mode != 1 && mode != 2 || t1 - t0 > (size_t)65535 * 32)
+    if ((mode != 1 && mode != 2) || t1 < t0 || t1 - t0 > (size_t)65535 * 32)
         return SP_EINVAL;
     cublasHandle_t h = handle_for_current_device();
     if (!h)
