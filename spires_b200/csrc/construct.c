@@ -192,18 +192,62 @@ static int csr_from_trips(sp_host_model *m, tripbuf *b, int sorted)
 
 /* ------------------------------------------------------------ topologies -- */
 
-/* Erdos-Renyi directed, no self loops; src/reservoir.c:386-397 */
-static int topo_random(sp_host_model *m, tripbuf *b)
+/* Erdos-Renyi directed, no self loops; src/reservoir.c:386-397. Rows come
+ * out in order and columns ascending, so the CSR is written directly (zero
+ * weights dropped, as csr_build_from_dense does), with the draws in the
+ * reference's order: the edge test, then the weight's two draws. */
+static int topo_random(sp_host_model *m)
 {
-    size_t n = m->n;
-    for (size_t i = 0; i < n; i++)
+    const size_t n = m->n;
+    size_t cap = (size_t)((double)n * (double)n * m->connectivity * 1.05) + 1024;
+    m->row_ptr = calloc(n + 1, sizeof(int64_t));
+    m->col = malloc(cap * sizeof(int32_t));
+    m->w = malloc(cap * sizeof(double));
+    if (!m->row_ptr || !m->col || !m->w)
+        return SP_EALLOC;
+    /* urand01() < c  <=>  draw < K for the smallest K with K / RAND_MAX >= c
+     * (the correctly rounded division is monotone in the numerator), so the
+     * edge test needs no division per pair */
+    long long lo = 0, hi = (long long)RAND_MAX + 1;
+    while (lo < hi) {
+        const long long mid = lo + (hi - lo) / 2;
+        if ((double)mid / (double)RAND_MAX < m->connectivity)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    const long long K = lo;
+    sp_rand_state *g = tl_rng;
+    size_t e = 0;
+    for (size_t i = 0; i < n; i++) {
+        m->row_ptr[i] = (int64_t)e;
         for (size_t j = 0; j < n; j++) {
             if (i == j)
                 continue;
-            if (urand01() < m->connectivity)
-                if (tb_push(b, (int32_t)i, (int32_t)j, draw_weight(m->ei_ratio)))
-                    return SP_EALLOC;
+            if ((long long)(g ? sp_rand_next(g) : rand()) < K) {
+                const double v = draw_weight(m->ei_ratio);
+                if (v == 0.0)
+                    continue;
+                if (e == cap) {
+                    const size_t nc = cap + cap / 2 + 1024;
+                    int32_t *nc_col = realloc(m->col, nc * sizeof(int32_t));
+                    if (!nc_col)
+                        return SP_EALLOC;
+                    m->col = nc_col;
+                    double *nc_w = realloc(m->w, nc * sizeof(double));
+                    if (!nc_w)
+                        return SP_EALLOC;
+                    m->w = nc_w;
+                    cap = nc;
+                }
+                m->col[e] = (int32_t)j;
+                m->w[e] = v;
+                e++;
+            }
         }
+    }
+    m->row_ptr[n] = (int64_t)e;
+    m->nnz = e;
     return SP_OK;
 }
 
@@ -879,9 +923,7 @@ int sp_model_build(sp_host_model *m)
     tripbuf b = {0};
     switch (m->conn_type) {
     case SP_CONN_RANDOM:
-        rc = topo_random(m, &b);
-        if (!rc)
-            rc = csr_from_trips(m, &b, 1);
+        rc = topo_random(m);
         break;
     case SP_CONN_SMALL_WORLD:
         rc = topo_small_world(m, &b);
