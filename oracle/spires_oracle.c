@@ -129,13 +129,10 @@ static void neurons_init(orc_state *s, int first)
             s->spike[i] = 0.0;
             s->nstep[i] = 0;
             s->refr_until[i] = -1;
+            /* SplitMix64 state after one discarded draw: the draw only
+             * advances the state by the golden-ratio increment */
             uint64_t z = s->m.diffusive_seed ^ (0xD1B54A32D192ED03ULL * (uint64_t)(i + 1));
-            z += 0x9E3779B97F4A7C15ULL;
-            s->rng[i] = z; /* first splitmix draw consumed below */
-            uint64_t t = s->rng[i];
-            t = (t ^ (t >> 30)) * 0xBF58476D1CE4E5B9ULL;
-            t = (t ^ (t >> 27)) * 0x94D049BB133111EBULL;
-            (void)t;
+            s->rng[i] = z + 0x9E3779B97F4A7C15ULL;
         }
         break;
     }
