@@ -82,6 +82,30 @@ static double draw_weight(double ei_ratio)
     return -magnitude;
 }
 
+/* The smallest K with (double)K / RAND_MAX >= c. The correctly rounded
+ * division is monotone in the numerator, so urand01() < c holds exactly when
+ * the draw is below K: a comparison of draws needs no division. */
+static long long draw_threshold(double c)
+{
+    long long lo = 0, hi = (long long)RAND_MAX + 1;
+    while (lo < hi) {
+        const long long mid = lo + (hi - lo) / 2;
+        if ((double)mid / (double)RAND_MAX < c)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+/* draw_weight(ei_ratio) with the sign test as a draw comparison against
+ * K_ei = draw_threshold(ei_ratio): the same two draws, the same value */
+static double draw_weight_k(long long K_ei)
+{
+    const double magnitude = (double)draw_int() / RAND_MAX;
+    return (long long)draw_int() < K_ei ? magnitude : -magnitude;
+}
+
 /* ------------------------------------------------------- triplet buffer -- */
 
 typedef struct {
@@ -205,18 +229,9 @@ static int topo_random(sp_host_model *m)
     m->w = malloc(cap * sizeof(double));
     if (!m->row_ptr || !m->col || !m->w)
         return SP_EALLOC;
-    /* urand01() < c  <=>  draw < K for the smallest K with K / RAND_MAX >= c
-     * (the correctly rounded division is monotone in the numerator), so the
-     * edge test needs no division per pair */
-    long long lo = 0, hi = (long long)RAND_MAX + 1;
-    while (lo < hi) {
-        const long long mid = lo + (hi - lo) / 2;
-        if ((double)mid / (double)RAND_MAX < m->connectivity)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    const long long K = lo;
+    /* the edge test and the weight's sign test as draw comparisons */
+    const long long K = draw_threshold(m->connectivity);
+    const long long K_ei = draw_threshold(m->ei_ratio);
     sp_rand_state *g = tl_rng;
     size_t e = 0;
     for (size_t i = 0; i < n; i++) {
@@ -225,7 +240,7 @@ static int topo_random(sp_host_model *m)
             if (i == j)
                 continue;
             if ((long long)(g ? sp_rand_next(g) : rand()) < K) {
-                const double v = draw_weight(m->ei_ratio);
+                const double v = draw_weight_k(K_ei);
                 if (v == 0.0)
                     continue;
                 if (e == cap) {
@@ -337,10 +352,11 @@ static int topo_small_world(sp_host_model *m, tripbuf *b)
     return SP_OK;
 }
 
-/* Fenwick tree over int64 weights (deg[u] + 1 per node). */
+/* Fenwick tree over int64 weights (deg[u] + 1 per node), sized to a power of
+ * two so that the descent takes a fixed number of levels with no bounds test. */
 typedef struct {
-    int64_t *t;
-    size_t n;
+    int64_t *t; /* t[1..n] */
+    size_t n;   /* a power of two */
 } fenwick;
 
 static void fw_add(fenwick *f, size_t i, int64_t v)
@@ -349,21 +365,19 @@ static void fw_add(fenwick *f, size_t i, int64_t v)
         f->t[k] += v;
 }
 
-/* smallest index u (0-based) with prefix(u) >= target, target >= 1;
- * returns n if the total is below target */
+/* The smallest 0-based u with prefix(u) >= target, for 1 <= target <= total.
+ * The path through the tree is random, so each level selects with a mask
+ * instead of a branch. */
 static size_t fw_lower_bound(const fenwick *f, int64_t target)
 {
     size_t pos = 0;
-    size_t step = 1;
-    while (step * 2 <= f->n)
-        step *= 2;
-    for (; step; step >>= 1) {
-        if (pos + step <= f->n && f->t[pos + step] < target) {
-            pos += step;
-            target -= f->t[pos];
-        }
+    for (size_t step = f->n >> 1; step; step >>= 1) {
+        const int64_t t = f->t[pos + step];
+        const int64_t mask = -(int64_t)(t < target);
+        pos += step & (size_t)mask;
+        target -= t & mask;
     }
-    return pos; /* 0-based index of the element reaching target */
+    return pos;
 }
 
 static int cmp_i32(const void *a, const void *b)
@@ -373,12 +387,14 @@ static int cmp_i32(const void *a, const void *b)
 }
 
 /* Barabasi-Albert with initial attractiveness A = 1 and random orientation;
- * src/reservoir.c:445-536 */
-static int topo_scale_free(sp_host_model *m, tripbuf *b)
+ * src/reservoir.c:445-536. The CSR is written directly. */
+static int topo_scale_free(sp_host_model *m)
 {
     size_t n = m->n;
-    if (n < 2)
-        return SP_OK;
+    if (n < 2) {
+        tripbuf none = {0};
+        return csr_from_trips(m, &none, 1);
+    }
     int mm = (int)((m->connectivity) * (double)(n - 1) + 0.5);
     if (mm < 1)
         mm = 1;
@@ -389,15 +405,20 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
         m0 = (int)n - 1;
 
     int rc = SP_EALLOC;
+    size_t tree_n = 1;
+    while (tree_n < n)
+        tree_n <<= 1;
     int64_t *deg = calloc(n, sizeof(int64_t));
-    fenwick fw = {calloc(n + 1, sizeof(int64_t)), n};
+    fenwick fw = {calloc(tree_n + 1, sizeof(int64_t)), tree_n};
     size_t max_edges = (size_t)m0 * (size_t)(m0 - 1) / 2 + (n - (size_t)m0) * (size_t)mm;
     int32_t *eu = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
     int32_t *ev = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
     int32_t *picks = malloc((size_t)mm * sizeof(int32_t));
     int64_t *stamp = malloc(n * sizeof(int64_t)); /* stamp[u] = last v that picked u */
-    int64_t *adj_off = NULL;
+    int64_t *adj_off = NULL, *fill = NULL;
     int32_t *adj = NULL;
+    unsigned char *fwd = NULL;
+    double *wv = NULL;
     size_t ne = 0;
     if (!deg || !fw.t || !eu || !ev || !picks || !stamp)
         goto done;
@@ -413,12 +434,15 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
             deg[u]++;
             deg[v]++;
         }
-    for (size_t u = 0; u < n; u++)
-        fw_add(&fw, u, (u < (size_t)m0) ? deg[u] + 1 : 0);
+    for (size_t u = 0; u < (size_t)m0; u++)
+        fw_add(&fw, u, deg[u] + 1);
     int64_t degsum = 0;
     for (int u = 0; u < m0; u++)
         degsum += deg[u];
 
+    /* The tree holds deg[u] + 1 for every u < v, and so sums to degsum + v,
+     * the roulette total. The draw r = urand01() * total never exceeds that
+     * integer total, so ceil(r) is a valid target of the descent. */
     for (size_t v = (size_t)m0; v < n; v++) {
         int added = 0, guard = 0;
         while (added < mm && guard < 50 * mm) {
@@ -430,11 +454,9 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
             /* first u with r <= acc(u); acc(u) integral, so acc >= ceil(r) */
             double cr = ceil(r);
             size_t pick = 0;
-            if (cr <= 0.0) {
-                pick = 0;
-            } else {
+            if (cr > 0.0) {
                 size_t u = fw_lower_bound(&fw, (int64_t)cr);
-                pick = (u < v) ? u : 0; /* no u satisfies: pick stays 0 */
+                pick = (u < v) ? u : 0;
             }
             const int dup = stamp[pick] == (int64_t)v; /* already picked for v */
             if (pick != v && !dup) {
@@ -478,7 +500,8 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
      * adjacency would give for the j > i part the orientation pass reads. */
     adj_off = calloc(n + 1, sizeof(int64_t));
     adj = malloc((ne > 0 ? ne : 1) * sizeof(int32_t));
-    if (!adj_off || !adj)
+    fill = malloc(n * sizeof(int64_t));
+    if (!adj_off || !adj || !fill)
         goto done;
     for (size_t e = 0; e < ne; e++) {
         const int32_t lo = eu[e] < ev[e] ? eu[e] : ev[e];
@@ -486,17 +509,11 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
     }
     for (size_t u = 0; u < n; u++)
         adj_off[u + 1] += adj_off[u];
-    {
-        int64_t *fill = malloc(n * sizeof(int64_t));
-        if (!fill)
-            goto done;
-        memcpy(fill, adj_off, n * sizeof(int64_t));
-        for (size_t e = 0; e < ne; e++) {
-            const int32_t lo = eu[e] < ev[e] ? eu[e] : ev[e];
-            const int32_t hi = eu[e] < ev[e] ? ev[e] : eu[e];
-            adj[fill[lo]++] = hi;
-        }
-        free(fill);
+    memcpy(fill, adj_off, n * sizeof(int64_t));
+    for (size_t e = 0; e < ne; e++) {
+        const int32_t lo = eu[e] < ev[e] ? eu[e] : ev[e];
+        const int32_t hi = eu[e] < ev[e] ? ev[e] : eu[e];
+        adj[fill[lo]++] = hi;
     }
     for (size_t u = 0; u < n; u++) /* guard: keep the ascending order exact */
         for (int64_t k = adj_off[u] + 1; k < adj_off[u + 1]; k++)
@@ -505,21 +522,57 @@ static int topo_scale_free(sp_host_model *m, tripbuf *b)
                       cmp_i32);
                 break;
             }
+    free(eu);
+    free(ev);
+    eu = ev = NULL;
 
-    /* orientation pass in row-major order over i < j */
+    /* Orientation in row-major order over i < j (the bucket order): per edge
+     * the orientation draw (urand01() < 0.5 keeps i -> j), then the weight's
+     * two draws. Orientations and weights are kept per edge and the rows
+     * counted; zero weights are dropped as csr_build_from_dense drops them. */
+    fwd = malloc(ne > 0 ? ne : 1);
+    wv = malloc((ne > 0 ? ne : 1) * sizeof(double));
+    m->row_ptr = calloc(n + 1, sizeof(int64_t));
+    if (!fwd || !wv || !m->row_ptr)
+        goto done;
+    {
+        const long long K_half = draw_threshold(0.5);
+        const long long K_ei = draw_threshold(m->ei_ratio);
+        for (size_t i = 0; i < n; i++)
+            for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++) {
+                const int f = (long long)draw_int() < K_half;
+                const double w = draw_weight_k(K_ei);
+                fwd[k] = (unsigned char)f;
+                wv[k] = w;
+                if (w != 0.0)
+                    m->row_ptr[(f ? i : (size_t)adj[k]) + 1]++;
+            }
+    }
     for (size_t i = 0; i < n; i++)
-        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++) {
-            size_t j = (size_t)adj[k];
-            if (j <= i)
-                continue;
-            int fail;
-            if (urand01() < 0.5)
-                fail = tb_push(b, (int32_t)i, (int32_t)j, draw_weight(m->ei_ratio));
-            else
-                fail = tb_push(b, (int32_t)j, (int32_t)i, draw_weight(m->ei_ratio));
-            if (fail)
-                goto done;
-        }
+        m->row_ptr[i + 1] += m->row_ptr[i];
+    m->nnz = (size_t)m->row_ptr[n];
+    m->col = malloc((m->nnz ? m->nnz : 1) * sizeof(int32_t));
+    m->w = malloc((m->nnz ? m->nnz : 1) * sizeof(double));
+    if (!m->col || !m->w)
+        goto done;
+    memcpy(fill, m->row_ptr, n * sizeof(int64_t));
+    /* Row r holds its columns below r (edges (i, r) oriented r -> i; the outer
+     * loop visits i ascending) and then those above r (its own bucket,
+     * ascending): ascending columns with no sort. */
+    for (size_t i = 0; i < n; i++)
+        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++)
+            if (!fwd[k] && wv[k] != 0.0) {
+                const int64_t at = fill[adj[k]]++;
+                m->col[at] = (int32_t)i;
+                m->w[at] = wv[k];
+            }
+    for (size_t i = 0; i < n; i++)
+        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++)
+            if (fwd[k] && wv[k] != 0.0) {
+                const int64_t at = fill[i]++;
+                m->col[at] = adj[k];
+                m->w[at] = wv[k];
+            }
     rc = SP_OK;
 done:
     free(deg);
@@ -530,6 +583,9 @@ done:
     free(stamp);
     free(adj_off);
     free(adj);
+    free(fill);
+    free(fwd);
+    free(wv);
     return rc;
 }
 
@@ -931,9 +987,7 @@ int sp_model_build(sp_host_model *m)
             rc = csr_from_trips(m, &b, 1);
         break;
     case SP_CONN_SCALE_FREE:
-        rc = topo_scale_free(m, &b);
-        if (!rc)
-            rc = csr_from_trips(m, &b, 0);
+        rc = topo_scale_free(m);
         break;
     default:
         rc = SP_EINVAL;

@@ -22,6 +22,8 @@ CASES = [
     (250, sp.CONN_SCALE_FREE, 5 / 249, 13, 10, sp.FLIF_GL, GL, sp.SYN_SIMPLE, 0, None),
     (150, sp.CONN_SCALE_FREE, 0.1, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 1, None),
     (2, sp.CONN_SCALE_FREE, 0.5, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 0, None),
+    (1000, sp.CONN_SCALE_FREE, 0.1, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 0, None),
+    (600, sp.CONN_RANDOM, 0.3, 1, 1, sp.LIF_DISCRETE, (0, 1, 0.9, 0), sp.SYN_SIMPLE, 0, None),
     (120, sp.CONN_RANDOM, 0.1, 1, 1, sp.FLIF_GL, GL, sp.SYN_PSC_HET, 0, (1.0, 20.0)),
     (80, sp.CONN_SMALL_WORLD, 0.1, 1, 1, sp.FLIF_GL, GL, sp.SYN_PSC_HET, 1, (2.0, 8.0)),
     (100, sp.CONN_SCALE_FREE, 0.03, 1, 1, sp.FLIF_GL, GL, sp.SYN_FRAC_MEXP, 0,
