@@ -13,7 +13,7 @@
  *
  * The reference materialises a dense n x n scratch (3.2 GB at n = 20000) and an
  * n x n byte adjacency for scale-free graphs; here rows are produced directly
- * in CSR order and the Barabasi-Albert roulette runs on a Fenwick tree. Both
+ * in CSR order and the Barabasi-Albert roulette runs on a prefix-sum tree. Both
  * choices give the same picks: the roulette totals are sums of small integers,
  * which double arithmetic holds exactly, so "first u with r <= prefix(u)" is
  * the same integer search either way.
@@ -352,28 +352,104 @@ static int topo_small_world(sp_host_model *m, tripbuf *b)
     return SP_OK;
 }
 
-/* Fenwick tree over int64 weights (deg[u] + 1 per node), sized to a power of
- * two so that the descent takes a fixed number of levels with no bounds test. */
-typedef struct {
-    int64_t *t; /* t[1..n] */
-    size_t n;   /* a power of two */
-} fenwick;
+/* The Barabasi-Albert roulette: weights deg[u] + 1 per node, a point update
+ * per pick and the search for the first node whose prefix sum reaches a
+ * target. The path of that search is random, so it is the latency of its
+ * dependent loads that sets the pace.
+ *
+ * Main form: a 16-ary tree of int32 inclusive prefix sums, one 64-byte node
+ * per 16 children (35 KB at 8000 nodes, cache-resident): a level costs one
+ * node load and 16 comparisons in 4-lane vectors, against one load per level
+ * of a binary tree. Graphs whose totals could pass INT32_MAX use a Fenwick
+ * tree over int64 instead. Both return the same node for the same target. */
+typedef int32_t sp_v4i __attribute__((vector_size(16)));
 
-static void fw_add(fenwick *f, size_t i, int64_t v)
+typedef struct {
+    int32_t *e;        /* 16 entries per node, levels stored leaf-parents first */
+    size_t off[16];    /* first entry of each level */
+    int levels;        /* 16^levels >= n; the last level is the root node */
+    int64_t *t;        /* Fenwick form: t[1..tn], tn a power of two */
+    size_t tn;
+} roulette;
+
+static int rl_init(roulette *r, size_t n, int64_t max_total)
 {
-    for (size_t k = i + 1; k <= f->n; k += k & (~k + 1))
-        f->t[k] += v;
+    memset(r, 0, sizeof(*r));
+    if (max_total <= INT32_MAX) {
+        size_t total = 0, span = 16;
+        int l = 0;
+        do {
+            r->off[l] = total;
+            total += (n + span - 1) / span * 16;
+            l++;
+            if (span >= n)
+                break;
+            span <<= 4;
+        } while (l < 16);
+        r->levels = l;
+        if (posix_memalign((void **)&r->e, 64, total * sizeof(int32_t)))
+            return SP_EALLOC;
+        memset(r->e, 0, total * sizeof(int32_t));
+        return SP_OK;
+    }
+    r->tn = 1;
+    while (r->tn < n)
+        r->tn <<= 1;
+    r->t = calloc(r->tn + 1, sizeof(int64_t));
+    return r->t ? SP_OK : SP_EALLOC;
 }
 
-/* The smallest 0-based u with prefix(u) >= target, for 1 <= target <= total.
- * The path through the tree is random, so each level selects with a mask
- * instead of a branch. */
-static size_t fw_lower_bound(const fenwick *f, int64_t target)
+static void rl_free(roulette *r)
 {
+    free(r->e);
+    free(r->t);
+}
+
+static void rl_add(roulette *r, size_t u, int64_t d)
+{
+    if (r->e) {
+        const sp_v4i i0 = {0, 1, 2, 3}, i1 = {4, 5, 6, 7}, i2 = {8, 9, 10, 11},
+                     i3 = {12, 13, 14, 15};
+        const int32_t d32 = (int32_t)d;
+        const sp_v4i dd = {d32, d32, d32, d32};
+        for (int l = 0; l < r->levels; l++) {
+            sp_v4i *x = (sp_v4i *)(r->e + r->off[l] + (u >> (4 * (l + 1))) * 16);
+            const int32_t slot = (int32_t)((u >> (4 * l)) & 15);
+            const sp_v4i sl = {slot, slot, slot, slot};
+            x[0] += (i0 >= sl) & dd; /* the entries from the slot on hold u */
+            x[1] += (i1 >= sl) & dd;
+            x[2] += (i2 >= sl) & dd;
+            x[3] += (i3 >= sl) & dd;
+        }
+        return;
+    }
+    for (size_t k = u + 1; k <= r->tn; k += k & (~k + 1))
+        r->t[k] += d;
+}
+
+/* The smallest 0-based u with prefix(u) >= target, for 1 <= target <= total. */
+static size_t rl_pick(const roulette *r, int64_t target)
+{
+    if (r->e) {
+        int32_t tg = (int32_t)target;
+        size_t node = 0;
+        for (int l = r->levels - 1; l >= 0; l--) {
+            const int32_t *p = r->e + r->off[l] + node * 16;
+            const sp_v4i *x = (const sp_v4i *)p;
+            const sp_v4i t = {tg, tg, tg, tg};
+            /* entries are nondecreasing: the count below the target is the
+             * child holding it */
+            const sp_v4i below = (x[0] < t) + (x[1] < t) + (x[2] < t) + (x[3] < t);
+            const int32_t c = -(below[0] + below[1] + below[2] + below[3]);
+            tg -= c ? p[c - 1] : 0;
+            node = node * 16 + (size_t)c;
+        }
+        return node;
+    }
     size_t pos = 0;
-    for (size_t step = f->n >> 1; step; step >>= 1) {
-        const int64_t t = f->t[pos + step];
-        const int64_t mask = -(int64_t)(t < target);
+    for (size_t step = r->tn >> 1; step; step >>= 1) {
+        const int64_t t = r->t[pos + step];
+        const int64_t mask = -(int64_t)(t < target); /* a mask, not a branch */
         pos += step & (size_t)mask;
         target -= t & mask;
     }
@@ -405,12 +481,11 @@ static int topo_scale_free(sp_host_model *m)
         m0 = (int)n - 1;
 
     int rc = SP_EALLOC;
-    size_t tree_n = 1;
-    while (tree_n < n)
-        tree_n <<= 1;
     int64_t *deg = calloc(n, sizeof(int64_t));
-    fenwick fw = {calloc(tree_n + 1, sizeof(int64_t)), tree_n};
     size_t max_edges = (size_t)m0 * (size_t)(m0 - 1) / 2 + (n - (size_t)m0) * (size_t)mm;
+    roulette rl;
+    /* totals never pass sum (deg + 1) = 2 edges + n */
+    const int rl_rc = rl_init(&rl, n, 2 * (int64_t)max_edges + (int64_t)n);
     int32_t *eu = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
     int32_t *ev = malloc((max_edges ? max_edges : 1) * sizeof(int32_t));
     int32_t *picks = malloc((size_t)mm * sizeof(int32_t));
@@ -420,7 +495,7 @@ static int topo_scale_free(sp_host_model *m)
     unsigned char *fwd = NULL;
     double *wv = NULL;
     size_t ne = 0;
-    if (!deg || !fw.t || !eu || !ev || !picks || !stamp)
+    if (rl_rc || !deg || !eu || !ev || !picks || !stamp)
         goto done;
     for (size_t u = 0; u < n; u++)
         stamp[u] = -1;
@@ -435,12 +510,12 @@ static int topo_scale_free(sp_host_model *m)
             deg[v]++;
         }
     for (size_t u = 0; u < (size_t)m0; u++)
-        fw_add(&fw, u, deg[u] + 1);
+        rl_add(&rl, u, deg[u] + 1);
     int64_t degsum = 0;
     for (int u = 0; u < m0; u++)
         degsum += deg[u];
 
-    /* The tree holds deg[u] + 1 for every u < v, and so sums to degsum + v,
+    /* The roulette holds deg[u] + 1 for every u < v, and so sums to degsum + v,
      * the roulette total. The draw r = urand01() * total never exceeds that
      * integer total, so ceil(r) is a valid target of the descent. */
     for (size_t v = (size_t)m0; v < n; v++) {
@@ -455,7 +530,7 @@ static int topo_scale_free(sp_host_model *m)
             double cr = ceil(r);
             size_t pick = 0;
             if (cr > 0.0) {
-                size_t u = fw_lower_bound(&fw, (int64_t)cr);
+                size_t u = rl_pick(&rl, (int64_t)cr);
                 pick = (u < v) ? u : 0;
             }
             const int dup = stamp[pick] == (int64_t)v; /* already picked for v */
@@ -465,7 +540,7 @@ static int topo_scale_free(sp_host_model *m)
                 deg[v]++;
                 deg[pick]++;
                 degsum += 1; /* only deg[pick] counts in totals for u < v */
-                fw_add(&fw, pick, 1);
+                rl_add(&rl, pick, 1);
             }
             guard++;
         }
@@ -480,7 +555,7 @@ static int topo_scale_free(sp_host_model *m)
                 deg[v]++;
                 deg[pick]++;
                 degsum += 1;
-                fw_add(&fw, pick, 1);
+                rl_add(&rl, pick, 1);
             }
         }
         for (int a = 0; a < added; a++) {
@@ -489,7 +564,7 @@ static int topo_scale_free(sp_host_model *m)
             ne++;
         }
         /* node v joins the roulette for later nodes with weight deg[v] + A */
-        fw_add(&fw, v, deg[v] + 1);
+        rl_add(&rl, v, deg[v] + 1);
         degsum += deg[v];
     }
 
@@ -576,7 +651,7 @@ static int topo_scale_free(sp_host_model *m)
     rc = SP_OK;
 done:
     free(deg);
-    free(fw.t);
+    rl_free(&rl);
     free(eu);
     free(ev);
     free(picks);
