@@ -617,10 +617,10 @@ static int topo_scale_free(sp_host_model *m)
             for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++) {
                 const int f = (long long)draw_int() < K_half;
                 const double w = draw_weight_k(K_ei);
+                const size_t r = f ? i : (size_t)adj[k];
                 fwd[k] = (unsigned char)f;
                 wv[k] = w;
-                if (w != 0.0)
-                    m->row_ptr[(f ? i : (size_t)adj[k]) + 1]++;
+                m->row_ptr[r + 1] += (w != 0.0);
             }
     }
     for (size_t i = 0; i < n; i++)
@@ -631,23 +631,21 @@ static int topo_scale_free(sp_host_model *m)
     if (!m->col || !m->w)
         goto done;
     memcpy(fill, m->row_ptr, n * sizeof(int64_t));
-    /* Row r holds its columns below r (edges (i, r) oriented r -> i; the outer
-     * loop visits i ascending) and then those above r (its own bucket,
-     * ascending): ascending columns with no sort. */
+    /* One pass with i ascending: row r receives its columns below r while
+     * i < r (edges (i, r) oriented r -> i), then its columns above r at i = r
+     * (its own bucket, ascending), and nothing later -- ascending columns with
+     * no sort. The orientation is random, so the row and column are selected
+     * rather than branched on. */
     for (size_t i = 0; i < n; i++)
-        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++)
-            if (!fwd[k] && wv[k] != 0.0) {
-                const int64_t at = fill[adj[k]]++;
-                m->col[at] = (int32_t)i;
-                m->w[at] = wv[k];
-            }
-    for (size_t i = 0; i < n; i++)
-        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++)
-            if (fwd[k] && wv[k] != 0.0) {
-                const int64_t at = fill[i]++;
-                m->col[at] = adj[k];
-                m->w[at] = wv[k];
-            }
+        for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++) {
+            if (wv[k] == 0.0)
+                continue;
+            const size_t j = (size_t)adj[k];
+            const int f = fwd[k];
+            const int64_t at = fill[f ? i : j]++;
+            m->col[at] = (int32_t)(f ? j : i);
+            m->w[at] = wv[k];
+        }
     rc = SP_OK;
 done:
     free(deg);
