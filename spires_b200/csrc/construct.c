@@ -64,11 +64,62 @@ int sp_rand_next(sp_rand_state *s)
     return (int)(v >> 1);
 }
 
+/* Block reader over a private generator: the same draws, produced a block at
+ * a time, and open to loops that look at several upcoming draws at once. It
+ * keeps the raw words x[q] = x[q-31] + x[q-3] (mod 2^32), the draws being
+ * x[q] >> 1, with the 31 words before the unread ones in front of them (the
+ * generator's state at any position is just the 31 raw words before it, the
+ * front index on the oldest, the back index three behind the front). */
+#define SP_STREAM_BLOCK 4096
+typedef struct {
+    uint32_t x[31 + SP_STREAM_BLOCK];
+    int pos; /* the next unread word, >= 31 */
+    int end; /* words held */
+} draw_stream;
+
+static void ds_open(draw_stream *d, const sp_rand_state *g)
+{
+    for (int k = 0; k < 31; k++) /* oldest first: it sits at the front index */
+        d->x[k] = (uint32_t)g->r[(g->f + k) % 31];
+    d->pos = d->end = 31;
+}
+
+/* keep the unread words and the 31 before them, then fill the block */
+static void ds_refill(draw_stream *d)
+{
+    const int from = d->pos - 31, keep = d->end - from;
+    memmove(d->x, d->x + from, (size_t)keep * sizeof(uint32_t));
+    d->pos = 31;
+    /* the last three words ride in registers: three independent add chains */
+    uint32_t a = d->x[keep - 3], b = d->x[keep - 2], c = d->x[keep - 1];
+    int q = keep;
+    for (; q + 3 <= 31 + SP_STREAM_BLOCK; q += 3) {
+        a += d->x[q - 31];
+        b += d->x[q - 30];
+        c += d->x[q - 29];
+        d->x[q] = a;
+        d->x[q + 1] = b;
+        d->x[q + 2] = c;
+    }
+    for (; q < 31 + SP_STREAM_BLOCK; q++)
+        d->x[q] = d->x[q - 31] + d->x[q - 3];
+    d->end = 31 + SP_STREAM_BLOCK;
+}
+
+static inline int ds_next(draw_stream *d)
+{
+    if (d->pos == d->end)
+        ds_refill(d);
+    return (int)(d->x[d->pos++] >> 1);
+}
+
 /* The draw source of the current thread's build: the C library's rand()
- * (the reference behaviour) unless sp_model_build_seeded installed a private
- * generator. */
-static __thread sp_rand_state *tl_rng;
-static int draw_int(void) { return tl_rng ? sp_rand_next(tl_rng) : rand(); }
+ * (the reference behaviour) unless sp_model_build_seeded installed a reader
+ * over a private generator. Hot loops read the pointer once and draw through
+ * draw_from. */
+static __thread draw_stream *tl_stream;
+static inline int draw_from(draw_stream *d) { return d ? ds_next(d) : rand(); }
+static int draw_int(void) { return draw_from(tl_stream); }
 
 /* (double)rand()/RAND_MAX, src/reservoir.c:330-333 */
 static double urand01(void) { return (double)draw_int() / (double)RAND_MAX; }
@@ -98,120 +149,28 @@ static long long draw_threshold(double c)
     return lo;
 }
 
-/* draw_weight(ei_ratio) with the sign test as a draw comparison against
- * K_ei = draw_threshold(ei_ratio): the same two draws, the same value */
-static double draw_weight_k(long long K_ei)
+/* urand01() from a given source */
+static inline double urand01_from(draw_stream *d) { return (double)draw_from(d) / (double)RAND_MAX; }
+
+/* draw_weight(ei_ratio) from a given source, with the sign test as a draw
+ * comparison against K_ei = draw_threshold(ei_ratio): the same two draws,
+ * the same value */
+static inline double weight_from(draw_stream *d, long long K_ei)
 {
-    const double magnitude = (double)draw_int() / RAND_MAX;
-    return (long long)draw_int() < K_ei ? magnitude : -magnitude;
+    const double magnitude = (double)draw_from(d) / RAND_MAX;
+    return (long long)draw_from(d) < K_ei ? magnitude : -magnitude;
 }
 
-/* ------------------------------------------------------- triplet buffer -- */
+/* ------------------------------------------------------------------ CSR -- */
 
-typedef struct {
-    int32_t r, c;
-    double v;
-} trip;
-
-typedef struct {
-    trip *t;
-    size_t n, cap;
-} tripbuf;
-
-static int tb_push(tripbuf *b, int32_t r, int32_t c, double v)
+/* a graph with no edges: every row empty */
+static int csr_empty(sp_host_model *m)
 {
-    if (b->n == b->cap) {
-        size_t nc = b->cap ? b->cap * 2 : 1024;
-        trip *nt = realloc(b->t, nc * sizeof(trip));
-        if (!nt)
-            return -1;
-        b->t = nt;
-        b->cap = nc;
-    }
-    b->t[b->n].r = r;
-    b->t[b->n].c = c;
-    b->t[b->n].v = v;
-    b->n++;
-    return 0;
-}
-
-static int trip_cmp(const void *a, const void *b)
-{
-    const trip *x = a, *y = b;
-    if (x->r != y->r)
-        return x->r < y->r ? -1 : 1;
-    if (x->c != y->c)
-        return x->c < y->c ? -1 : 1;
-    return 0;
-}
-
-/* Triplets (unique (r,c), any order) -> CSR with ascending columns, dropping
- * entries equal to zero exactly as csr_build_from_dense does
- * (src/sparse.c:7-42: `dense[k] != 0.0`). */
-/* Stable counting sort of the triplets by row; rows whose columns are then
- * not ascending (none, for the generators here) are sorted on their own. */
-static int trips_sort_rows(size_t n, tripbuf *b)
-{
-    int64_t *off = calloc(n + 1, sizeof(int64_t));
-    trip *t = malloc((b->n ? b->n : 1) * sizeof(trip));
-    if (!off || !t) {
-        free(off);
-        free(t);
-        return SP_EALLOC;
-    }
-    for (size_t k = 0; k < b->n; k++)
-        off[b->t[k].r + 1]++;
-    for (size_t i = 0; i < n; i++)
-        off[i + 1] += off[i];
-    for (size_t k = 0; k < b->n; k++)
-        t[off[b->t[k].r]++] = b->t[k];
-    /* off[i] now holds the end of row i */
-    int64_t start = 0;
-    for (size_t i = 0; i < n; i++) {
-        for (int64_t k = start + 1; k < off[i]; k++)
-            if (t[k].c < t[k - 1].c) {
-                qsort(t + start, (size_t)(off[i] - start), sizeof(trip), trip_cmp);
-                break;
-            }
-        start = off[i];
-    }
-    free(off);
-    free(b->t);
-    b->t = t;
-    b->cap = b->n ? b->n : 1;
-    return SP_OK;
-}
-
-static int csr_from_trips(sp_host_model *m, tripbuf *b, int sorted)
-{
-    size_t n = m->n;
-    if (!sorted) {
-        int rc = trips_sort_rows(n, b);
-        if (rc)
-            return rc;
-    }
-    size_t nnz = 0;
-    for (size_t k = 0; k < b->n; k++)
-        if (b->t[k].v != 0.0)
-            nnz++;
-    m->row_ptr = calloc(n + 1, sizeof(int64_t));
-    m->col = malloc((nnz ? nnz : 1) * sizeof(int32_t));
-    m->w = malloc((nnz ? nnz : 1) * sizeof(double));
-    if (!m->row_ptr || !m->col || !m->w)
-        return SP_EALLOC;
-    size_t idx = 0;
-    for (size_t k = 0; k < b->n; k++) {
-        if (b->t[k].v == 0.0)
-            continue;
-        m->row_ptr[b->t[k].r + 1]++;
-        m->col[idx] = b->t[k].c;
-        m->w[idx] = b->t[k].v;
-        idx++;
-    }
-    for (size_t i = 0; i < n; i++)
-        m->row_ptr[i + 1] += m->row_ptr[i];
-    m->nnz = nnz;
-    return SP_OK;
+    m->row_ptr = calloc(m->n + 1, sizeof(int64_t));
+    m->col = malloc(sizeof(int32_t));
+    m->w = malloc(sizeof(double));
+    m->nnz = 0;
+    return (m->row_ptr && m->col && m->w) ? SP_OK : SP_EALLOC;
 }
 
 /* ------------------------------------------------------------ topologies -- */
@@ -220,6 +179,25 @@ static int csr_from_trips(sp_host_model *m, tripbuf *b, int sorted)
  * out in order and columns ascending, so the CSR is written directly (zero
  * weights dropped, as csr_build_from_dense does), with the draws in the
  * reference's order: the edge test, then the weight's two draws. */
+static int er_reserve(sp_host_model *m, size_t *cap, size_t need)
+{
+    if (need <= *cap)
+        return SP_OK;
+    size_t nc = *cap + *cap / 2 + 1024;
+    if (nc < need)
+        nc = need;
+    int32_t *col = realloc(m->col, nc * sizeof(int32_t));
+    if (!col)
+        return SP_EALLOC;
+    m->col = col;
+    double *w = realloc(m->w, nc * sizeof(double));
+    if (!w)
+        return SP_EALLOC;
+    m->w = w;
+    *cap = nc;
+    return SP_OK;
+}
+
 static int topo_random(sp_host_model *m)
 {
     const size_t n = m->n;
@@ -232,32 +210,76 @@ static int topo_random(sp_host_model *m)
     /* the edge test and the weight's sign test as draw comparisons */
     const long long K = draw_threshold(m->connectivity);
     const long long K_ei = draw_threshold(m->ei_ratio);
-    sp_rand_state *g = tl_rng;
+    draw_stream *ds = tl_stream;
     size_t e = 0;
-    for (size_t i = 0; i < n; i++) {
-        m->row_ptr[i] = (int64_t)e;
-        for (size_t j = 0; j < n; j++) {
-            if (i == j)
-                continue;
-            if ((long long)(g ? sp_rand_next(g) : rand()) < K) {
-                const double v = draw_weight_k(K_ei);
-                if (v == 0.0)
-                    continue;
-                if (e == cap) {
-                    const size_t nc = cap + cap / 2 + 1024;
-                    int32_t *nc_col = realloc(m->col, nc * sizeof(int32_t));
-                    if (!nc_col)
-                        return SP_EALLOC;
-                    m->col = nc_col;
-                    double *nc_w = realloc(m->w, nc * sizeof(double));
-                    if (!nc_w)
-                        return SP_EALLOC;
-                    m->w = nc_w;
-                    cap = nc;
+    if (ds) {
+        /* Private generator: a pair takes one draw, or three when it is an
+         * edge. Reading them from a block, the pairs up to the next edge are
+         * a run of draws at or above K, found by a scan that does not branch
+         * per pair on the random outcome; rows are crossed by counting. */
+        const size_t per_row = n - 1; /* pairs (i, j), j != i, of a row */
+        size_t i = 0, jj = 0;         /* the next pair: row i, its jj-th column */
+        int pos = ds->pos, end = ds->end; /* local: the stores below may alias */
+        while (i < n) {
+            if (pos == end) {
+                ds->pos = pos;
+                ds_refill(ds);
+                pos = ds->pos;
+                end = ds->end;
+            }
+            const size_t left = per_row - jj, avail = (size_t)(end - pos);
+            const size_t span = left < avail ? left : avail;
+            const uint32_t *x = ds->x + pos;
+            size_t q = 0;
+            while (q < span && (long long)(x[q] >> 1) >= K)
+                q++;
+            pos += (int)q;
+            jj += q;
+            if (q < span) { /* an edge: its test draw, then the weight's two */
+                pos++;
+                if (end - pos < 2) {
+                    ds->pos = pos;
+                    ds_refill(ds);
+                    pos = ds->pos;
+                    end = ds->end;
                 }
-                m->col[e] = (int32_t)j;
-                m->w[e] = v;
-                e++;
+                const int mag_draw = (int)(ds->x[pos] >> 1);
+                const long long sign_draw = (long long)(ds->x[pos + 1] >> 1);
+                pos += 2;
+                if (mag_draw != 0) { /* a zero weight is dropped, either sign */
+                    if (e == cap && er_reserve(m, &cap, e + 1))
+                        return SP_EALLOC;
+                    const double mag = (double)mag_draw / RAND_MAX;
+                    m->col[e] = (int32_t)(jj + (jj >= i));
+                    m->w[e] = sign_draw < K_ei ? mag : -mag;
+                    e++;
+                }
+                jj++;
+            }
+            if (jj == per_row) {
+                i++;
+                jj = 0;
+                if (i < n)
+                    m->row_ptr[i] = (int64_t)e;
+            }
+        }
+        ds->pos = pos;
+    } else {
+        for (size_t i = 0; i < n; i++) {
+            m->row_ptr[i] = (int64_t)e;
+            for (size_t j = 0; j < n; j++) {
+                if (i == j)
+                    continue;
+                if ((long long)rand() < K) {
+                    const double v = weight_from(NULL, K_ei);
+                    if (v == 0.0)
+                        continue;
+                    if (er_reserve(m, &cap, e + 1))
+                        return SP_EALLOC;
+                    m->col[e] = (int32_t)j;
+                    m->w[e] = v;
+                    e++;
+                }
             }
         }
     }
@@ -266,14 +288,33 @@ static int topo_random(sp_host_model *m)
     return SP_OK;
 }
 
+static void sort_i32_small(int32_t *v, int k)
+{
+    for (int a = 1; a < k; a++) { /* insertion sort: a row's rewired targets */
+        const int32_t x = v[a];
+        int c = a - 1;
+        while (c >= 0 && v[c] > x) {
+            v[c + 1] = v[c];
+            c--;
+        }
+        v[c + 1] = x;
+    }
+}
+
 /* Watts-Strogatz on a directed ring; src/reservoir.c:399-443. The ring pass
  * draws every ring weight before any rewiring draw, so ring weights are kept
- * per row and each row is then rewired against its own dense scratch row. */
-static int topo_small_world(sp_host_model *m, tripbuf *b)
+ * per row and each row is then rewired against its own dense scratch row.
+ * A row's columns are its ring targets -- two ascending runs, 0..i+half-n
+ * when the ring wraps and i+1..min(i+half, n-1) -- and its rewired targets,
+ * sorted on their own; merging the three gives the row's columns ascending,
+ * written straight to CSR (zero weights, the rewired-away ring edges among
+ * them, dropped as csr_build_from_dense drops them). A row never holds more
+ * than half entries: each rewiring removes one and adds at most one. */
+static int topo_small_world(sp_host_model *m)
 {
     size_t n = m->n;
     if (n < 3)
-        return SP_OK;
+        return csr_empty(m);
     int K = (int)((m->connectivity) * (double)(n - 1) + 0.5);
     if (K < 2)
         K = 2;
@@ -282,73 +323,99 @@ static int topo_small_world(sp_host_model *m, tripbuf *b)
     if (K >= (int)n)
         K = (int)n - 1;
     const double p = 0.1;
-    int half = K / 2;
+    draw_stream *ds = tl_stream;
+    const long long K_ei = draw_threshold(m->ei_ratio);
+    const int half = K / 2;
+    const size_t cap = n * (size_t)half;
 
-    double *ring = malloc((size_t)n * (size_t)(half > 0 ? half : 1) * sizeof(double));
+    double *ring = malloc((cap ? cap : 1) * sizeof(double));
     double *row = calloc(n, sizeof(double));
-    int32_t *touched = malloc(((size_t)2 * half + 2) * sizeof(int32_t));
-    if (!ring || !row || !touched) {
+    int32_t *added = malloc(((size_t)half + 1) * sizeof(int32_t));
+    m->row_ptr = calloc(n + 1, sizeof(int64_t));
+    m->col = malloc((cap ? cap : 1) * sizeof(int32_t));
+    m->w = malloc((cap ? cap : 1) * sizeof(double));
+    if (!ring || !row || !added || !m->row_ptr || !m->col || !m->w) {
         free(ring);
         free(row);
-        free(touched);
+        free(added);
         return SP_EALLOC;
     }
     for (size_t i = 0; i < n; i++)
         for (int s = 1; s <= half; s++)
-            ring[i * half + (s - 1)] = draw_weight(m->ei_ratio);
+            ring[i * half + (s - 1)] = weight_from(ds, K_ei);
 
+    size_t e = 0;
     for (size_t i = 0; i < n; i++) {
-        int nt = 0;
-        for (int s = 1; s <= half; s++) {
-            size_t j = (i + (size_t)s) % n;
-            row[j] = ring[i * half + (s - 1)];
-            touched[nt++] = (int32_t)j;
-        }
+        for (int s = 1; s <= half; s++)
+            row[(i + (size_t)s) % n] = ring[i * half + (s - 1)];
+        int na = 0;
         for (int s = 1; s <= half; s++) {
             size_t j_old = (i + (size_t)s) % n;
-            if (urand01() < p) {
+            if (urand01_from(ds) < p) {
                 row[j_old] = 0.0;
                 size_t j_new;
                 int attempts = 0;
                 do {
-                    j_new = (size_t)(urand01() * (double)n);
+                    j_new = (size_t)(urand01_from(ds) * (double)n);
                     if (j_new >= n)
                         j_new = n - 1;
                     if (++attempts > 10 * (int)n)
                         break;
                 } while (j_new == i || row[j_new] != 0.0);
                 if (j_new != i) {
-                    row[j_new] = draw_weight(m->ei_ratio);
-                    touched[nt++] = (int32_t)j_new;
+                    row[j_new] = weight_from(ds, K_ei);
+                    added[na++] = (int32_t)j_new;
                 }
             }
         }
-        /* emit the row in ascending column order, each column once */
-        for (int a = 1; a < nt; a++) { /* insertion sort: nt <= 2*half */
-            int32_t v = touched[a];
-            int c = a - 1;
-            while (c >= 0 && touched[c] > v) {
-                touched[c + 1] = touched[c];
-                c--;
-            }
-            touched[c + 1] = v;
-        }
-        for (int a = 0; a < nt; a++) {
-            if (a > 0 && touched[a] == touched[a - 1])
+        sort_i32_small(added, na);
+        /* ring runs: [lo_a, hi_a] above i, [0, hi_b] after the wrap (if any) */
+        const size_t top = i + (size_t)half;
+        const size_t hi_a = top < n ? top : n - 1;
+        const long long hi_b = top < n ? -1 : (long long)(top - n);
+        long long rb = 0;     /* next of the wrapped run */
+        size_t ra = i + 1;    /* next of the run above i */
+        int k = 0;            /* next rewired target */
+        int64_t last = -1;
+        for (;;) {
+            /* the smallest pending column of the three lists */
+            int64_t c;
+            if (rb <= hi_b)
+                c = rb;
+            else if (ra <= hi_a)
+                c = (int64_t)ra;
+            else
+                c = INT64_MAX;
+            if (k < na && added[k] < c)
+                c = added[k];
+            if (c == INT64_MAX)
+                break;
+            if (rb <= hi_b && c == rb)
+                rb++;
+            else if (ra <= hi_a && c == (int64_t)ra)
+                ra++;
+            if (k < na && added[k] == c)
+                k++;
+            if (c == last)
                 continue;
-            if (tb_push(b, (int32_t)i, touched[a], row[touched[a]])) {
-                free(ring);
-                free(row);
-                free(touched);
-                return SP_EALLOC;
+            last = c;
+            const double v = row[c];
+            if (v != 0.0) {
+                m->col[e] = (int32_t)c;
+                m->w[e] = v;
+                e++;
             }
         }
-        for (int a = 0; a < nt; a++)
-            row[touched[a]] = 0.0;
+        for (int s = 1; s <= half; s++)
+            row[(i + (size_t)s) % n] = 0.0;
+        for (int a2 = 0; a2 < na; a2++)
+            row[added[a2]] = 0.0;
+        m->row_ptr[i + 1] = (int64_t)e;
     }
+    m->nnz = e;
     free(ring);
     free(row);
-    free(touched);
+    free(added);
     return SP_OK;
 }
 
@@ -467,10 +534,8 @@ static int cmp_i32(const void *a, const void *b)
 static int topo_scale_free(sp_host_model *m)
 {
     size_t n = m->n;
-    if (n < 2) {
-        tripbuf none = {0};
-        return csr_from_trips(m, &none, 1);
-    }
+    if (n < 2)
+        return csr_empty(m);
     int mm = (int)((m->connectivity) * (double)(n - 1) + 0.5);
     if (mm < 1)
         mm = 1;
@@ -481,6 +546,7 @@ static int topo_scale_free(sp_host_model *m)
         m0 = (int)n - 1;
 
     int rc = SP_EALLOC;
+    draw_stream *ds = tl_stream;
     int64_t *deg = calloc(n, sizeof(int64_t));
     size_t max_edges = (size_t)m0 * (size_t)(m0 - 1) / 2 + (n - (size_t)m0) * (size_t)mm;
     roulette rl;
@@ -525,7 +591,7 @@ static int topo_scale_free(sp_host_model *m)
             double total = (double)(degsum + (int64_t)v);
             if (total <= 0.0)
                 total = (double)v;
-            double r = urand01() * total;
+            double r = urand01_from(ds) * total;
             /* first u with r <= acc(u); acc(u) integral, so acc >= ceil(r) */
             double cr = ceil(r);
             size_t pick = 0;
@@ -545,7 +611,7 @@ static int topo_scale_free(sp_host_model *m)
             guard++;
         }
         while (added < mm) {
-            size_t pick = (size_t)(urand01() * (double)v);
+            size_t pick = (size_t)(urand01_from(ds) * (double)v);
             if (pick >= v)
                 pick = v - 1;
             const int dup = stamp[pick] == (int64_t)v; /* already picked for v */
@@ -615,8 +681,8 @@ static int topo_scale_free(sp_host_model *m)
         const long long K_ei = draw_threshold(m->ei_ratio);
         for (size_t i = 0; i < n; i++)
             for (int64_t k = adj_off[i]; k < adj_off[i + 1]; k++) {
-                const int f = (long long)draw_int() < K_half;
-                const double w = draw_weight_k(K_ei);
+                const int f = (long long)draw_from(ds) < K_half;
+                const double w = weight_from(ds, K_ei);
                 const size_t r = f ? i : (size_t)adj[k];
                 fwd[k] = (unsigned char)f;
                 wv[k] = w;
@@ -1049,15 +1115,12 @@ int sp_model_build(sp_host_model *m)
     for (size_t k = 0; k < n * m->din; k++)
         m->W_in[k] = draw_weight(m->ei_ratio);
 
-    tripbuf b = {0};
     switch (m->conn_type) {
     case SP_CONN_RANDOM:
         rc = topo_random(m);
         break;
     case SP_CONN_SMALL_WORLD:
-        rc = topo_small_world(m, &b);
-        if (!rc)
-            rc = csr_from_trips(m, &b, 1);
+        rc = topo_small_world(m);
         break;
     case SP_CONN_SCALE_FREE:
         rc = topo_scale_free(m);
@@ -1065,7 +1128,6 @@ int sp_model_build(sp_host_model *m)
     default:
         rc = SP_EINVAL;
     }
-    free(b.t);
     if (rc)
         return rc;
 
@@ -1163,9 +1225,14 @@ int sp_model_build_seeded(sp_host_model *m, unsigned seed)
 {
     sp_rand_state st;
     sp_rand_seed(&st, seed);
-    sp_rand_state *prev = tl_rng;
-    tl_rng = &st;
+    draw_stream *ds = malloc(sizeof(*ds));
+    if (!ds)
+        return SP_EALLOC;
+    ds_open(ds, &st);
+    draw_stream *prev = tl_stream;
+    tl_stream = ds;
     const int rc = sp_model_build(m);
-    tl_rng = prev;
+    tl_stream = prev;
+    free(ds);
     return rc;
 }

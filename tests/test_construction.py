@@ -92,6 +92,22 @@ def test_private_generator_matches_global_rand(seed, topo):
     assert np.array_equal(a.w_out(), b.w_out())
 
 
+@pytest.mark.parametrize("n,conn", [(1500, 0.3), (1500, 0.0005), (2500, 0.02)])
+@pytest.mark.parametrize("topo", [sp.CONN_RANDOM, sp.CONN_SMALL_WORLD, sp.CONN_SCALE_FREE])
+def test_private_generator_matches_global_rand_large(n, conn, topo):
+    """Dense and near-empty graphs (edge runs that cross rows and draw blocks),
+    an uneven sign ratio, and per-edge synapse draws after the topology."""
+    cfg = sp.make_config(n, 1, 2, rho=0.9, ei=0.37, conn=conn, topo=topo, neuron=sp.FLIF_GL,
+                         nparams=(1.0, 0.0, 0.0, 20.0, 0.7, 32.0, 0.1, 2.0),
+                         synapse=sp.SYN_PSC_HET, sparams=(1.0, 20.0))
+    a = sp.HostModel(cfg, seed=11)
+    b = sp.HostModel(cfg, seed=11, private=True)
+    for x, y in zip(a.csr(), b.csr()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.w_in(), b.w_in())
+    assert np.array_equal(a.w_out(), b.w_out())
+
+
 def test_private_generator_leaves_global_rand_alone():
     sp.libc.srand(7)
     first = sp.libc.rand()
