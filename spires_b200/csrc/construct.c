@@ -22,10 +22,20 @@
  * cos) are computed here with the same expressions the reference evaluates, so
  * the device only ever sees their bits.
  */
+#include <limits.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
 #include "sp_model.h"
+
+/* (int)x as x86-64's truncating conversion performs it -- NaN and values
+ * outside the int range give INT_MIN, which is what the reference's casts of
+ * configuration values produce there -- without the undefined behaviour of
+ * the C cast. */
+static int trunc_int(double x)
+{
+    return (x > -2147483649.0 && x < 2147483648.0) ? (int)x : INT_MIN;
+}
 
 /* ---------------------------------------------------------------- draws -- */
 
@@ -201,7 +211,9 @@ static int er_reserve(sp_host_model *m, size_t *cap, size_t need)
 static int topo_random(sp_host_model *m)
 {
     const size_t n = m->n;
-    size_t cap = (size_t)((double)n * (double)n * m->connectivity * 1.05) + 1024;
+    const double density = m->connectivity > 0.0 ? (m->connectivity < 1.0 ? m->connectivity : 1.0)
+                                                 : 0.0; /* NaN: no edges */
+    size_t cap = (size_t)((double)n * (double)n * density * 1.05) + 1024;
     m->row_ptr = calloc(n + 1, sizeof(int64_t));
     m->col = malloc(cap * sizeof(int32_t));
     m->w = malloc(cap * sizeof(double));
@@ -315,7 +327,7 @@ static int topo_small_world(sp_host_model *m)
     size_t n = m->n;
     if (n < 3)
         return csr_empty(m);
-    int K = (int)((m->connectivity) * (double)(n - 1) + 0.5);
+    int K = trunc_int((m->connectivity) * (double)(n - 1) + 0.5);
     if (K < 2)
         K = 2;
     if (K % 2)
@@ -354,12 +366,12 @@ static int topo_small_world(sp_host_model *m)
             if (urand01_from(ds) < p) {
                 row[j_old] = 0.0;
                 size_t j_new;
-                int attempts = 0;
+                long long attempts = 0;
                 do {
                     j_new = (size_t)(urand01_from(ds) * (double)n);
                     if (j_new >= n)
                         j_new = n - 1;
-                    if (++attempts > 10 * (int)n)
+                    if (++attempts > 10 * (long long)n)
                         break;
                 } while (j_new == i || row[j_new] != 0.0);
                 if (j_new != i) {
@@ -536,7 +548,7 @@ static int topo_scale_free(sp_host_model *m)
     size_t n = m->n;
     if (n < 2)
         return csr_empty(m);
-    int mm = (int)((m->connectivity) * (double)(n - 1) + 0.5);
+    int mm = trunc_int((m->connectivity) * (double)(n - 1) + 0.5);
     if (mm < 1)
         mm = 1;
     if (mm >= (int)n)
@@ -585,8 +597,9 @@ static int topo_scale_free(sp_host_model *m)
      * the roulette total. The draw r = urand01() * total never exceeds that
      * integer total, so ceil(r) is a valid target of the descent. */
     for (size_t v = (size_t)m0; v < n; v++) {
-        int added = 0, guard = 0;
-        while (added < mm && guard < 50 * mm) {
+        int added = 0;
+        long long guard = 0;
+        while (added < mm && guard < 50LL * mm) {
             /* total = sum_{u<v} (deg[u] + A): an exact integer in double */
             double total = (double)(degsum + (int64_t)v);
             if (total <= 0.0)
@@ -840,7 +853,7 @@ int sp_model_derive_neuron(sp_host_model *m)
         break;
     case SP_FLIF_GL: { /* src/neurons/flif_gl.c:7-49, src/neuron.c:36-54 */
         double T_mem = p[5];
-        int L = (T_mem > 0 && dt > 0) ? (int)(T_mem / dt) : 2000;
+        int L = (T_mem > 0 && dt > 0) ? trunc_int(T_mem / dt) : 2000;
         if (L > SP_MAX_MEM_LEN)
             L = SP_MAX_MEM_LEN;
         if (L < 1)
@@ -867,7 +880,7 @@ int sp_model_derive_neuron(sp_host_model *m)
     }
     case SP_FLIF_CAPUTO: { /* src/neurons/flif_caputo.c:5-40 */
         double T_mem = p[8];
-        int mem_len = (T_mem > 0) ? (int)(T_mem / dt) : SP_MAX_MEM_LEN;
+        int mem_len = (T_mem > 0) ? trunc_int(T_mem / dt) : SP_MAX_MEM_LEN;
         if (mem_len > SP_MAX_MEM_LEN)
             mem_len = SP_MAX_MEM_LEN;
         int D = mem_len - 2;
@@ -1017,7 +1030,7 @@ int sp_model_build_synapse(sp_host_model *m, const double *unused)
         double alpha = sp ? sp[0] : 1.0;
         double tau = sp ? sp[1] : 1.0;
         double T_mem = sp ? sp[2] : 10.0;
-        int L = (T_mem > 0 && dt > 0) ? (int)(T_mem / dt) : 2000;
+        int L = (T_mem > 0 && dt > 0) ? trunc_int(T_mem / dt) : 2000;
         if (L > SP_MAX_MEM_LEN)
             L = SP_MAX_MEM_LEN;
         if (L < 1)
@@ -1037,7 +1050,7 @@ int sp_model_build_synapse(sp_host_model *m, const double *unused)
         double tau_syn = sp ? sp[1] : 1.0;
         double tau_min = sp ? sp[2] : 1.0;
         double tau_max = sp ? sp[3] : 20.0;
-        int N = sp ? (int)(sp[4] + 0.5) : 8;
+        int N = sp ? trunc_int(sp[4] + 0.5) : 8;
         if (N < 1)
             N = 1;
         double sin_apia = sin(alpha * PI_);

@@ -115,3 +115,30 @@ def test_private_generator_leaves_global_rand_alone():
     cfg = sp.make_config(64, 1, 1, conn=0.1)
     sp.HostModel(cfg, seed=99, private=True)
     assert sp.libc.rand() == first
+
+
+@pytest.mark.parametrize("topo", [sp.CONN_SMALL_WORLD, sp.CONN_SCALE_FREE])
+def test_out_of_range_connectivity_truncates_as_x86(topo):
+    """A degree parameter (connectivity * (n - 1) + 0.5) that is NaN or beyond
+    the int range converts to INT_MIN, as the reference's cast does on
+    x86-64, and so falls to the smallest degree -- the same graph as
+    connectivity 0."""
+    base = sp.HostModel(sp.make_config(200, conn=0.0, topo=topo), seed=5, private=True).csr()
+    for c in (1e12, -1e12, float("nan")):
+        g = sp.HostModel(sp.make_config(200, conn=c, topo=topo), seed=5, private=True).csr()
+        for x, y in zip(base, g):
+            assert np.array_equal(x, y)
+
+
+def test_out_of_range_ring_length_rejected():
+    lib = sp.load()
+    import ctypes as C
+    h = C.c_void_p()
+    # beyond the int range: INT_MIN, rejected as a ring length below one
+    cfg = sp.make_config(10, neuron=sp.FLIF_GL, nparams=(1.0, 0.0, 0.0, 20.0, 0.7, 1e300, 0.1, 2.0))
+    assert lib.spires_ext_model_build(C.byref(cfg), C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
+    # NaN fails T_mem > 0 and takes the default ring, as in the reference
+    cfg = sp.make_config(10, neuron=sp.FLIF_GL,
+                         nparams=(1.0, 0.0, 0.0, 20.0, 0.7, float("nan"), 0.1, 2.0))
+    m = sp.HostModel(cfg, seed=1)
+    assert m.n == 10
