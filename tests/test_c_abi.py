@@ -1,7 +1,8 @@
 """A C caller builds against include/spires.h -- and against the original
-project's header when it is present -- and links against libspires.so: the
-signatures the compiler checks, the enumerator values and the argument-check
-paths that need no GPU (tests/c/relink_check.c)."""
+project's header when it is present -- and links against libspires.so, or
+libspires.a with its documented extra libraries: the signatures the compiler
+checks, the enumerator values and the argument-check paths that need no GPU
+(tests/c/relink_check.c)."""
 import os
 import shutil
 import subprocess
@@ -16,10 +17,16 @@ REF_INCLUDE = "/root/reference/include"
 pytestmark = pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
 
 
-def build_and_run(include_dir, tmp_path):
-    exe = str(tmp_path / "relink_check")
-    cmd = ["gcc", "-std=c11", "-Wall", "-Werror", "-I", include_dir, SRC, "-o", exe,
-           "-L", LIB, "-lspires", "-Wl,-rpath," + LIB]
+CUDA_LIB = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64")
+# the static archive's extra libraries, as the integration notes give them
+STATIC = [os.path.join(LIB, "libspires.a"), "-L" + CUDA_LIB, "-lcudart_static", "-lcublas",
+          "-Wl,-rpath," + CUDA_LIB, "-lstdc++", "-fopenmp", "-lpthread", "-ldl", "-lrt", "-lm"]
+
+
+def build_and_run(include_dir, tmp_path, static=False):
+    exe = str(tmp_path / ("relink_check_static" if static else "relink_check"))
+    link = STATIC if static else ["-L", LIB, "-lspires", "-Wl,-rpath," + LIB]
+    cmd = ["gcc", "-std=c11", "-Wall", "-Werror", "-I", include_dir, SRC, "-o", exe] + link
     out = subprocess.run(cmd, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     run = subprocess.run([exe], capture_output=True, text=True, timeout=120)
@@ -29,6 +36,12 @@ def build_and_run(include_dir, tmp_path):
 
 def test_c_caller_against_this_header(tmp_path):
     build_and_run(os.path.join(ROOT, "include"), tmp_path)
+
+
+@pytest.mark.skipif(not os.path.isfile(os.path.join(CUDA_LIB, "libcudart_static.a")),
+                    reason="static CUDA runtime absent")
+def test_c_caller_static_archive(tmp_path):
+    build_and_run(os.path.join(ROOT, "include"), tmp_path, static=True)
 
 
 @pytest.mark.skipif(not os.path.isfile(os.path.join(REF_INCLUDE, "spires.h")),
