@@ -48,3 +48,23 @@ def test_c_caller_static_archive(tmp_path):
                     reason="original header absent")
 def test_c_caller_against_the_original_header(tmp_path):
     build_and_run(REF_INCLUDE, tmp_path)
+
+
+REF_EXAMPLES = "/root/reference/examples"
+
+
+@pytest.mark.parametrize("name", ["mackey_glass_prediction", "spoken_digit_recognition"])
+def test_original_examples_link_unchanged(name, tmp_path):
+    """The original project's example programs that use only the public API
+    compile against this include/spires.h and link against libspires.so as
+    they are (running them needs a GPU and, for the digits, a dataset). The
+    third example reaches into the original's internal headers and is not a
+    public-API caller."""
+    src = os.path.join(REF_EXAMPLES, name, name + ".c")
+    if not os.path.isfile(src):
+        pytest.skip("original examples absent")
+    exe = str(tmp_path / name)
+    cmd = ["gcc", "-std=gnu11", "-I", os.path.join(ROOT, "include"), src, "-o", exe, "-L", LIB,
+           "-lspires", "-Wl,-rpath," + LIB, "-lm"]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
