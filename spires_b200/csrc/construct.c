@@ -436,17 +436,22 @@ static int topo_small_world(sp_host_model *m)
  * target. The path of that search is random, so it is the latency of its
  * dependent loads that sets the pace.
  *
- * Main form: a 16-ary tree of int32 inclusive prefix sums, one 64-byte node
- * per 16 children (35 KB at 8000 nodes, cache-resident): a level costs one
- * node load and 16 comparisons in 4-lane vectors, against one load per level
- * of a binary tree. Graphs whose totals could pass INT32_MAX use a Fenwick
- * tree over int64 instead. Both return the same node for the same target. */
+ * Main form: a tree of int32 inclusive prefix sums -- 16-ary levels, one
+ * 64-byte node per 16 children, up to a single root node of at most 64
+ * entries (8000 nodes: 500 and 32 nodes of 16, a root of 32; 34 KB,
+ * cache-resident). A level costs one node load and its comparisons in 4-lane
+ * vectors, against one load per level of a binary tree; the wide root saves
+ * a level. Graphs whose totals could pass INT32_MAX use a Fenwick tree over
+ * int64 instead. Both return the same node for the same target. */
 typedef int32_t sp_v4i __attribute__((vector_size(16)));
+
+#define SP_ROOT_MAX 64
 
 typedef struct {
     int32_t *e;        /* 16 entries per node, levels stored leaf-parents first */
     size_t off[16];    /* first entry of each level */
-    int levels;        /* 16^levels >= n; the last level is the root node */
+    int levels;        /* 16-ary levels, then the root */
+    int root_w;        /* root entries, a multiple of 4, <= SP_ROOT_MAX */
     int64_t *t;        /* Fenwick form: t[1..tn], tn a power of two */
     size_t tn;
 } roulette;
@@ -455,16 +460,17 @@ static int rl_init(roulette *r, size_t n, int64_t max_total)
 {
     memset(r, 0, sizeof(*r));
     if (max_total <= INT32_MAX) {
-        size_t total = 0, span = 16;
+        size_t total = 0, count = n; /* units below the level being added */
         int l = 0;
-        do {
-            r->off[l] = total;
-            total += (n + span - 1) / span * 16;
-            l++;
-            if (span >= n)
-                break;
-            span <<= 4;
-        } while (l < 16);
+        while (count > SP_ROOT_MAX) {
+            const size_t nodes = (count + 15) / 16;
+            r->off[l++] = total;
+            total += nodes * 16;
+            count = nodes;
+        }
+        r->root_w = (int)((count + 3) / 4 * 4);
+        r->off[l++] = total;
+        total += (size_t)r->root_w;
         r->levels = l;
         if (posix_memalign((void **)&r->e, 64, total * sizeof(int32_t)))
             return SP_EALLOC;
@@ -488,10 +494,11 @@ static void rl_add(roulette *r, size_t u, int64_t d)
 {
     if (r->e) {
         const sp_v4i i0 = {0, 1, 2, 3}, i1 = {4, 5, 6, 7}, i2 = {8, 9, 10, 11},
-                     i3 = {12, 13, 14, 15};
+                     i3 = {12, 13, 14, 15}, four = {4, 4, 4, 4};
         const int32_t d32 = (int32_t)d;
         const sp_v4i dd = {d32, d32, d32, d32};
-        for (int l = 0; l < r->levels; l++) {
+        const int top = r->levels - 1;
+        for (int l = 0; l < top; l++) {
             sp_v4i *x = (sp_v4i *)(r->e + r->off[l] + (u >> (4 * (l + 1))) * 16);
             const int32_t slot = (int32_t)((u >> (4 * l)) & 15);
             const sp_v4i sl = {slot, slot, slot, slot};
@@ -500,6 +507,12 @@ static void rl_add(roulette *r, size_t u, int64_t d)
             x[2] += (i2 >= sl) & dd;
             x[3] += (i3 >= sl) & dd;
         }
+        sp_v4i *x = (sp_v4i *)(r->e + r->off[top]);
+        const int32_t slot = (int32_t)(u >> (4 * top));
+        const sp_v4i sl = {slot, slot, slot, slot};
+        sp_v4i idx = i0;
+        for (int q = 0; q < r->root_w / 4; q++, idx += four)
+            x[q] += (idx >= sl) & dd;
         return;
     }
     for (size_t k = u + 1; k <= r->tn; k += k & (~k + 1))
@@ -511,15 +524,23 @@ static size_t rl_pick(const roulette *r, int64_t target)
 {
     if (r->e) {
         int32_t tg = (int32_t)target;
-        size_t node = 0;
-        for (int l = r->levels - 1; l >= 0; l--) {
-            const int32_t *p = r->e + r->off[l] + node * 16;
+        const int top = r->levels - 1;
+        /* entries are nondecreasing: the count below the target is the child
+         * holding it */
+        const int32_t *p = r->e + r->off[top];
+        sp_v4i t = {tg, tg, tg, tg};
+        sp_v4i below = {0, 0, 0, 0};
+        for (int q = 0; q < r->root_w / 4; q++)
+            below += ((const sp_v4i *)p)[q] < t;
+        int32_t c = -(below[0] + below[1] + below[2] + below[3]);
+        tg -= c ? p[c - 1] : 0;
+        size_t node = (size_t)c;
+        for (int l = top - 1; l >= 0; l--) {
+            p = r->e + r->off[l] + node * 16;
             const sp_v4i *x = (const sp_v4i *)p;
-            const sp_v4i t = {tg, tg, tg, tg};
-            /* entries are nondecreasing: the count below the target is the
-             * child holding it */
-            const sp_v4i below = (x[0] < t) + (x[1] < t) + (x[2] < t) + (x[3] < t);
-            const int32_t c = -(below[0] + below[1] + below[2] + below[3]);
+            t = (sp_v4i){tg, tg, tg, tg};
+            below = (x[0] < t) + (x[1] < t) + (x[2] < t) + (x[3] < t);
+            c = -(below[0] + below[1] + below[2] + below[3]);
             tg -= c ? p[c - 1] : 0;
             node = node * 16 + (size_t)c;
         }
@@ -594,33 +615,37 @@ static int topo_scale_free(sp_host_model *m)
         degsum += deg[u];
 
     /* The roulette holds deg[u] + 1 for every u < v, and so sums to degsum + v,
-     * the roulette total. The draw r = urand01() * total never exceeds that
-     * integer total, so ceil(r) is a valid target of the descent. */
+     * the roulette total (an exact integer in double, at least v > 0). The
+     * draw r = urand01() * total never exceeds it, so ceil(r) is a valid
+     * target of the descent: the first u with r <= acc(u), acc(u) being
+     * integral, is the first with acc(u) >= ceil(r). */
     for (size_t v = (size_t)m0; v < n; v++) {
         int added = 0;
         long long guard = 0;
+        /* The attempts carry no branch on their random outcome: a repeated
+         * pick is written again and adds zero. The target of an attempt,
+         * ceil(urand01() * total), depends on whether the previous pick was
+         * kept (total + 1) or not, so both candidates are formed from the
+         * previous total while that pick is still being searched, and the
+         * outcome only selects one. */
+        int64_t total = degsum + (int64_t)v; /* the previous attempt's total */
+        int kept = 0;                         /* ... and whether it kept its pick */
         while (added < mm && guard < 50LL * mm) {
-            /* total = sum_{u<v} (deg[u] + A): an exact integer in double */
-            double total = (double)(degsum + (int64_t)v);
-            if (total <= 0.0)
-                total = (double)v;
-            double r = urand01_from(ds) * total;
-            /* first u with r <= acc(u); acc(u) integral, so acc >= ceil(r) */
-            double cr = ceil(r);
-            size_t pick = 0;
-            if (cr > 0.0) {
-                size_t u = rl_pick(&rl, (int64_t)cr);
-                pick = (u < v) ? u : 0;
-            }
-            const int dup = stamp[pick] == (int64_t)v; /* already picked for v */
-            if (pick != v && !dup) {
-                stamp[pick] = (int64_t)v;
-                picks[added++] = (int32_t)pick;
-                deg[v]++;
-                deg[pick]++;
-                degsum += 1; /* only deg[pick] counts in totals for u < v */
-                rl_add(&rl, pick, 1);
-            }
+            const double r01 = urand01_from(ds);
+            const int64_t t_same = (int64_t)ceil(r01 * (double)total);
+            const int64_t t_more = (int64_t)ceil(r01 * (double)(total + 1));
+            const int64_t target = kept ? t_more : t_same;
+            total += kept;
+            size_t pick = rl_pick(&rl, target); /* a zero target gives node 0 */
+            pick = (pick < v) ? pick : 0;
+            kept = stamp[pick] != (int64_t)v; /* not yet picked for v */
+            stamp[pick] = (int64_t)v;
+            picks[added] = (int32_t)pick;
+            added += kept;
+            deg[v] += kept;
+            deg[pick] += kept;
+            degsum += kept; /* only deg[pick] counts in totals for u < v */
+            rl_add(&rl, pick, kept);
             guard++;
         }
         while (added < mm) {
