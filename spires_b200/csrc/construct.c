@@ -773,6 +773,49 @@ done:
 /* edge count from which the power iteration runs on the device */
 #define SP_DEVICE_SR_MIN_NNZ ((size_t)1 << 15)
 
+/* y[i] = the row-i sum over its edges in ascending order, for rows [i0, i1).
+ * Four rows at a time, each with its own accumulator, keep four add chains in
+ * flight where one row alone would wait on each addition; every row's sum
+ * keeps its order and so its bits. */
+static void csr_matvec_rows(const int64_t *rp, const int32_t *col, const double *w,
+                            const double *x, double *y, size_t i0, size_t i1)
+{
+    size_t i = i0;
+    for (; i + 4 <= i1; i += 4) {
+        int64_t a0 = rp[i], a1 = rp[i + 1], a2 = rp[i + 2], a3 = rp[i + 3];
+        const int64_t e0 = a1, e1 = a2, e2 = a3, e3 = rp[i + 4];
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int64_t common = e0 - a0;
+        common = e1 - a1 < common ? e1 - a1 : common;
+        common = e2 - a2 < common ? e2 - a2 : common;
+        common = e3 - a3 < common ? e3 - a3 : common;
+        for (int64_t t = 0; t < common; t++) {
+            s0 += w[a0 + t] * x[col[a0 + t]];
+            s1 += w[a1 + t] * x[col[a1 + t]];
+            s2 += w[a2 + t] * x[col[a2 + t]];
+            s3 += w[a3 + t] * x[col[a3 + t]];
+        }
+        for (a0 += common; a0 < e0; a0++)
+            s0 += w[a0] * x[col[a0]];
+        for (a1 += common; a1 < e1; a1++)
+            s1 += w[a1] * x[col[a1]];
+        for (a2 += common; a2 < e2; a2++)
+            s2 += w[a2] * x[col[a2]];
+        for (a3 += common; a3 < e3; a3++)
+            s3 += w[a3] * x[col[a3]];
+        y[i] = s0;
+        y[i + 1] = s1;
+        y[i + 2] = s2;
+        y[i + 3] = s3;
+    }
+    for (; i < i1; i++) {
+        double s = 0.0;
+        for (int64_t k = rp[i]; k < rp[i + 1]; k++)
+            s += w[k] * x[col[k]];
+        y[i] = s;
+    }
+}
+
 double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *col,
                               const double *w)
 {
@@ -792,14 +835,11 @@ double sp_csr_spectral_radius(size_t n, const int64_t *row_ptr, const int32_t *c
      * maximum is exact in any order, so splitting the rows over threads gives
      * the same bits as the serial loop. */
     const int par = row_ptr[n] > 65536;
+    const size_t blk = 256, nblk = (n + blk - 1) / blk;
     for (unsigned int it = 0; it < max_iter; it++) {
 #pragma omp parallel for schedule(static) if (par)
-        for (size_t i = 0; i < n; i++) {
-            double s = 0.0;
-            for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++)
-                s += w[k] * x[col[k]];
-            y[i] = s;
-        }
+        for (size_t b = 0; b < nblk; b++)
+            csr_matvec_rows(row_ptr, col, w, x, y, b * blk, (b + 1) * blk < n ? (b + 1) * blk : n);
         lambda_new = 0.0;
         for (size_t i = 0; i < n; i++) {
             double a = fabs(y[i]);
