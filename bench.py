@@ -477,6 +477,50 @@ def run_classify_workload(args):
     print(json.dumps(out))
 
 
+def run_construct_workload(args):
+    """Host construction over the search space: --construct-count
+    configurations (N log-uniform in [500, 8000], connectivity U[0.02, 0.2],
+    the three topologies, sign ratios cycling through six values), each built
+    with its own seed by the private-generator host build on one thread, with
+    the graph drawing and the spectral-radius rescale timed apart. No GPU."""
+    import numpy as np
+
+    import spires_b200 as sp
+    from spires_b200 import search as S
+
+    space = S.Space()
+    rng = np.random.default_rng(0)
+    eis = (0.5, 0.3, 0.8, 0.0, 1.0, 0.123456789)
+    names = {sp.CONN_RANDOM: "erdos_renyi", sp.CONN_SMALL_WORLD: "small_world",
+             sp.CONN_SCALE_FREE: "scale_free"}
+    per = {v: {"count": 0, "topology_s": 0.0, "spectral_s": 0.0, "edges": 0} for v in names.values()}
+    t0 = time.perf_counter()
+    for k in range(args.construct_count):
+        th = rng.uniform(0, 1, S.DIM)
+        d = space.decode(th)
+        cfg = sp.make_config(d["n"], 1, 1, rho=d["rho"], ei=eis[k % len(eis)], conn=d["conn"],
+                             topo=d["topo"], neuron=sp.LIF_DISCRETE, nparams=(0.0, 1.0, 0.9, 0.0))
+        m = sp.HostModel(cfg, seed=k + 1, private=True)
+        e = per[names[d["topo"]]]
+        e["count"] += 1
+        e["topology_s"] += m.info.topology_ms / 1e3
+        e["spectral_s"] += m.info.spectral_ms / 1e3
+        e["edges"] += int(m.info.nnz)
+        del m
+    wall = time.perf_counter() - t0
+    topo_s = sum(v["topology_s"] for v in per.values())
+    print(json.dumps({
+        "metric": "host graph construction time", "value": topo_s, "unit": "s",
+        "higher_is_better": False, "workload": "construct", "graph_threads": 1,
+        "spectral_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+        "data": "synthetic", "count": args.construct_count,
+        "spectral_s": sum(v["spectral_s"] for v in per.values()), "wall_s": wall,
+        "per_topology": per,
+        "note": "graph drawing (value, one thread) and host power iteration (OpenMP "
+                "threads above 65536 edges) timed by the library; the batch and reservoir "
+                "builds run the power iteration of large graphs on the GPU"}))
+
+
 def run_small_lif_workload(args):
     """LIF_DISCRETE N=1000 [V_0=0, V_th=1, leak=0.9, bias=0], Erdos-Renyi 0.1
     with N(0,1) weights on the present edges rescaled to spectral radius 0.9
@@ -615,9 +659,10 @@ def main():
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
     ap.add_argument("--workload", default="step",
-                    choices=["step", "sweep", "search", "classify", "ridge", "small"],
+                    choices=["step", "sweep", "search", "classify", "ridge", "small", "construct"],
                     help="step (default, the headline line) or an additional workload")
     ap.add_argument("--sweep-count", type=int, default=256)
+    ap.add_argument("--construct-count", type=int, default=300)
     ap.add_argument("--sweep-tmax", type=int, default=10000,
                     help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
@@ -627,7 +672,7 @@ def main():
     if args.workload != "step":
         {"sweep": run_sweep_workload, "search": run_search_workload,
          "classify": run_classify_workload, "ridge": run_ridge_workload,
-         "small": run_small_lif_workload}[args.workload](args)
+         "small": run_small_lif_workload, "construct": run_construct_workload}[args.workload](args)
         return
 
     rank = int(os.environ.get("RANK", "0"))

@@ -32,6 +32,8 @@ typedef struct {
     int    syn_ring_len;      /* FRACTIONAL synapse history length */
     int    syn_components;    /* FRACTIONAL_MULTIEXP component count */
     double spectral_radius_before_rescale;
+    double topology_ms;       /* host time drawing the recurrent graph */
+    double spectral_ms;       /* time of the spectral-radius rescale (host or device) */
 } spires_ext_model_info;
 
 spires_status spires_ext_model_build(const spires_reservoir_config *cfg,

@@ -74,7 +74,8 @@ class ModelInfo(C.Structure):
                 ("num_outputs", C.c_size_t), ("nnz", C.c_size_t), ("ring_len", C.c_int),
                 ("micro_steps", C.c_int), ("syn_ring_len", C.c_int),
                 ("syn_components", C.c_int),
-                ("spectral_radius_before_rescale", C.c_double)]
+                ("spectral_radius_before_rescale", C.c_double), ("topology_ms", C.c_double),
+                ("spectral_ms", C.c_double)]
 
 
 class Launch(C.Structure):

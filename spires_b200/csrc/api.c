@@ -354,6 +354,8 @@ static void fill_info(const sp_host_model *m, spires_ext_model_info *info)
     info->syn_ring_len = m->sc.frac_L;
     info->syn_components = m->sc.mexp_N;
     info->spectral_radius_before_rescale = m->spectral_radius_before;
+    info->topology_ms = m->topology_ms;
+    info->spectral_ms = m->spectral_ms;
 }
 
 SPIRES_EXPORT spires_status spires_ext_model_info_get(const spires_ext_model *h,

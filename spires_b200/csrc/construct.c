@@ -26,6 +26,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include "sp_model.h"
 
 /* (int)x as x86-64's truncating conversion performs it -- NaN and values
@@ -1173,6 +1174,13 @@ int sp_model_build_synapse(sp_host_model *m, const double *unused)
 
 /* ------------------------------------------------------------- top level -- */
 
+static double wall_ms(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return 1e3 * (double)t.tv_sec + 1e-6 * (double)t.tv_nsec;
+}
+
 int sp_model_build(sp_host_model *m)
 {
     int rc;
@@ -1193,6 +1201,7 @@ int sp_model_build(sp_host_model *m)
     for (size_t k = 0; k < n * m->din; k++)
         m->W_in[k] = draw_weight(m->ei_ratio);
 
+    const double t_topo = wall_ms();
     switch (m->conn_type) {
     case SP_CONN_RANDOM:
         rc = topo_random(m);
@@ -1206,6 +1215,7 @@ int sp_model_build(sp_host_model *m)
     default:
         rc = SP_EINVAL;
     }
+    m->topology_ms = wall_ms() - t_topo;
     if (rc)
         return rc;
 
@@ -1215,6 +1225,7 @@ int sp_model_build(sp_host_model *m)
 
     /* rescale_weights, src/reservoir.c:548-557 */
     /* large matrices: the device runs the same iteration bit for bit */
+    const double t_sr = wall_ms();
     double sr = 0.0;
     const char *host_env = getenv("SPIRES_HOST_SPECTRAL_RADIUS");
     if (m->host_only || m->nnz < SP_DEVICE_SR_MIN_NNZ || (host_env && host_env[0] == '1') ||
@@ -1226,6 +1237,7 @@ int sp_model_build(sp_host_model *m)
         for (size_t k = 0; k < m->nnz; k++)
             m->w[k] = f * m->w[k];
     }
+    m->spectral_ms = wall_ms() - t_sr;
 
     /* randomize_output_layer, src/reservoir.c:559-571 */
     for (size_t k = 0; k < n * m->dout; k++)

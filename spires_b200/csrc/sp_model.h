@@ -89,6 +89,8 @@ typedef struct sp_host_model {
 
     /* diagnostics from construction */
     double spectral_radius_before;  /* power-iteration estimate before rescale */
+    double topology_ms;             /* host time drawing the recurrent graph */
+    double spectral_ms;             /* host time of the spectral-radius rescale */
     uint64_t diffusive_seed;        /* FLIF_DIFFUSIVE per-reservoir seed */
 
     /* construction policy: 1 = never use the GPU (spires_ext_model_build) */

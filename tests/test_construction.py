@@ -142,3 +142,11 @@ def test_out_of_range_ring_length_rejected():
                          nparams=(1.0, 0.0, 0.0, 20.0, 0.7, float("nan"), 0.1, 2.0))
     m = sp.HostModel(cfg, seed=1)
     assert m.n == 10
+
+
+def test_model_info_reports_construction_times():
+    cfg = sp.make_config(1500, conn=0.05, topo=sp.CONN_SCALE_FREE)
+    m = sp.HostModel(cfg, seed=3, private=True)
+    assert m.info.topology_ms > 0.0
+    assert m.info.spectral_ms > 0.0
+    assert m.info.nnz > 0
