@@ -454,9 +454,12 @@ def run_search_workload(args):
         line[name] = {"best_nrmse": r.best_nrmse, "wall_s": r.wall_s,
                       "time_to_target_s": r.time_to(target), "evals": r.evals,
                       "neuron_steps": st.neuron_steps, "build_s": st.build_s,
+                      "construct_s": st.construct_s, "setup_s": st.setup_s,
                       "surrogate_rmse_logNRMSE": r.extra.get("surrogate_rmse"),
                       "low_fidelity_rmse_logNRMSE": r.extra.get("low_fidelity_rmse")}
     line["plain_neuron_steps"] = out["plain"][1].neuron_steps
+    line["plain_build_s"] = out["plain"][1].build_s
+    line["plain_construct_s"] = out["plain"][1].construct_s
     line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
                       "rungs": list(rungs), "points": points, "chains": chains, "waves": 8}
     line["data"] = "synthetic (seeded Mackey-Glass)"

@@ -120,6 +120,8 @@ class EvalStats:
     neuron_steps: float = 0.0
     sim_s: float = 0.0     # whole evaluate() calls
     build_s: float = 0.0   # reservoir construction (host topology + device upload)
+    construct_s: float = 0.0  # ... of which host construction (all host threads)
+    setup_s: float = 0.0      # ... of which device layouts and uploads
     fit_s: float = 0.0     # batched simulation + ridge fits + readouts
     calls: int = 0
 
@@ -165,6 +167,9 @@ class Evaluator:
             tb = time.perf_counter()
             batch = Batch([cfgs[k] for k in ch], [self.instance_seed(ids[k]) for k in ch])
             tf = time.perf_counter()
+            c_ms, s_ms = batch.timing()
+            self.stats.construct_s += c_ms / 1e3
+            self.stats.setup_s += s_ms / 1e3
             lams = [decs[k]["lam"] for k in ch]
             for out, T in zip(outs, rungs):
                 u, y = self.task.series(T)
