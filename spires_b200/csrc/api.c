@@ -886,46 +886,59 @@ SPIRES_EXPORT spires_status spires_ext_batch_timing(const spires_ext_batch *b, d
     return SPIRES_OK;
 }
 
-/* Replace the recurrent weights by a dense matrix (zeros are no edge), as the
- * reference's synapse_build_from_dense builds them (per-edge synapse draws
- * included), optionally rescaled to the configured spectral radius with the
- * construction's power iteration; the reservoir returns to its reset state. */
-SPIRES_EXPORT spires_status spires_ext_set_weights(spires_reservoir *r, const double *dense,
-                                                   int rescale)
+/* The arrays of a model that a change of recurrent weights rebuilds: freed
+ * (do_free) or just forgotten, when another copy of the model owns them. */
+static void drop_graph_arrays(sp_host_model *m, int do_free)
 {
-    if (!r || !r->dev || !dense)
-        return SPIRES_ERR_INVALID_ARG;
-    sp_host_model *m = &r->m;
-    void *old[] = {m->row_ptr, m->col, m->w, m->edge_decay, m->edge_omd, m->edge_tau,
-                   m->syn_coef, m->mexp_decay, m->mexp_omd, m->mexp_c, m->mexp_tau};
+    void *p[] = {m->row_ptr, m->col, m->w, m->edge_decay, m->edge_omd, m->edge_tau,
+                 m->syn_coef, m->mexp_decay, m->mexp_omd, m->mexp_c, m->mexp_tau};
+    if (do_free)
+        for (size_t k = 0; k < sizeof(p) / sizeof(p[0]); ++k)
+            free(p[k]);
     m->row_ptr = NULL;
     m->col = NULL;
     m->w = NULL;
     m->edge_decay = m->edge_omd = m->edge_tau = m->syn_coef = NULL;
     m->mexp_decay = m->mexp_omd = m->mexp_c = m->mexp_tau = NULL;
-    for (size_t k = 0; k < sizeof(old) / sizeof(old[0]); ++k)
-        free(old[k]);
-    int rc = sp_model_set_dense_weights(m, dense);
+}
+
+/* Replace the recurrent weights by a dense matrix (zeros are no edge), as the
+ * reference's synapse_build_from_dense builds them (per-edge synapse draws
+ * included), optionally rescaled to the configured spectral radius with the
+ * construction's power iteration; the reservoir returns to its reset state.
+ * The new graph is built beside the old one, which stays in place (host and
+ * device) if anything fails. */
+SPIRES_EXPORT spires_status spires_ext_set_weights(spires_reservoir *r, const double *dense,
+                                                   int rescale)
+{
+    if (!r || !r->dev || !dense)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_host_model t = r->m; /* shares the neuron-side arrays with r->m */
+    drop_graph_arrays(&t, 0);
+    int rc = sp_model_set_dense_weights(&t, dense);
     if (!rc && rescale) {
         double sr = 0.0;
-        if (m->nnz < ((size_t)1 << 15) ||
-            sp_dev_spectral_radius(m->n, m->row_ptr, m->col, m->w, &sr) != SP_OK)
-            sr = sp_csr_spectral_radius(m->n, m->row_ptr, m->col, m->w);
-        m->spectral_radius_before = sr;
+        if (t.nnz < ((size_t)1 << 15) ||
+            sp_dev_spectral_radius(t.n, t.row_ptr, t.col, t.w, &sr) != SP_OK)
+            sr = sp_csr_spectral_radius(t.n, t.row_ptr, t.col, t.w);
+        t.spectral_radius_before = sr;
         if (sr > 1e-9) {
-            const double f = m->spectral_radius / sr;
-            for (size_t k = 0; k < m->nnz; k++)
-                m->w[k] = f * m->w[k];
+            const double f = t.spectral_radius / sr;
+            for (size_t k = 0; k < t.nnz; k++)
+                t.w[k] = f * t.w[k];
         }
     }
     if (!rc)
-        rc = sp_model_derive_neuron(m);
-    if (rc)
-        return to_status(rc);
+        rc = sp_model_derive_neuron(&t);
     sp_dev *nd = NULL;
-    rc = sp_dev_create(m, &nd);
-    if (rc)
+    if (!rc)
+        rc = sp_dev_create(&t, &nd);
+    if (rc) {
+        drop_graph_arrays(&t, 1);
         return to_status(rc);
+    }
+    drop_graph_arrays(&r->m, 1);
+    r->m = t;
     sp_dev_destroy(r->dev);
     r->dev = nd;
     return SPIRES_OK;
