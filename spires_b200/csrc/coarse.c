@@ -23,6 +23,11 @@ SPIRES_EXPORT spires_status spires_coarse_grain(const spires_reservoir *r, doubl
 {
     if (!r || !r->dev || !out_r)
         return SPIRES_ERR_INVALID_ARG;
+    /* Below zero (or NaN) every pass merges again -- the zeroed rows of merged
+     * neurons pass the test -- and the reference's loop never ends; refuse
+     * such thresholds instead. */
+    if (!(weight_threshold >= 0.0))
+        return SPIRES_ERR_INVALID_ARG;
     const sp_host_model *m = &r->m;
     const size_t n = m->n, nin = m->din, nout = m->dout;
     spires_status st = SPIRES_ERR_ALLOC;

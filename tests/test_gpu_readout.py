@@ -207,6 +207,10 @@ def test_coarse_grain_matches_restatement():
     for t in range(5):
         r.lib.spires_step(h, sp.dptr(np.ascontiguousarray(u[t])))
     r.lib.spires_reservoir_destroy(h)
+    # thresholds below zero (or NaN) would merge forever: refused
+    h2 = C.c_void_p()
+    for thr in (-0.5, float("nan")):
+        assert r.lib.spires_coarse_grain(r.h, thr, C.byref(h2)) == sp.SPIRES_ERR_INVALID_ARG
     r.close()
 
 
