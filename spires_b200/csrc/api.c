@@ -840,7 +840,7 @@ SPIRES_EXPORT spires_status spires_ext_ridge_fit(const double *states, size_t T,
                                                  double *w_out, spires_ext_ridge_report *report)
 {
     if (!states || !targets || !w_out || n == 0 || n > (size_t)INT32_MAX || dout == 0 ||
-        dout > 16)
+        dout > (size_t)INT32_MAX)
         return SPIRES_ERR_INVALID_ARG;
     sp_ridge_opts o;
     memset(&o, 0, sizeof(o));

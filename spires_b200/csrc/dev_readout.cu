@@ -893,13 +893,11 @@ out:
     return rc;
 }
 
-// Ridge on states already on the device: Phi [T x n] row-major (neuron order),
-// Y [T x dout]; rows [washout, T) enter the Gram. On success d_W_out [dout x n]
-// holds the solution; SP_RIDGE_SINGULAR leaves it untouched (dgesv failure in
-// the reference leaves W_out as it was). Work buffers are allocated per call.
-extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
-                            const double *Y, int dout, double lambda, const sp_ridge_opts *o,
-                            sp_ridge_report *rep, double *d_W_out)
+// One group of at most 16 outputs of sp_ridge_phi (below). Work buffers are
+// allocated per call.
+static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
+                           const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                           sp_ridge_report *rep, double *d_W_out)
 {
     int rc = SP_OK;
     double *A = nullptr, *Aw = nullptr, *B = nullptr, *W = nullptr, *R = nullptr, *E = nullptr,
@@ -1049,6 +1047,59 @@ out:
     return rc;
 }
 
+// Ridge on states already on the device: Phi [T x n] row-major (neuron order),
+// Y [T x dout]; rows [washout, T) enter the Gram. On success d_W_out [dout x n]
+// holds the solution; SP_RIDGE_SINGULAR leaves it untouched (dgesv failure in
+// the reference leaves W_out as it was). The solver's per-thread accumulators
+// hold 16 outputs; with more, the outputs are solved 16 at a time -- the system
+// matrix is the same for all of them -- each group's targets copied to a
+// contiguous block and its rows of W gathered in a work array that reaches
+// d_W_out only when every group has succeeded.
+extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
+                            const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                            sp_ridge_report *rep, double *d_W_out)
+{
+    if (dout <= 16)
+        return ridge_phi_group(s, Phi, n, T, Y, dout, lambda, o, rep, d_W_out);
+    int rc = SP_OK;
+    double *Yg = nullptr, *Wall = nullptr;
+    sp_ridge_report sum;
+    memset(&sum, 0, sizeof(sum));
+    RK(cudaMalloc(&Yg, (T ? T : 1) * 16 * sizeof(double)));
+    RK(cudaMalloc(&Wall, (size_t)dout * n * sizeof(double)));
+    for (int g0 = 0; g0 < dout && !rc; g0 += 16) {
+        const int dg = dout - g0 < 16 ? dout - g0 : 16;
+        if (T)
+            RK(cudaMemcpy2DAsync(Yg, (size_t)dg * sizeof(double), Y + g0,
+                                 (size_t)dout * sizeof(double), (size_t)dg * sizeof(double), T,
+                                 cudaMemcpyDeviceToDevice, s));
+        sp_ridge_report r1;
+        memset(&r1, 0, sizeof(r1));
+        rc = ridge_phi_group(s, Phi, n, T, Yg, dg, lambda, o, &r1, Wall + (size_t)g0 * n);
+        sum.gram_mode_used = r1.gram_mode_used;
+        sum.dual = r1.dual;
+        sum.refine_iters = r1.refine_iters > sum.refine_iters ? r1.refine_iters : sum.refine_iters;
+        sum.rel_residual = r1.rel_residual > sum.rel_residual ? r1.rel_residual : sum.rel_residual;
+        sum.gram_ms += r1.gram_ms;
+        sum.factor_ms += r1.factor_ms;
+        sum.refine_ms += r1.refine_ms;
+        sum.factor_failed |= r1.factor_failed;
+        sum.lu_fallback |= r1.lu_fallback;
+    }
+    if (!rc)
+        RK(cudaMemcpyAsync(d_W_out, Wall, (size_t)dout * n * sizeof(double),
+                           cudaMemcpyDeviceToDevice, s));
+out:
+    cudaStreamSynchronize(s);
+    if (Yg)
+        cudaFree(Yg);
+    if (Wall)
+        cudaFree(Wall);
+    sum.collect_ms = rep->collect_ms;
+    *rep = sum;
+    return rc;
+}
+
 // Ridge on caller-provided states (host arrays): Phi [T x n], Y [T x dout];
 // writes W_out [dout x n] to the host. Same solver (and dual/split choices) as
 // the reservoir readouts, on the current device and a stream of its own.
@@ -1060,7 +1111,7 @@ extern "C" int sp_ridge_host(const double *h_phi, size_t T, int n, const double 
     cudaStream_t s = nullptr;
     double *Phi = nullptr, *Y = nullptr, *Wt = nullptr;
     memset(rep, 0, sizeof(*rep));
-    if (dout <= 0 || dout > 16 || n <= 0 || T == 0 || o->washout >= T)
+    if (dout <= 0 || n <= 0 || T == 0 || o->washout >= T)
         return SP_EINVAL;
     auto t0 = std::chrono::steady_clock::now();
     RK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -1099,8 +1150,6 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
     memset(rep, 0, sizeof(*rep));
     if (dout == 0)
         return SP_OK;
-    if (dout > 16)
-        return SP_EINVAL;
     auto tstart = std::chrono::steady_clock::now();
 
     rc = sp_dev_reset_neurons(d, m);
