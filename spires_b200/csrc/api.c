@@ -574,6 +574,40 @@ static double now_ms(void)
     return 1e3 * (double)t.tv_sec + 1e-6 * (double)t.tv_nsec;
 }
 
+/* Rough host time of one build, only to order the builds of a batch: per
+ * pair drawn (Erdos-Renyi), per ring edge (small-world), per roulette pick
+ * (scale-free), plus the host power iteration of graphs small enough to keep
+ * it on the host (1000 sweeps of their edges). */
+typedef struct {
+    double cost;
+    size_t index;
+} build_job;
+
+static double build_cost(const spires_reservoir_config *c)
+{
+    const double n = (double)c->num_neurons;
+    const double conn = c->connectivity > 0.0 ? (c->connectivity < 1.0 ? c->connectivity : 1.0)
+                                              : 0.0;
+    const double deg = conn * (n > 1.0 ? n - 1.0 : 0.0) + 1.0, edges = n * deg;
+    double t;
+    switch ((int)c->connectivity_type) {
+    case SP_CONN_RANDOM: t = 6e-9 * n * n + 2e-8 * edges; break;
+    case SP_CONN_SMALL_WORLD: t = 4e-8 * edges; break;
+    default: t = 1.2e-7 * edges; break;
+    }
+    if (edges < 32768.0)
+        t += 6e-7 * edges;
+    return t;
+}
+
+static int cmp_build_job(const void *a, const void *b)
+{
+    const build_job *x = a, *y = b;
+    if (x->cost != y->cost)
+        return x->cost > y->cost ? -1 : 1;
+    return (x->index > y->index) - (x->index < y->index);
+}
+
 SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_config *cfgs,
                                                     const unsigned *seeds, size_t count,
                                                     spires_ext_batch **out)
@@ -591,16 +625,27 @@ SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_confi
     int rc = SP_OK;
     const double t0 = now_ms();
     if (seeds) {
-        /* independent private generators: instances build on all host threads */
+        /* Independent private generators: instances build on all host threads,
+         * the costliest first so that no large build starts last (the order
+         * changes no instance: each draws from its own generator). */
         const int dev = sp_dev_current_device();
         int *rcs = calloc(count, sizeof(int));
-        if (!rcs) {
+        build_job *jobs = malloc(count * sizeof(build_job));
+        if (!rcs || !jobs) {
+            free(rcs);
+            free(jobs);
             free(ms);
             free(h);
             return SPIRES_ERR_ALLOC;
         }
-#pragma omp parallel for schedule(dynamic, 1)
         for (size_t k = 0; k < count; ++k) {
+            jobs[k].cost = build_cost(&cfgs[k]);
+            jobs[k].index = k;
+        }
+        qsort(jobs, count, sizeof(build_job), cmp_build_job);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t q = 0; q < count; ++q) {
+            const size_t k = jobs[q].index;
             sp_dev_use_device(dev);
             int r = model_from_config(&cfgs[k], &ms[k]);
             if (!r)
@@ -610,6 +655,7 @@ SPIRES_EXPORT spires_status spires_ext_batch_create(const spires_reservoir_confi
         for (size_t k = 0; k < count && !rc; ++k)
             rc = rcs[k];
         free(rcs);
+        free(jobs);
     } else {
         /* one global rand() sequence, as count consecutive creates */
         for (size_t k = 0; k < count && !rc; ++k) {
