@@ -65,7 +65,9 @@ static int model_from_config(const spires_reservoir_config *cfg, sp_host_model *
     m->conn_type = (int)cfg->connectivity_type;
     m->neuron_type = (int)cfg->neuron_type;
     m->syn_type = (int)cfg->synapse_type;
-    m->syn_backend = (int)cfg->synapse_backend;
+    /* the reference builds sparse storage for SPARSE and dense for any other
+     * value (synapse_build_from_dense, src/synapse.c:13-38) */
+    m->syn_backend = cfg->synapse_backend == SPIRES_SYNAPSE_SPARSE ? 0 : 1;
     m->neuron_params = cfg->neuron_params;
     m->synapse_params = cfg->synapse_params;
     return SP_OK;

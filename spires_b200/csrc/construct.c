@@ -867,15 +867,16 @@ int sp_validate_config(size_t n, size_t din, size_t dout, double dt, int conn_ty
 {
     (void)din;
     (void)dout;
+    /* any topology and backend value is accepted, as in the reference: an
+     * unknown topology draws no recurrent edges, and every backend other than
+     * SPARSE stores dense */
+    (void)conn_type;
+    (void)syn_backend;
     if (n == 0 || n > (size_t)INT32_MAX)
-        return SP_EINVAL;
-    if (conn_type < SP_CONN_RANDOM || conn_type > SP_CONN_SCALE_FREE)
         return SP_EINVAL;
     if (neuron_type < SP_LIF_DISCRETE || neuron_type > SP_FLIF_DIFFUSIVE)
         return SP_EINVAL;
     if (syn_type < SP_SYN_SIMPLE || syn_type > SP_SYN_FRAC_MEXP)
-        return SP_EINVAL;
-    if (syn_backend != 0 && syn_backend != 1)
         return SP_EINVAL;
     if (!neuron_params)
         return SP_EINVAL;
@@ -1212,8 +1213,8 @@ int sp_model_build(sp_host_model *m)
     case SP_CONN_SCALE_FREE:
         rc = topo_scale_free(m);
         break;
-    default:
-        rc = SP_EINVAL;
+    default: /* the reference's switch has no default: no recurrent edges */
+        rc = csr_empty(m);
     }
     m->topology_ms = wall_ms() - t_topo;
     if (rc)

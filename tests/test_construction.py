@@ -72,7 +72,7 @@ def test_invalid_configs_rejected():
     lib = sp.load()
     import ctypes as C
     h = C.c_void_p()
-    for kw in [dict(dt=0.0), dict(dt=0.3), dict(dt=1.5), dict(neuron=9), dict(topo=5)]:
+    for kw in [dict(dt=0.0), dict(dt=0.3), dict(dt=1.5), dict(neuron=9), dict(synapse=9)]:
         cfg = sp.make_config(10, **kw)
         assert lib.spires_ext_model_build(C.byref(cfg), C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
     assert lib.spires_reservoir_create(None, C.byref(h)) == sp.SPIRES_ERR_INVALID_ARG
@@ -150,3 +150,22 @@ def test_model_info_reports_construction_times():
     assert m.info.topology_ms > 0.0
     assert m.info.spectral_ms > 0.0
     assert m.info.nnz > 0
+
+
+@pytest.mark.skipif(not _oracle.have_ref(), reason="reference build absent")
+@pytest.mark.parametrize("topo,backend,syn", [(5, 0, sp.SYN_SIMPLE), (sp.CONN_RANDOM, 7, sp.SYN_SIMPLE),
+                                              (sp.CONN_SMALL_WORLD, 3, sp.SYN_PSC_HET)])
+def test_unlisted_topology_and_backend_values_as_the_reference(topo, backend, syn):
+    """The reference accepts any topology value (no recurrent edges for one it
+    does not list) and stores dense for any backend but SPARSE; same weights
+    and the same draw count here."""
+    sparams = (1.0, 20.0) if syn == sp.SYN_PSC_HET else None
+    cfg = sp.make_config(90, 2, 2, rho=0.9, ei=0.6, conn=0.1, topo=topo, neuron=sp.FLIF_GL,
+                         nparams=GL, synapse=syn, backend=backend, sparams=sparams)
+    mine = sp.HostModel(cfg, seed=4)
+    ref = sp.Reservoir(cfg, lib=_oracle.ref_lib(), seed=4)
+    assert np.array_equal(ref.weights(), mine.dense())
+    assert np.array_equal(ref.readout(), mine.w_out())
+    ref.close()
+    if topo == 5:
+        assert mine.info.nnz == 0
