@@ -169,3 +169,34 @@ def test_unlisted_topology_and_backend_values_as_the_reference(topo, backend, sy
     ref.close()
     if topo == 5:
         assert mine.info.nnz == 0
+
+
+@pytest.mark.skipif(not _oracle.have_ref(), reason="reference build absent")
+def test_randomised_configurations_match_reference():
+    """Randomised sizes, densities, sign ratios (including beyond [0, 1]),
+    spectral radii, topologies, synapse types and backends: the same W, W_out
+    and draw count as the reference's create."""
+    rng = np.random.default_rng(2025)
+    syn_params = {sp.SYN_SIMPLE: None, sp.SYN_PSC_HOM: (3.0,), sp.SYN_PSC_HET: (1.0, 20.0),
+                  sp.SYN_FRAC: (0.6, 2.0, 8.0), sp.SYN_FRAC_MEXP: (0.5, 5.0, 1.0, 50.0, 4)}
+    for trial in range(30):
+        n = int(rng.integers(2, 120))
+        syn = int(rng.integers(0, 5))
+        cfg = sp.make_config(n, int(rng.integers(1, 4)), int(rng.integers(1, 4)),
+                             rho=float(rng.choice([0.0, 0.5, 1.3, -0.7])),
+                             ei=float(rng.choice([0.0, 0.25, 0.5, 1.0, 1.5, -0.2])),
+                             gamma=0.5, conn=float(rng.choice([0.0, 0.01, 0.1, 0.5, 1.0, 2.0])),
+                             topo=int(rng.integers(0, 3)), neuron=sp.FLIF_GL, nparams=GL,
+                             synapse=syn, backend=int(rng.integers(0, 2)),
+                             sparams=syn_params[syn])
+        seed = int(rng.integers(1, 2**31 - 1))
+        mine = sp.HostModel(cfg, seed=seed)
+        after_mine = sp.libc.rand()
+        ref = sp.Reservoir(cfg, lib=_oracle.ref_lib(), seed=seed)
+        after_ref = sp.libc.rand()
+        Wr = ref.weights()
+        Wo = ref.readout()
+        ref.close()
+        assert np.array_equal(Wr, mine.dense()), trial
+        assert np.array_equal(Wo, mine.w_out()), trial
+        assert after_mine == after_ref, trial  # the same number of draws
