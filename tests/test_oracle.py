@@ -71,3 +71,28 @@ def test_oracle_readout_and_reset():
     _, _, Yo2 = orc.run(u, y=True)
     assert np.array_equal(Yr, Yo)
     assert np.array_equal(Yr2, Yo2)
+
+
+def test_oracle_matches_reference_randomised():
+    """Randomised neuron x synapse x micro-stepping x topology x backend,
+    with the fractional order and memory of FLIF_GL, the leak of LIF_DISCRETE
+    and the input gain drawn too: the checker itself pinned beyond the grid."""
+    rng = np.random.default_rng(77)
+    for trial in range(12):
+        neuron = NEURONS[int(rng.integers(0, len(NEURONS)))]
+        synapse = SYNAPSES[int(rng.integers(0, len(SYNAPSES)))]
+        params = list(O.NEURON_PARAMS[neuron])
+        if neuron == sp.FLIF_GL:
+            params[4] = float(rng.uniform(0.3, 1.0))
+            params[5] = float(rng.choice([8.0, 33.0, 64.0]))
+        if neuron == sp.LIF_DISCRETE:
+            params[2] = float(rng.uniform(0.05, 0.6))
+        topo = int(rng.integers(0, 3))
+        n = int(rng.integers(20, 100))
+        cfg = sp.make_config(n, int(rng.integers(1, 3)), 2, rho=float(rng.uniform(0.6, 1.6)),
+                             ei=float(rng.uniform(0.3, 0.8)), gamma=float(rng.uniform(0.3, 2.0)),
+                             conn=(0.1 if topo == sp.CONN_RANDOM else 4.0 / (n - 1)),
+                             dt=float(rng.choice([1.0, 0.5])), topo=topo, neuron=neuron,
+                             nparams=tuple(params), synapse=synapse,
+                             backend=int(rng.integers(0, 2)), sparams=O.SYNAPSE_PARAMS[synapse])
+        check(cfg, seed=int(rng.integers(1, 10**6)), T=40)
