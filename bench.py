@@ -684,7 +684,11 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            run_reference_arm(args)
+            try:
+                run_reference_arm(args)
+            except Exception as exc:  # a missing build must not end the run with a traceback
+                print(json.dumps({"impl": "reference",
+                                  "unavailable": f"{type(exc).__name__}: {exc}"[:300]}))
         return
     if args.profile_case:
         run_profile_case(args)
