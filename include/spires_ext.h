@@ -150,7 +150,8 @@ spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_se
  * row-major, targets [T x dout], rows [washout, T) fitted; w_out [dout x n].
  * The reservoir readouts' solver, including the dual form when fewer than
  * n/2 rows are fitted (the classification workload's 500 time-averaged
- * states against 20000 neurons) and the split-Gram modes. A singular system
+ * states against 20000 neurons) and the split-Gram modes; any number of
+ * outputs (solved 16 at a time over one system matrix). A singular system
  * returns SPIRES_ERR_INTERNAL. */
 spires_status spires_ext_ridge_fit(const double *states, size_t T, size_t n,
                                    const double *targets, size_t dout, double lambda,
