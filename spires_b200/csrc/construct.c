@@ -345,8 +345,8 @@ static int topo_small_world(sp_host_model *m)
     double *row = calloc(n, sizeof(double));
     int32_t *added = malloc(((size_t)half + 1) * sizeof(int32_t));
     m->row_ptr = calloc(n + 1, sizeof(int64_t));
-    m->col = malloc((cap ? cap : 1) * sizeof(int32_t));
-    m->w = malloc((cap ? cap : 1) * sizeof(double));
+    m->col = malloc((cap + 1) * sizeof(int32_t)); /* + 1: see the merge below */
+    m->w = malloc((cap + 1) * sizeof(double));
     if (!ring || !row || !added || !m->row_ptr || !m->col || !m->w) {
         free(ring);
         free(row);
@@ -382,42 +382,41 @@ static int topo_small_world(sp_host_model *m)
             }
         }
         sort_i32_small(added, na);
-        /* ring runs: [lo_a, hi_a] above i, [0, hi_b] after the wrap (if any) */
+        /* The ring runs in ascending order -- [0, top - n] after the wrap (if
+         * any), then [i + 1, min(top, n - 1)] -- with the sorted rewired
+         * targets merged in. Every column is written and kept (e advanced)
+         * only when its weight is nonzero and it is not a repeat; the one
+         * spare slot of the arrays absorbs a last write that is not kept. */
         const size_t top = i + (size_t)half;
-        const size_t hi_a = top < n ? top : n - 1;
-        const long long hi_b = top < n ? -1 : (long long)(top - n);
-        long long rb = 0;     /* next of the wrapped run */
-        size_t ra = i + 1;    /* next of the run above i */
-        int k = 0;            /* next rewired target */
-        int64_t last = -1;
-        for (;;) {
-            /* the smallest pending column of the three lists */
-            int64_t c;
-            if (rb <= hi_b)
-                c = rb;
-            else if (ra <= hi_a)
-                c = (int64_t)ra;
-            else
-                c = INT64_MAX;
-            if (k < na && added[k] < c)
-                c = added[k];
-            if (c == INT64_MAX)
-                break;
-            if (rb <= hi_b && c == rb)
-                rb++;
-            else if (ra <= hi_a && c == (int64_t)ra)
-                ra++;
-            if (k < na && added[k] == c)
-                k++;
-            if (c == last)
-                continue;
-            last = c;
-            const double v = row[c];
-            if (v != 0.0) {
-                m->col[e] = (int32_t)c;
-                m->w[e] = v;
-                e++;
+        const int64_t runs[2][2] = {{0, top < n ? -1 : (int64_t)(top - n)},
+                                    {(int64_t)i + 1, (int64_t)(top < n ? top : n - 1)}};
+        int k = 0;         /* next rewired target */
+        int64_t last = -1; /* last column looked at */
+        int32_t *col = m->col;
+        double *w = m->w;
+        for (int rr = 0; rr < 2; rr++)
+            for (int64_t c = runs[rr][0]; c <= runs[rr][1]; c++) {
+                for (; k < na && added[k] < c; k++) {
+                    const int64_t a = added[k];
+                    const double v = row[a];
+                    col[e] = (int32_t)a;
+                    w[e] = v;
+                    e += (size_t)((v != 0.0) & (a != last));
+                    last = a;
+                }
+                const double v = row[c];
+                col[e] = (int32_t)c;
+                w[e] = v;
+                e += (size_t)((v != 0.0) & (c != last));
+                last = c;
             }
+        for (; k < na; k++) {
+            const int64_t a = added[k];
+            const double v = row[a];
+            col[e] = (int32_t)a;
+            w[e] = v;
+            e += (size_t)((v != 0.0) & (a != last));
+            last = a;
         }
         for (int s = 1; s <= half; s++)
             row[(i + (size_t)s) % n] = 0.0;
