@@ -512,13 +512,32 @@ def run_construct_workload(args):
         del m
     wall = time.perf_counter() - t0
     topo_s = sum(v["topology_s"] for v in per.values())
+    vs_ref = None
+    if args.construct_reference:
+        # the baseline leg: whole builds (graph, power iteration, W_in, W_out)
+        # by the reference's spires_reservoir_create and by this library's host
+        # build, N = 4000, connectivity 0.1, each topology
+        from tests import _oracle as O
+
+        ref = O.ref_lib()
+        vs_ref = {}
+        for topo in (sp.CONN_RANDOM, sp.CONN_SMALL_WORLD, sp.CONN_SCALE_FREE):
+            cfg = sp.make_config(4000, 1, 1, rho=0.9, ei=0.5, conn=0.1, topo=topo,
+                                 neuron=sp.LIF_DISCRETE, nparams=(0.0, 1.0, 0.9, 0.0))
+            ta = time.perf_counter()
+            r = sp.Reservoir(cfg, lib=ref, seed=3)
+            tb = time.perf_counter()
+            r.close()
+            sp.HostModel(cfg, seed=3, private=True)
+            tc = time.perf_counter()
+            vs_ref[names[topo]] = {"reference_create_s": tb - ta, "host_build_s": tc - tb}
     print(json.dumps({
         "metric": "host graph construction time", "value": topo_s, "unit": "s",
         "higher_is_better": False, "workload": "construct", "graph_threads": 1,
         "spectral_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
         "data": "synthetic", "count": args.construct_count,
         "spectral_s": sum(v["spectral_s"] for v in per.values()), "wall_s": wall,
-        "per_topology": per,
+        "per_topology": per, "vs_reference": vs_ref,
         "note": "graph drawing (value, one thread) and host power iteration (OpenMP "
                 "threads above 65536 edges) timed by the library; the batch and reservoir "
                 "builds run the power iteration of large graphs on the GPU"}))
@@ -666,6 +685,8 @@ def main():
                     help="step (default, the headline line) or an additional workload")
     ap.add_argument("--sweep-count", type=int, default=256)
     ap.add_argument("--construct-count", type=int, default=300)
+    ap.add_argument("--construct-reference", action="store_true",
+                    help="also time whole N=4000 builds against the reference's create")
     ap.add_argument("--sweep-tmax", type=int, default=10000,
                     help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
