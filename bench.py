@@ -537,7 +537,10 @@ def run_construct_workload(args):
         "spectral_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
         "data": "synthetic", "count": args.construct_count,
         "spectral_s": sum(v["spectral_s"] for v in per.values()), "wall_s": wall,
-        "per_topology": per, "vs_reference": vs_ref,
+        "per_topology": per,
+        "cpu_baseline": None if vs_ref is None else {
+            "kind": "reference", "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+            "sample": "whole builds, N=4000, connectivity 0.1, one per topology", "builds": vs_ref},
         "note": "graph drawing (value, one thread) and host power iteration (OpenMP "
                 "threads above 65536 edges) timed by the library; the batch and reservoir "
                 "builds run the power iteration of large graphs on the GPU"}))
