@@ -96,6 +96,20 @@ spires_status spires_ext_autotune(spires_reservoir *r, size_t steps);
  * stream derived from seed and i). Takes effect at the next reset. */
 spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed);
 
+/* ---- state checkpoint -------------------------------------------------------
+ * Everything a run continues from: membrane potentials, refractory clocks,
+ * the FLIF_GL history ring or Caputo registers, the FLIF_DIFFUSIVE sampler
+ * states, the latest spike words, synaptic drive and traces, the fractional
+ * synapse history, the step counters -- and the readout W_out. Saving waits
+ * for the steps already queued. A buffer loads only into a reservoir of the
+ * same sizes and models (SPIRES_ERR_INVALID_ARG otherwise); one built from
+ * the same configuration and seed then continues bit for bit as the saved
+ * one would have. The weights W and W_in are not part of it. No counterpart
+ * in the reference, which has no state setter. */
+size_t        spires_ext_state_bytes(spires_reservoir *r);
+spires_status spires_ext_state_save(spires_reservoir *r, void *buf);
+spires_status spires_ext_state_load(spires_reservoir *r, const void *buf);
+
 /* ---- recurrent weights from a dense matrix ----------------------------------
  * Replaces W by dense[N x N] (row-major, zero = no edge) the way the
  * reference's synapse_build_from_dense builds a synapse matrix (per-edge

@@ -517,6 +517,41 @@ SPIRES_EXPORT spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t se
     return to_status(sp_dev_set_seed(r->dev, seed));
 }
 
+/* state checkpoint: the device state (sp_dev_state_*), then W_out [dout x n] */
+SPIRES_EXPORT size_t spires_ext_state_bytes(spires_reservoir *r)
+{
+    if (!r || !r->dev)
+        return 0;
+    return sp_dev_state_bytes(r->dev) + r->m.dout * r->m.n * sizeof(double);
+}
+
+SPIRES_EXPORT spires_status spires_ext_state_save(spires_reservoir *r, void *buf)
+{
+    if (!r || !r->dev || !buf)
+        return SPIRES_ERR_INVALID_ARG;
+    int rc = sp_dev_state_save(r->dev, buf);
+    if (rc)
+        return to_status(rc);
+    memcpy((char *)buf + sp_dev_state_bytes(r->dev), r->m.W_out,
+           r->m.dout * r->m.n * sizeof(double));
+    return SPIRES_OK;
+}
+
+SPIRES_EXPORT spires_status spires_ext_state_load(spires_reservoir *r, const void *buf)
+{
+    if (!r || !r->dev || !buf)
+        return SPIRES_ERR_INVALID_ARG;
+    int rc = sp_dev_state_load(r->dev, buf);
+    if (rc)
+        return to_status(rc);
+    const size_t wb = r->m.dout * r->m.n * sizeof(double);
+    if (wb) {
+        memcpy(r->m.W_out, (const char *)buf + sp_dev_state_bytes(r->dev), wb);
+        rc = sp_dev_upload_w_out(r->dev, r->m.W_out);
+    }
+    return to_status(rc);
+}
+
 SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
                                                    const double *input_series,
                                                    const double *target_series,

@@ -959,26 +959,32 @@ struct sp_snap_item {
     void *save;
 };
 
+// Every mutable buffer of the dynamics (the step counters are kept apart):
+// what the autotuner restores after each candidate and what a state
+// checkpoint holds.
+static void state_items(sp_dev *d, std::vector<sp_snap_item> &items)
+{
+    const size_t rs = (size_t)d->rs;
+    items = {
+        {d->V, rs * 8, nullptr},
+        {d->tprev, rs * 8, nullptr},
+        {d->ring, d->ring ? d->ring_elems * 8 : 0, nullptr},
+        {d->cap_pos, d->cap_pos ? rs * 4 : 0, nullptr},
+        {d->refr_until, d->refr_until ? rs * 8 : 0, nullptr},
+        {d->rng, d->rng ? rs * 8 : 0, nullptr},
+        {d->spk, 2 * d->nwords * 4, nullptr},
+        {d->eff, d->eff ? 2 * rs * 8 : 0, nullptr},
+        {d->trace, d->trace ? rs * 8 : 0, nullptr},
+        {d->edge_trace, d->edge_trace ? d->nnz * 8 : 0, nullptr},
+        {d->Iring, d->Iring ? rs * (size_t)d->sc.frac_L * 8 : 0, nullptr},
+        {d->mx_tr, d->mx_tr ? rs * (size_t)d->sc.mexp_N * 8 : 0, nullptr},
+    };
+}
+
 static int snapshot(sp_dev *d, std::vector<sp_snap_item> &items, bool take)
 {
     if (take) {
-        const size_t rs = (size_t)d->rs;
-        const size_t L = (size_t)(d->nc.L > 0 ? d->nc.L : 0);
-        items = {
-            {d->V, rs * 8, nullptr},
-            {d->tprev, rs * 8, nullptr},
-            {d->ring, d->ring ? d->ring_elems * 8 : 0, nullptr},
-            {d->cap_pos, d->cap_pos ? rs * 4 : 0, nullptr},
-            {d->refr_until, d->refr_until ? rs * 8 : 0, nullptr},
-            {d->rng, d->rng ? rs * 8 : 0, nullptr},
-            {d->spk, 2 * d->nwords * 4, nullptr},
-            {d->eff, d->eff ? 2 * rs * 8 : 0, nullptr},
-            {d->trace, d->trace ? rs * 8 : 0, nullptr},
-            {d->edge_trace, d->edge_trace ? d->nnz * 8 : 0, nullptr},
-            {d->Iring, d->Iring ? rs * (size_t)d->sc.frac_L * 8 : 0, nullptr},
-            {d->mx_tr, d->mx_tr ? rs * (size_t)d->sc.mexp_N * 8 : 0, nullptr},
-        };
-        (void)L;
+        state_items(d, items);
         for (auto &it : items) {
             if (!it.ptr || !it.bytes)
                 continue;
@@ -1081,5 +1087,89 @@ extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
     }
     if (sp_dev_set_launch(d, &best) != SP_OK)
         d->launch = keep;
+    return SP_OK;
+}
+
+// ------------------------------------------------------ state checkpoint --
+// A header (the sizes the buffers depend on, then the step counters) followed
+// by the state_items buffers in order. Loading checks the sizes against this
+// reservoir, so a checkpoint only goes back into a reservoir of the same
+// configuration.
+
+struct sp_state_header {
+    char magic[8];
+    long long n, rs, ntype, stype, ring_elems, nwords, nnz, frac_L, mexp_N;
+    long long step, syn_step, phase;
+};
+
+static void fill_header(const sp_dev *d, sp_state_header *h)
+{
+    memset(h, 0, sizeof(*h));
+    memcpy(h->magic, "SPSTATE1", 8);
+    h->n = d->n;
+    h->rs = d->rs;
+    h->ntype = d->ntype;
+    h->stype = d->stype;
+    h->ring_elems = (long long)d->ring_elems;
+    h->nwords = (long long)d->nwords;
+    h->nnz = (long long)d->nnz;
+    h->frac_L = d->sc.frac_L;
+    h->mexp_N = d->sc.mexp_N;
+    h->step = d->step;
+    h->syn_step = d->syn_step;
+    h->phase = d->phase;
+}
+
+extern "C" size_t sp_dev_state_bytes(sp_dev *d)
+{
+    std::vector<sp_snap_item> items;
+    state_items(d, items);
+    size_t b = sizeof(sp_state_header);
+    for (const auto &it : items)
+        b += it.ptr ? it.bytes : 0;
+    return b;
+}
+
+extern "C" int sp_dev_state_save(sp_dev *d, void *buf)
+{
+    SP_CK(cudaStreamSynchronize(d->stream)); // steps still queued belong to the state
+    sp_state_header h;
+    fill_header(d, &h);
+    memcpy(buf, &h, sizeof(h));
+    char *p = (char *)buf + sizeof(h);
+    std::vector<sp_snap_item> items;
+    state_items(d, items);
+    for (const auto &it : items) {
+        if (!it.ptr || !it.bytes)
+            continue;
+        SP_CK(cudaMemcpy(p, it.ptr, it.bytes, cudaMemcpyDeviceToHost));
+        p += it.bytes;
+    }
+    return SP_OK;
+}
+
+extern "C" int sp_dev_state_load(sp_dev *d, const void *buf)
+{
+    sp_state_header h, mine;
+    memcpy(&h, buf, sizeof(h));
+    fill_header(d, &mine);
+    if (memcmp(h.magic, mine.magic, 8) != 0 || h.n != mine.n || h.rs != mine.rs ||
+        h.ntype != mine.ntype || h.stype != mine.stype || h.ring_elems != mine.ring_elems ||
+        h.nwords != mine.nwords || h.nnz != mine.nnz || h.frac_L != mine.frac_L ||
+        h.mexp_N != mine.mexp_N || (h.phase != 0 && h.phase != 1))
+        return SP_EINVAL;
+    SP_CK(cudaStreamSynchronize(d->stream));
+    const char *p = (const char *)buf + sizeof(h);
+    std::vector<sp_snap_item> items;
+    state_items(d, items);
+    for (const auto &it : items) {
+        if (!it.ptr || !it.bytes)
+            continue;
+        SP_CK(cudaMemcpy(it.ptr, p, it.bytes, cudaMemcpyHostToDevice));
+        p += it.bytes;
+    }
+    d->step = h.step;
+    d->syn_step = h.syn_step;
+    d->phase = (int)h.phase;
     return SP_OK;
 }

@@ -68,6 +68,11 @@ int  sp_dev_get_launch(sp_dev *d, sp_launch *l);
 int  sp_dev_set_launch(sp_dev *d, const sp_launch *l);
 int  sp_dev_set_seed(sp_dev *d, uint64_t seed);
 int  sp_dev_autotune(sp_dev *d, size_t steps);
+/* State checkpoint: every mutable buffer of the dynamics and the step
+ * counters, to and from a host buffer of sp_dev_state_bytes bytes. */
+size_t sp_dev_state_bytes(sp_dev *d);
+int  sp_dev_state_save(sp_dev *d, void *buf);
+int  sp_dev_state_load(sp_dev *d, const void *buf);
 size_t sp_dev_nwords(const sp_dev *d);
 long long sp_dev_kernel_launches(const sp_dev *d);
 
