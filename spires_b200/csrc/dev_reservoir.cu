@@ -1142,9 +1142,10 @@ extern "C" int sp_dev_state_save(sp_dev *d, void *buf)
     for (const auto &it : items) {
         if (!it.ptr || !it.bytes)
             continue;
-        SP_CK(cudaMemcpy(p, it.ptr, it.bytes, cudaMemcpyDeviceToHost));
+        SP_CK(cudaMemcpyAsync(p, it.ptr, it.bytes, cudaMemcpyDeviceToHost, d->stream));
         p += it.bytes;
     }
+    SP_CK(cudaStreamSynchronize(d->stream));
     return SP_OK;
 }
 
@@ -1165,9 +1166,10 @@ extern "C" int sp_dev_state_load(sp_dev *d, const void *buf)
     for (const auto &it : items) {
         if (!it.ptr || !it.bytes)
             continue;
-        SP_CK(cudaMemcpy(it.ptr, p, it.bytes, cudaMemcpyHostToDevice));
+        SP_CK(cudaMemcpyAsync(it.ptr, p, it.bytes, cudaMemcpyHostToDevice, d->stream));
         p += it.bytes;
     }
+    SP_CK(cudaStreamSynchronize(d->stream)); // the caller's buffer may go away
     d->step = h.step;
     d->syn_step = h.syn_step;
     d->phase = (int)h.phase;
