@@ -54,26 +54,6 @@ def test_ridge_matches_fp64_oracle(lam):
     assert rel(W, Wo) < (1e-9 if lam >= 1e-2 else 1e-5)
 
 
-def test_ridge_more_than_sixteen_outputs():
-    """21 outputs, as many as a caller likes in the reference: solved 16 at a
-    time over the one system matrix, the FP64 oracle's solution for all of
-    them, through the reservoir and through ridge_fit on host states."""
-    cfg = cfg_gl(dout=21)
-    u, y = data(500, 2, 21, seed=9)
-    r = sp.Reservoir(cfg, seed=3)
-    r.train_ridge(u, y, 1e-2)
-    W = r.readout()
-    r.close()
-    orc = O.Oracle(cfg, sp.HostModel(cfg, seed=3))
-    phi, _, _ = orc.run(u)
-    Wo = O.oracle_ridge(phi, y, 1e-2)
-    assert W.shape == (21, cfg.num_neurons)
-    assert rel(phi @ W.T, phi @ Wo.T) < 1e-9
-    assert rel(W, Wo) < 1e-9
-    W2, _ = sp.ridge_fit(phi, y, 1e-2)
-    assert rel(W2, Wo) < 1e-9
-
-
 @pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
 def test_ridge_matches_compiled_reference():
     cfg = cfg_gl(n=150)
@@ -253,3 +233,23 @@ def test_ridge_dual_form_when_rows_are_few(lam):
     assert rel(phi[20:] @ W.T, phi[20:] @ Wo.T) < 1e-8
     assert rel(W, Wo) < (1e-6 if lam >= 1e-2 else 1e-3)
     assert rep.rel_residual < 1e-8
+
+
+def test_ridge_more_than_sixteen_outputs():
+    """21 outputs, as many as a caller likes in the reference: solved 16 at a
+    time over the one system matrix, the FP64 oracle's solution for all of
+    them, through the reservoir and through ridge_fit on host states."""
+    cfg = cfg_gl(dout=21)
+    u, y = data(500, 2, 21, seed=9)
+    r = sp.Reservoir(cfg, seed=3)
+    r.train_ridge(u, y, 1e-2)
+    W = r.readout()
+    r.close()
+    orc = O.Oracle(cfg, sp.HostModel(cfg, seed=3))
+    phi, _, _ = orc.run(u)
+    Wo = O.oracle_ridge(phi, y, 1e-2)
+    assert W.shape == (21, cfg.num_neurons)
+    assert rel(phi @ W.T, phi @ Wo.T) < 1e-9
+    assert rel(W, Wo) < 1e-9
+    W2, _ = sp.ridge_fit(phi, y, 1e-2)
+    assert rel(W2, Wo) < 1e-9
