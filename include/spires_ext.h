@@ -96,19 +96,58 @@ spires_status spires_ext_autotune(spires_reservoir *r, size_t steps);
  * stream derived from seed and i). Takes effect at the next reset. */
 spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t seed);
 
+/* ---- bounded waits and failure paths ---------------------------------------
+ * No counterpart in the reference, which prints or exits on internal errors.
+ * Every wait inside the step kernel (the grid barrier between micro-steps, the
+ * history pipeline's barriers) is bounded: when one runs out, the kernel
+ * records an error code (1 = a wait ran out) and the micro-step, every CTA
+ * returns at its next wait, in-flight copies are drained, and the call that
+ * waited for the launch returns SPIRES_ERR_INTERNAL. The reservoir's state
+ * is then undefined until spires_reservoir_reset; the device stays usable.
+ *
+ * set_wait_limit: the limit of those waits in milliseconds (default 2000,
+ * at most 60000).
+ * last_device_error: code and micro-step (counted from the reservoir's
+ * creation or last reset) of the last such error, 0 if none.
+ * test_withhold_arrival: test hook, one-shot. In the next launch, CTA `cta`
+ * does not arrive at the grid barrier that opens micro-step `micro_step`
+ * (counted from that launch's first micro-step, >= 1), so the others' wait
+ * runs out as it would if a CTA had stopped. Ignored by single-CTA launches.
+ * test_fail_device_alloc: test hook, process-wide. After `after` more device
+ * allocations by this library the next one fails (as an out-of-memory
+ * cudaMalloc would), then allocations succeed again; -1 clears it.
+ * test_live_device_allocs: device allocations of this library not yet freed
+ * (process-wide), to check that failed calls release what they allocated. */
+spires_status spires_ext_set_wait_limit(spires_reservoir *r, double ms);
+spires_status spires_ext_last_device_error(const spires_reservoir *r, int *code,
+                                           long long *micro_step);
+spires_status spires_ext_test_withhold_arrival(spires_reservoir *r, int cta,
+                                               long long micro_step);
+void          spires_ext_test_fail_device_alloc(long long after);
+long long     spires_ext_test_live_device_allocs(void);
+
 /* ---- state checkpoint -------------------------------------------------------
  * Everything a run continues from: membrane potentials, refractory clocks,
  * the FLIF_GL history ring or Caputo registers, the FLIF_DIFFUSIVE sampler
  * states, the latest spike words, synaptic drive and traces, the fractional
  * synapse history, the step counters -- and the readout W_out. Saving waits
- * for the steps already queued. A buffer loads only into a reservoir of the
- * same sizes and models (SPIRES_ERR_INVALID_ARG otherwise); one built from
- * the same configuration and seed then continues bit for bit as the saved
- * one would have. The weights W and W_in are not part of it. No counterpart
- * in the reference, which has no state setter. */
+ * for the steps already queued; buf_bytes must be at least
+ * spires_ext_state_bytes(r). The buffer starts with a header holding the
+ * sizes (neurons, inputs, outputs, ring lengths, edges), the micro-step count,
+ * the models and a 64-bit hash of everything the dynamics read (dt, the
+ * derived neuron and synapse constants, the recurrent weights and their
+ * pattern, W_in, the history coefficients). Load accepts only a buffer of
+ * exactly spires_ext_state_bytes(r) bytes whose header equals this
+ * reservoir's, and checks all of it before touching the reservoir
+ * (SPIRES_ERR_INVALID_ARG otherwise, reservoir unchanged): a reservoir built
+ * from the same configuration and seed then continues bit for bit as the saved
+ * one would have. If a device copy fails during a load (SPIRES_ERR_INTERNAL),
+ * the reservoir's state is undefined until spires_reservoir_reset. The weights
+ * W and W_in are not part of the buffer. No counterpart in the reference,
+ * which has no state setter. */
 size_t        spires_ext_state_bytes(spires_reservoir *r);
-spires_status spires_ext_state_save(spires_reservoir *r, void *buf);
-spires_status spires_ext_state_load(spires_reservoir *r, const void *buf);
+spires_status spires_ext_state_save(spires_reservoir *r, void *buf, size_t buf_bytes);
+spires_status spires_ext_state_load(spires_reservoir *r, const void *buf, size_t buf_bytes);
 
 /* ---- recurrent weights from a dense matrix ----------------------------------
  * Replaces W by dense[N x N] (row-major, zero = no edge) the way the
@@ -233,12 +272,15 @@ spires_status spires_ext_agile_batch_best(const spires_ext_agile_batch *b, int c
  * It calls no cudaMalloc/cudaFree: its working memory is one fixed array of
  * this library (8.6 MB, held on every GPU that loads the library until the
  * process exits), which bounds the sizes: n <= 512, dout <= 16, T <= 16384;
- * larger requests return SPIRES_ERR_INVALID_ARG. The first call on a device
+ * larger requests return SPIRES_ERR_INVALID_ARG. A singular system (the
+ * Cholesky factorisation fails and so does LU with partial pivoting) returns
+ * SPIRES_ERR_INTERNAL with d_w_out left as it was. The first call on a device
  * looks up the array's device address, so make that first call before any
  * stream capture. Every call shares the one array, so calls that overlap on
  * the GPU (other streams, other host threads) race; serialise them. `stream`
- * is a cudaStream_t (NULL = default stream); the call returns after the work
- * on that stream has finished. */
+ * is a cudaStream_t (NULL = default stream). Each call waits on the host for
+ * its work on that stream: the refinement reads a residual norm back after
+ * every sweep, and the call returns after the last kernel has finished. */
 spires_status spires_ext_ridge_solve_noalloc(const double *d_states, const double *d_targets,
                                              size_t T, size_t n, size_t dout, size_t washout,
                                              double lambda, double *d_w_out, void *stream);

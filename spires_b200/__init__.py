@@ -160,9 +160,15 @@ EXT_SIGNATURES = {
     "spires_ext_set_launch": (C.c_int, [_VP, C.POINTER(Launch)]),
     "spires_ext_autotune": (C.c_int, [_VP, C.c_size_t]),
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),
+    "spires_ext_set_wait_limit": (C.c_int, [_VP, C.c_double]),
+    "spires_ext_last_device_error": (C.c_int, [_VP, C.POINTER(C.c_int),
+                                              C.POINTER(C.c_longlong)]),
+    "spires_ext_test_withhold_arrival": (C.c_int, [_VP, C.c_int, C.c_longlong]),
+    "spires_ext_test_fail_device_alloc": (None, [C.c_longlong]),
+    "spires_ext_test_live_device_allocs": (C.c_longlong, []),
     "spires_ext_state_bytes": (C.c_size_t, [_VP]),
-    "spires_ext_state_save": (C.c_int, [_VP, _VP]),
-    "spires_ext_state_load": (C.c_int, [_VP, _VP]),
+    "spires_ext_state_save": (C.c_int, [_VP, _VP, C.c_size_t]),
+    "spires_ext_state_load": (C.c_int, [_VP, _VP, C.c_size_t]),
     "spires_ext_train_ridge": (C.c_int, [_VP, _dp, _dp, C.c_size_t, C.c_double,
                                          C.POINTER(RidgeOpts), C.POINTER(RidgeReport)]),
     "spires_ext_ridge_fit": (C.c_int, [_dp, C.c_size_t, C.c_size_t, _dp, C.c_size_t, C.c_double,

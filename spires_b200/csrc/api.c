@@ -517,36 +517,178 @@ SPIRES_EXPORT spires_status spires_ext_set_seed(spires_reservoir *r, uint64_t se
     return to_status(sp_dev_set_seed(r->dev, seed));
 }
 
-/* state checkpoint: the device state (sp_dev_state_*), then W_out [dout x n] */
+/* bounded waits and failure-path test hooks */
+long long sp_alloc_live(void);
+void      sp_alloc_fail_after(long long count);
+
+SPIRES_EXPORT spires_status spires_ext_set_wait_limit(spires_reservoir *r, double ms)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_set_wait_limit(r->dev, ms));
+}
+
+SPIRES_EXPORT spires_status spires_ext_test_withhold_arrival(spires_reservoir *r, int cta,
+                                                             long long micro_step)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_hold_arrival(r->dev, cta, micro_step));
+}
+
+SPIRES_EXPORT spires_status spires_ext_last_device_error(const spires_reservoir *r, int *code,
+                                                         long long *micro_step)
+{
+    if (!r || !r->dev)
+        return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_dev_last_error(r->dev, code, micro_step));
+}
+
+SPIRES_EXPORT void spires_ext_test_fail_device_alloc(long long after)
+{
+    sp_alloc_fail_after(after);
+}
+
+SPIRES_EXPORT long long spires_ext_test_live_device_allocs(void)
+{
+    return sp_alloc_live();
+}
+
+/* state checkpoint: a model header (sizes, micro-steps and a hash of
+ * everything the dynamics read), the device state (sp_dev_state_*), then
+ * W_out [dout x n]. */
+typedef struct {
+    char     magic[8];
+    uint64_t total_bytes;
+    uint64_t n, din, dout;
+    int64_t  micro, neuron_type, syn_type, syn_backend;
+    uint64_t model_hash;
+} sp_ckpt_header;
+
+/* FNV-1a (64-bit) over a byte range */
+static uint64_t fnv1a(uint64_t h, const void *p, size_t bytes)
+{
+    const unsigned char *c = (const unsigned char *)p;
+    for (size_t k = 0; k < bytes; ++k) {
+        h ^= c[k];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+#define HASH_FIELD(h, x) (h) = fnv1a((h), &(x), sizeof(x))
+
+/* Identity of the dynamics a checkpoint belongs to: dt, the derived neuron and
+ * synapse constants (which follow the current parameter arrays), the recurrent
+ * CSR, W_in and the history coefficients. Two reservoirs with the same hash
+ * step the same state to the same next state. */
+static uint64_t model_hash(const sp_host_model *m)
+{
+    uint64_t h = 14695981039346656037ull;
+    const sp_neuron_consts *nc = &m->nc;
+    const sp_synapse_consts *sc = &m->sc;
+    HASH_FIELD(h, m->dt);
+    HASH_FIELD(h, m->input_strength);
+    h = fnv1a(h, &nc->a, 12 * sizeof(double));
+    HASH_FIELD(h, nc->v_init);
+    HASH_FIELD(h, nc->tprev_init);
+    HASH_FIELD(h, nc->L);
+    HASH_FIELD(h, nc->det_refr_steps);
+    HASH_FIELD(h, nc->diff_stochastic);
+    HASH_FIELD(h, sc->decay);
+    HASH_FIELD(h, sc->omd);
+    HASH_FIELD(h, sc->frac_dta);
+    HASH_FIELD(h, sc->frac_tau);
+    HASH_FIELD(h, sc->frac_L);
+    HASH_FIELD(h, sc->mexp_N);
+    HASH_FIELD(h, m->diffusive_seed);
+    if (m->row_ptr)
+        h = fnv1a(h, m->row_ptr, (m->n + 1) * sizeof(int64_t));
+    if (m->col)
+        h = fnv1a(h, m->col, m->nnz * sizeof(int32_t));
+    if (m->w)
+        h = fnv1a(h, m->w, m->nnz * sizeof(double));
+    if (m->W_in)
+        h = fnv1a(h, m->W_in, m->n * m->din * sizeof(double));
+    if (m->coef && nc->L > 0)
+        h = fnv1a(h, m->coef, (size_t)nc->L * sizeof(double));
+    if (m->edge_decay)
+        h = fnv1a(h, m->edge_decay, m->nnz * sizeof(double));
+    if (m->syn_coef && sc->frac_L > 0)
+        h = fnv1a(h, m->syn_coef, (size_t)sc->frac_L * sizeof(double));
+    if (m->mexp_decay && sc->mexp_N > 0) {
+        h = fnv1a(h, m->mexp_decay, (size_t)sc->mexp_N * sizeof(double));
+        h = fnv1a(h, m->mexp_c, (size_t)sc->mexp_N * sizeof(double));
+    }
+    return h;
+}
+
+static void ckpt_header(const spires_reservoir *r, size_t total, sp_ckpt_header *h)
+{
+    memset(h, 0, sizeof(*h));
+    memcpy(h->magic, "SPCKPT02", 8);
+    h->total_bytes = total;
+    h->n = r->m.n;
+    h->din = r->m.din;
+    h->dout = r->m.dout;
+    h->micro = r->m.micro_steps;
+    h->neuron_type = r->m.neuron_type;
+    h->syn_type = r->m.syn_type;
+    h->syn_backend = r->m.syn_backend;
+    h->model_hash = model_hash(&r->m);
+}
+
 SPIRES_EXPORT size_t spires_ext_state_bytes(spires_reservoir *r)
 {
     if (!r || !r->dev)
         return 0;
-    return sp_dev_state_bytes(r->dev) + r->m.dout * r->m.n * sizeof(double);
+    return sizeof(sp_ckpt_header) + sp_dev_state_bytes(r->dev) +
+           r->m.dout * r->m.n * sizeof(double);
 }
 
-SPIRES_EXPORT spires_status spires_ext_state_save(spires_reservoir *r, void *buf)
+SPIRES_EXPORT spires_status spires_ext_state_save(spires_reservoir *r, void *buf,
+                                                  size_t buf_bytes)
 {
     if (!r || !r->dev || !buf)
         return SPIRES_ERR_INVALID_ARG;
-    int rc = sp_dev_state_save(r->dev, buf);
+    const size_t total = spires_ext_state_bytes(r);
+    if (buf_bytes < total)
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ckpt_header h;
+    ckpt_header(r, total, &h);
+    memcpy(buf, &h, sizeof(h));
+    char *p = (char *)buf + sizeof(h);
+    int rc = sp_dev_state_save(r->dev, p);
     if (rc)
         return to_status(rc);
-    memcpy((char *)buf + sp_dev_state_bytes(r->dev), r->m.W_out,
-           r->m.dout * r->m.n * sizeof(double));
+    memcpy(p + sp_dev_state_bytes(r->dev), r->m.W_out, r->m.dout * r->m.n * sizeof(double));
     return SPIRES_OK;
 }
 
-SPIRES_EXPORT spires_status spires_ext_state_load(spires_reservoir *r, const void *buf)
+SPIRES_EXPORT spires_status spires_ext_state_load(spires_reservoir *r, const void *buf,
+                                                  size_t buf_bytes)
 {
     if (!r || !r->dev || !buf)
         return SPIRES_ERR_INVALID_ARG;
-    int rc = sp_dev_state_load(r->dev, buf);
+    /* every check comes before anything of the reservoir is touched */
+    const size_t total = spires_ext_state_bytes(r);
+    if (buf_bytes != total || buf_bytes < sizeof(sp_ckpt_header))
+        return SPIRES_ERR_INVALID_ARG;
+    sp_ckpt_header h, mine;
+    memcpy(&h, buf, sizeof(h));
+    ckpt_header(r, total, &mine);
+    if (memcmp(&h, &mine, sizeof(h)) != 0)
+        return SPIRES_ERR_INVALID_ARG;
+    const char *p = (const char *)buf + sizeof(h);
+    int rc = sp_dev_state_check(r->dev, p);
+    if (rc)
+        return to_status(rc);
+    rc = sp_dev_state_load(r->dev, p);
     if (rc)
         return to_status(rc);
     const size_t wb = r->m.dout * r->m.n * sizeof(double);
     if (wb) {
-        memcpy(r->m.W_out, (const char *)buf + sp_dev_state_bytes(r->dev), wb);
+        memcpy(r->m.W_out, p + sp_dev_state_bytes(r->dev), wb);
         rc = sp_dev_upload_w_out(r->dev, r->m.W_out);
     }
     return to_status(rc);

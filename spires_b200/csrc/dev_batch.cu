@@ -28,6 +28,7 @@
 #include <cstring>
 #include <numeric>
 #include <vector>
+#include "sp_alloc.h"
 #include "sp_dev.h"
 #include "sp_kernels.cuh"
 #include "sp_dev_internal.h"
@@ -72,11 +73,6 @@ struct BParams {
     int max_nw;               // most spike words of an instance
     int list_cap;             // largest column-block instance (spike list in smem)
 };
-
-__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p)
-{
-    return *(const volatile unsigned long long *)p;
-}
 
 constexpr int kHistChunk = 32;  // ring values in flight per thread (cost model)
 
@@ -568,7 +564,7 @@ static void batch_free_run(sp_batch *b)
     void *dv[] = {b->d_u, b->d_ras, b->d_ras_nat, b->d_vnat, b->d_phi};
     for (void *p : dv)
         if (p)
-            cudaFree(p);
+            sp_cuda_free(p);
     void *hv[] = {b->h_u, b->h_ras, b->h_vnat};
     for (void *p : hv)
         if (p)
@@ -589,7 +585,7 @@ extern "C" void sp_batch_destroy(sp_batch *b)
     void *d[] = {b->arena, b->d_inst, b->d_sched, b->d_bar, b->d_err};
     for (void *p : d)
         if (p)
-            cudaFree(p);
+            sp_cuda_free(p);
     for (auto &m : b->models)
         sp_model_free(&m);
     if (b->stream)
@@ -924,7 +920,7 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
     for (size_t k = 0; !rc && k < count; ++k)
         if (min_ctas(b->inst[k]) > b->P)
             rc = SP_EINVAL;  // wider than the whole grid
-    if (!rc && cudaMalloc(&b->arena, total) != cudaSuccess)
+    if (!rc && sp_cuda_malloc(&b->arena, total) != cudaSuccess)
         rc = SP_EALLOC;
     if (rc) {
         cudaGetLastError();
@@ -1070,9 +1066,9 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         sp_batch_destroy(b);
         return SP_EINTERNAL;
     }
-    if (cudaMalloc(&b->d_bar, (size_t)b->P * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc(&b->d_err, 4 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&b->d_inst, count * sizeof(BInst)) != cudaSuccess ||
+    if (sp_cuda_malloc(&b->d_bar, (size_t)b->P * sizeof(unsigned long long)) != cudaSuccess ||
+        sp_cuda_malloc(&b->d_err, 4 * sizeof(int)) != cudaSuccess ||
+        sp_cuda_malloc(&b->d_inst, count * sizeof(BInst)) != cudaSuccess ||
         cudaMemset(b->d_err, 0, 4 * sizeof(int)) != cudaSuccess) {
         sp_batch_destroy(b);
         return SP_EALLOC;
@@ -1105,12 +1101,12 @@ static int batch_prepare(sp_batch *b, const size_t *T, int want_phi)
     b->ras_total = ras_total;
     b->v_total = v_total;
     b->phi_total = phi_total;
-    BK(cudaMalloc(&b->d_u, (u_total ? u_total : 1) * 8));
-    BK(cudaMalloc(&b->d_ras, (ras_total ? ras_total : 1) * 4));
-    BK(cudaMalloc(&b->d_ras_nat, (ras_total ? ras_total : 1) * 4));
-    BK(cudaMalloc(&b->d_vnat, v_total * 8));
+    BK(sp_cuda_malloc(&b->d_u, (u_total ? u_total : 1) * 8));
+    BK(sp_cuda_malloc(&b->d_ras, (ras_total ? ras_total : 1) * 4));
+    BK(sp_cuda_malloc(&b->d_ras_nat, (ras_total ? ras_total : 1) * 4));
+    BK(sp_cuda_malloc(&b->d_vnat, v_total * 8));
     if (want_phi)
-        BK(cudaMalloc(&b->d_phi, (phi_total ? phi_total : 1) * 8));
+        BK(sp_cuda_malloc(&b->d_phi, (phi_total ? phi_total : 1) * 8));
     BK(cudaMallocHost(&b->h_u, (u_total ? u_total : 1) * 8));
     BK(cudaMallocHost(&b->h_ras, (ras_total ? ras_total : 1) * 4));
     BK(cudaMallocHost(&b->h_vnat, v_total * 8));
@@ -1136,9 +1132,9 @@ static int batch_prepare(sp_batch *b, const size_t *T, int want_phi)
     sched.insert(sched.end(), b->job_off.begin(), b->job_off.end());
     sched.insert(sched.end(), b->jobs.begin(), b->jobs.end());
     if (b->d_sched)
-        cudaFree(b->d_sched);
+        sp_cuda_free(b->d_sched);
     b->d_sched = nullptr;
-    BK(cudaMalloc(&b->d_sched, sched.size() * sizeof(int)));
+    BK(sp_cuda_malloc(&b->d_sched, sched.size() * sizeof(int)));
     BK(cudaMemcpy(b->d_sched, sched.data(), sched.size() * sizeof(int), cudaMemcpyHostToDevice));
     BK(cudaMemcpy(b->d_inst, b->inst.data(), cnt * sizeof(BInst), cudaMemcpyHostToDevice));
     return SP_OK;
@@ -1271,7 +1267,7 @@ static int batch_readout(sp_batch *b, const BInst &I, const double *phi, size_t 
     if (!I.dense)
         return sp_launch_readout(b->stream, b->w_pos[&I - b->inst.data()], phi, I.rs, T, dout, Y);
     double *tmp = nullptr;
-    if (cudaMallocAsync(&tmp, (T ? T : 1) * (size_t)I.rs * sizeof(double), b->stream) !=
+    if (sp_cuda_malloc_async(&tmp, (T ? T : 1) * (size_t)I.rs * sizeof(double), b->stream) !=
         cudaSuccess) {
         cudaGetLastError();
         return SP_EALLOC;
@@ -1282,7 +1278,7 @@ static int batch_readout(sp_batch *b, const BInst &I, const double *phi, size_t 
     int rc = cudaGetLastError() == cudaSuccess ? SP_OK : SP_EINTERNAL;
     if (!rc)
         rc = sp_launch_readout(b->stream, b->w_pos[&I - b->inst.data()], tmp, I.rs, T, dout, Y);
-    cudaFreeAsync(tmp, b->stream);
+    sp_cuda_free_async(tmp, b->stream);
     return rc;
 }
 
@@ -1311,14 +1307,14 @@ extern "C" int sp_batch_train_ridge(sp_batch *b, const double *const *u, const d
     auto cleanup = [&]() {
         cudaStreamSynchronize(b->stream);
         if (nat)
-            cudaFree(nat);
+            sp_cuda_free(nat);
         if (Y)
-            cudaFree(Y);
+            sp_cuda_free(Y);
         if (W)
-            cudaFree(W);
+            sp_cuda_free(W);
     };
-    if (cudaMalloc(&nat, max_tn * 8) != cudaSuccess || cudaMalloc(&Y, max_ty * 8) != cudaSuccess ||
-        cudaMalloc(&W, max_wn * 8) != cudaSuccess) {
+    if (sp_cuda_malloc(&nat, max_tn * 8) != cudaSuccess || sp_cuda_malloc(&Y, max_ty * 8) != cudaSuccess ||
+        sp_cuda_malloc(&W, max_wn * 8) != cudaSuccess) {
         cudaGetLastError();
         cleanup();
         return SP_EALLOC;
@@ -1387,7 +1383,7 @@ extern "C" int sp_batch_predict(sp_batch *b, const double *const *u, const size_
     for (size_t k = 0; k < b->inst.size(); ++k)
         max_ty = std::max(max_ty, T[k] * b->models[k].dout);
     double *Y = nullptr;
-    BK(cudaMalloc(&Y, max_ty * 8));
+    BK(sp_cuda_malloc(&Y, max_ty * 8));
     size_t po = 0;
     for (size_t k = 0; k < b->inst.size() && !rc; ++k) {
         const BInst &I = b->inst[k];
@@ -1404,7 +1400,7 @@ extern "C" int sp_batch_predict(sp_batch *b, const double *const *u, const size_
             rc = SP_EINTERNAL;
     }
     cudaStreamSynchronize(b->stream);
-    cudaFree(Y);
+    sp_cuda_free(Y);
     if (elapsed_ms)
         *elapsed_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1433,13 +1429,13 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
         max_wn = std::max(max_wn, (size_t)b->inst[k].n * b->models[k].dout);
     }
     double *nat = nullptr, *Y = nullptr, *W = nullptr;
-    if (cudaMalloc(&nat, max_tn * 8) != cudaSuccess || cudaMalloc(&Y, max_ty * 8) != cudaSuccess ||
-        cudaMalloc(&W, max_wn * 8) != cudaSuccess) {
+    if (sp_cuda_malloc(&nat, max_tn * 8) != cudaSuccess || sp_cuda_malloc(&Y, max_ty * 8) != cudaSuccess ||
+        sp_cuda_malloc(&W, max_wn * 8) != cudaSuccess) {
         cudaGetLastError();
         if (nat)
-            cudaFree(nat);
+            sp_cuda_free(nat);
         if (Y)
-            cudaFree(Y);
+            sp_cuda_free(Y);
         return SP_EALLOC;
     }
     size_t po = 0;
@@ -1481,9 +1477,9 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
             rc = SP_EINTERNAL;
     }
     cudaStreamSynchronize(b->stream);
-    cudaFree(nat);
-    cudaFree(Y);
-    cudaFree(W);
+    sp_cuda_free(nat);
+    sp_cuda_free(Y);
+    sp_cuda_free(W);
     if (elapsed_ms)
         *elapsed_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

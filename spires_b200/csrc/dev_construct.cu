@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include "sp_alloc.h"
 #include "sp_dev.h"
 #include "sp_kernels.cuh"
 #include "sp_dev_internal.h"
@@ -144,7 +145,7 @@ extern "C" int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const in
     // stream-ordered allocation: no device-wide synchronisation, so several
     // host threads building reservoirs at once do not serialise here
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocAsync(&buf, total, s) != cudaSuccess) {
+        sp_cuda_malloc_async(&buf, total, s) != cudaSuccess) {
         cudaGetLastError();
         if (s)
             cudaStreamDestroy(s);
@@ -187,7 +188,7 @@ extern "C" int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const in
     } else {
         *out = h_out[0];
     }
-    cudaFreeAsync(buf, s);
+    sp_cuda_free_async(buf, s);
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     return rc;

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <cmath>
 #include <chrono>
+#include "sp_alloc.h"
 #include "sp_dev.h"
 #include "sp_kernels.cuh"
 #include "sp_dev_internal.h"
@@ -733,8 +734,8 @@ static int ridge_dual(cudaStream_t s, const double *Phi, int n, size_t T, size_t
     const size_t tot = (size_t)n * dout;
     const dim3 gp((n + 127) / 128, parts);
     auto tg = std::chrono::steady_clock::now();
-    RK(cudaMalloc(&Pt, (size_t)n * tw * sizeof(double)));
-    RK(cudaMalloc(&K, tw * tw * sizeof(double)));
+    RK(sp_cuda_malloc(&Pt, (size_t)n * tw * sizeof(double)));
+    RK(sp_cuda_malloc(&K, tw * tw * sizeof(double)));
     {
         dim3 g((n + 31) / 32, (unsigned)((tw + 31) / 32));
         k_rows_to_cols<<<g, dim3(32, 8), 0, s>>>(Phi, n, w0, T, Pt);
@@ -776,9 +777,9 @@ static int ridge_dual(cudaStream_t s, const double *Phi, int n, size_t T, size_t
 out:
     cudaStreamSynchronize(s);
     if (Pt)
-        cudaFree(Pt);
+        sp_cuda_free(Pt);
     if (K)
-        cudaFree(K);
+        sp_cuda_free(K);
     return rc;
 }
 
@@ -804,13 +805,13 @@ static int ridge_mixed(cudaStream_t s, const double *Phi, int n, size_t T, size_
            *dots = nullptr;
     double h_rz[16], h_pq[16], h_c[16];
     auto tf = std::chrono::steady_clock::now();
-    RK(cudaMalloc(&A0, nn * sizeof(double)));
-    RK(cudaMalloc(&Z, tot * sizeof(double)));
-    RK(cudaMalloc(&P, tot * sizeof(double)));
-    RK(cudaMalloc(&Q, tot * sizeof(double)));
-    RK(cudaMalloc(&Yz, (T ? T : 1) * (size_t)dout * sizeof(double)));
-    RK(cudaMalloc(&c, 16 * sizeof(double)));
-    RK(cudaMalloc(&dots, 16 * sizeof(double)));
+    RK(sp_cuda_malloc(&A0, nn * sizeof(double)));
+    RK(sp_cuda_malloc(&Z, tot * sizeof(double)));
+    RK(sp_cuda_malloc(&P, tot * sizeof(double)));
+    RK(sp_cuda_malloc(&Q, tot * sizeof(double)));
+    RK(sp_cuda_malloc(&Yz, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(sp_cuda_malloc(&c, 16 * sizeof(double)));
+    RK(sp_cuda_malloc(&dots, 16 * sizeof(double)));
     RK(cudaMemsetAsync(Yz, 0, (T ? T : 1) * (size_t)dout * sizeof(double), s));
     RK(cudaMemcpyAsync(A0, A, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
     {
@@ -889,7 +890,7 @@ out:
     void *bufs[] = {A0, Z, P, Q, Yz, c, dots};
     for (void *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     return rc;
 }
 
@@ -909,15 +910,15 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
         return SP_OK;
     if (dout > 16)
         return SP_EINVAL; /* per-thread accumulators below hold up to 16 outputs */
-    RK(cudaMalloc(&A, (size_t)n * n * sizeof(double)));
-    RK(cudaMalloc(&B, (size_t)n * dout * sizeof(double)));
-    RK(cudaMalloc(&W, (size_t)n * dout * sizeof(double)));
-    RK(cudaMalloc(&R, (size_t)n * dout * sizeof(double)));
-    RK(cudaMalloc(&E, (T ? T : 1) * (size_t)dout * sizeof(double)));
-    RK(cudaMalloc(&part, (size_t)parts * n * dout * sizeof(double)));
-    RK(cudaMalloc(&tmp, 4 * sizeof(double)));
-    RK(cudaMalloc(&info, sizeof(int)));
-    RK(cudaMalloc(&piv, (size_t)n * sizeof(int)));
+    RK(sp_cuda_malloc(&A, (size_t)n * n * sizeof(double)));
+    RK(sp_cuda_malloc(&B, (size_t)n * dout * sizeof(double)));
+    RK(sp_cuda_malloc(&W, (size_t)n * dout * sizeof(double)));
+    RK(sp_cuda_malloc(&R, (size_t)n * dout * sizeof(double)));
+    RK(sp_cuda_malloc(&E, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(sp_cuda_malloc(&part, (size_t)parts * n * dout * sizeof(double)));
+    RK(sp_cuda_malloc(&tmp, 4 * sizeof(double)));
+    RK(sp_cuda_malloc(&info, sizeof(int)));
+    RK(sp_cuda_malloc(&piv, (size_t)n * sizeof(int)));
     RK(cudaMemsetAsync(info, 0, sizeof(int), s));
 
     if (lambda > 0.0 && 2 * (T - w0) <= (size_t)n) {
@@ -1043,7 +1044,7 @@ out:
     void *bufs[] = {A, Aw, B, W, R, E, part, tmp, info, piv};
     for (void *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     return rc;
 }
 
@@ -1065,8 +1066,8 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
     double *Yg = nullptr, *Wall = nullptr;
     sp_ridge_report sum;
     memset(&sum, 0, sizeof(sum));
-    RK(cudaMalloc(&Yg, (T ? T : 1) * 16 * sizeof(double)));
-    RK(cudaMalloc(&Wall, (size_t)dout * n * sizeof(double)));
+    RK(sp_cuda_malloc(&Yg, (T ? T : 1) * 16 * sizeof(double)));
+    RK(sp_cuda_malloc(&Wall, (size_t)dout * n * sizeof(double)));
     for (int g0 = 0; g0 < dout && !rc; g0 += 16) {
         const int dg = dout - g0 < 16 ? dout - g0 : 16;
         if (T)
@@ -1092,9 +1093,9 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
 out:
     cudaStreamSynchronize(s);
     if (Yg)
-        cudaFree(Yg);
+        sp_cuda_free(Yg);
     if (Wall)
-        cudaFree(Wall);
+        sp_cuda_free(Wall);
     sum.collect_ms = rep->collect_ms;
     *rep = sum;
     return rc;
@@ -1115,9 +1116,9 @@ extern "C" int sp_ridge_host(const double *h_phi, size_t T, int n, const double 
         return SP_EINVAL;
     auto t0 = std::chrono::steady_clock::now();
     RK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    RK(cudaMalloc(&Phi, T * (size_t)n * sizeof(double)));
-    RK(cudaMalloc(&Y, T * (size_t)dout * sizeof(double)));
-    RK(cudaMalloc(&Wt, (size_t)n * dout * sizeof(double)));
+    RK(sp_cuda_malloc(&Phi, T * (size_t)n * sizeof(double)));
+    RK(sp_cuda_malloc(&Y, T * (size_t)dout * sizeof(double)));
+    RK(sp_cuda_malloc(&Wt, (size_t)n * dout * sizeof(double)));
     RK(cudaMemcpyAsync(Phi, h_phi, T * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
     RK(cudaMemcpyAsync(Y, h_y, T * (size_t)dout * sizeof(double), cudaMemcpyHostToDevice, s));
     RK(cudaStreamSynchronize(s));
@@ -1133,7 +1134,7 @@ out:
     void *bufs[] = {Phi, Y, Wt};
     for (void *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     if (s)
         cudaStreamDestroy(s);
     return rc;
@@ -1155,9 +1156,9 @@ extern "C" int sp_dev_train_ridge(sp_dev *d, const sp_host_model *m, const doubl
     rc = sp_dev_reset_neurons(d, m);
     if (rc)
         return rc;
-    RK(cudaMalloc(&Phi, (T ? T : 1) * (size_t)n * sizeof(double)));
-    RK(cudaMalloc(&Y, (T ? T : 1) * (size_t)dout * sizeof(double)));
-    RK(cudaMalloc(&Wt, (size_t)n * dout * sizeof(double)));
+    RK(sp_cuda_malloc(&Phi, (T ? T : 1) * (size_t)n * sizeof(double)));
+    RK(sp_cuda_malloc(&Y, (T ? T : 1) * (size_t)dout * sizeof(double)));
+    RK(sp_cuda_malloc(&Wt, (size_t)n * dout * sizeof(double)));
     RK(cudaMemcpyAsync(Y, h_y, T * dout * sizeof(double), cudaMemcpyHostToDevice, s));
     {
         sp_run_args a;
@@ -1191,7 +1192,7 @@ out:
     void *bufs[] = {Phi, Y, Wt};
     for (void *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     return rc;
 }
 
@@ -1204,11 +1205,11 @@ extern "C" int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double 
     const int rs = d->rs, n = d->n, dout = d->dout;
     cudaStream_t s = d->stream;
     double *P = nullptr, *Px = nullptr, *scal = nullptr, *Yd = nullptr, *Wn = nullptr;
-    RK(cudaMalloc(&P, (size_t)rs * rs * sizeof(double)));
-    RK(cudaMalloc(&Px, (size_t)rs * sizeof(double)));
-    RK(cudaMalloc(&scal, (size_t)(dout + 1) * sizeof(double)));
-    RK(cudaMalloc(&Yd, (T ? T : 1) * (size_t)(dout ? dout : 1) * sizeof(double)));
-    RK(cudaMalloc(&Wn, (size_t)(dout ? dout : 1) * n * sizeof(double)));
+    RK(sp_cuda_malloc(&P, (size_t)rs * rs * sizeof(double)));
+    RK(sp_cuda_malloc(&Px, (size_t)rs * sizeof(double)));
+    RK(sp_cuda_malloc(&scal, (size_t)(dout + 1) * sizeof(double)));
+    RK(sp_cuda_malloc(&Yd, (T ? T : 1) * (size_t)(dout ? dout : 1) * sizeof(double)));
+    RK(sp_cuda_malloc(&Wn, (size_t)(dout ? dout : 1) * n * sizeof(double)));
     k_diag_init<<<1024, 256, 0, s>>>(P, rs, 1.0 / delta);
     RK(cudaMemsetAsync(d->W_out, 0, (size_t)rs * dout * sizeof(double), s));
     if (T && dout)
@@ -1238,11 +1239,11 @@ extern "C" int sp_dev_train_rls(sp_dev *d, const sp_host_model *m, const double 
     RK(cudaGetLastError());
 out:
     cudaStreamSynchronize(s);
-    if (P) cudaFree(P);
-    if (Px) cudaFree(Px);
-    if (scal) cudaFree(scal);
-    if (Yd) cudaFree(Yd);
-    if (Wn) cudaFree(Wn);
+    if (P) sp_cuda_free(P);
+    if (Px) sp_cuda_free(Px);
+    if (scal) sp_cuda_free(scal);
+    if (Yd) sp_cuda_free(Yd);
+    if (Wn) sp_cuda_free(Wn);
     return rc;
 }
 
@@ -1258,7 +1259,7 @@ extern "C" int sp_dev_train_online(sp_dev *d, const double *h_target, double lr,
     rc = sp_dev_readout(d, d->V, 1, d->d_y);
     if (rc)
         return rc;
-    RK(cudaMalloc(&Wn, (size_t)dout * n * sizeof(double)));
+    RK(sp_cuda_malloc(&Wn, (size_t)dout * n * sizeof(double)));
     RK(cudaMemcpyAsync(d->d_y + dout, h_target, (size_t)dout * sizeof(double),
                        cudaMemcpyHostToDevice, s));
     k_online<<<(unsigned)(((size_t)rs * dout + 255) / 256), 256, 0, s>>>(d->W_out, rs, dout, d->V,
@@ -1273,7 +1274,7 @@ extern "C" int sp_dev_train_online(sp_dev *d, const double *h_target, double lr,
 out:
     cudaStreamSynchronize(s);
     if (Wn)
-        cudaFree(Wn);
+        sp_cuda_free(Wn);
     return rc;
 }
 
@@ -1379,8 +1380,9 @@ spires_ext_ridge_solve_noalloc(const double *d_states, const double *d_targets, 
         k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(d_states, n, washout, T, A, n);
         k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, n, n, lambda);
         if (lu_factor_solve(s, A, n, piv, info, W, dout) != 0) {
-            fprintf(stderr, "Warning: Ridge regression failed (singular system).\n");
-            return cudaStreamSynchronize(s) == cudaSuccess ? SP_OK : SP_EINTERNAL;
+            // singular system: d_w_out is not written, and the caller is told
+            cudaStreamSynchronize(s);
+            return SP_EINTERNAL;
         }
     } else {
         chol_solve(s, A, n, W, dout);

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <numeric>
 #include <vector>
+#include "sp_alloc.h"
 #include "sp_dev.h"
 #include "sp_kernels.cuh"
 #include "sp_dev_internal.h"
@@ -210,7 +211,7 @@ static int dalloc(T **p, size_t count)
     *p = nullptr;
     if (count == 0)
         count = 1;
-    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    cudaError_t e = sp_cuda_malloc((void **)p, count * sizeof(T));
     if (e != cudaSuccess) {
         *p = nullptr;
         return e == cudaErrorMemoryAllocation ? SP_EALLOC : SP_EINTERNAL;
@@ -406,6 +407,8 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
     sp_dev *d = (sp_dev *)calloc(1, sizeof(sp_dev));
     if (!d)
         return SP_EALLOC;
+    d->hold_cta = -1;
+    d->hold_b = -1;
     int rc = SP_OK;
 #define TRY(x)                  \
     do {                        \
@@ -569,7 +572,7 @@ extern "C" void sp_dev_destroy(sp_dev *d)
                     d->d_spkd, d->d_ras, d->d_ras_nat, d->bar, d->err, d->pos_of, d->nid_of};
     for (void *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     if (d->stream)
         cudaStreamDestroy(d->stream);
     free(d);
@@ -599,15 +602,46 @@ extern "C" int sp_dev_set_seed(sp_dev *d, uint64_t seed)
 
 static int check_err(sp_dev *d)
 {
-    int h[2] = {0, 0};
-    SP_CK(cudaMemcpyAsync(h, d->err, 2 * sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+    int h[3] = {0, 0, 0};
+    SP_CK(cudaMemcpyAsync(h, d->err, 3 * sizeof(int), cudaMemcpyDeviceToHost, d->stream));
     SP_CK(cudaStreamSynchronize(d->stream));
     if (h[0] != kErrNone) {
+        const long long step =
+            (long long)(((unsigned long long)(unsigned)h[2] << 32) | (unsigned)h[1]);
+        d->last_err_code = h[0];
+        d->last_err_step = step;
         if (getenv("SPIRES_DEBUG"))
-            fprintf(stderr, "spires: device error %d at micro-step %d\n", h[0], h[1]);
-        cudaMemsetAsync(d->err, 0, 2 * sizeof(int), d->stream);
+            fprintf(stderr, "spires: device error %d at micro-step %lld\n", h[0], step);
+        cudaMemsetAsync(d->err, 0, 3 * sizeof(int), d->stream);
+        cudaStreamSynchronize(d->stream);
         return SP_EINTERNAL;
     }
+    return SP_OK;
+}
+
+extern "C" int sp_dev_set_wait_limit(sp_dev *d, double ms)
+{
+    if (!(ms > 0.0) || ms > 60000.0)
+        return SP_EINVAL;
+    d->wait_ns = (unsigned long long)(ms * 1e6);
+    return SP_OK;
+}
+
+extern "C" int sp_dev_hold_arrival(sp_dev *d, int cta, long long micro_step)
+{
+    if (cta < 0 || micro_step < 1)
+        return SP_EINVAL;
+    d->hold_cta = cta;
+    d->hold_b = micro_step;
+    return SP_OK;
+}
+
+extern "C" int sp_dev_last_error(const sp_dev *d, int *code, long long *micro_step)
+{
+    if (code)
+        *code = d->last_err_code;
+    if (micro_step)
+        *micro_step = d->last_err_step;
     return SP_OK;
 }
 
@@ -666,6 +700,15 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.W_in = d->W_in; p.gamma = d->gamma; p.u = u;
     p.phi = phi; p.raster = raster;
     p.bar = d->bar; p.err = d->err;
+    p.tmo = d->wait_ns ? d->wait_ns : kBarrierTimeoutNs;
+    p.hold_cta = -1;
+    p.hold_b = -1;
+    if (d->hold_cta >= 0 && d->hold_b >= 1 && d->hold_b < (long long)T * d->micro) {
+        p.hold_cta = d->hold_cta;  // one-shot: consumed by this launch
+        p.hold_b = d->hold_b;
+    }
+    d->hold_cta = -1;
+    d->hold_b = -1;
     p.nid_of = d->nid_of;
 
     kfn_t fn = pick_kernel(d->ntype, d->stype, l.variant);
@@ -677,7 +720,7 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
         SP_CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     if (l.ctas > 1) {
-        SP_CK(cudaMemsetAsync(d->bar, 0, sizeof(unsigned), d->stream));
+        SP_CK(cudaMemsetAsync(d->bar, 0, sizeof(unsigned long long), d->stream));
         void *args[] = {&p};
         SP_CK(cudaLaunchCooperativeKernel((const void *)fn, grid, block, args, smem, d->stream));
     } else {
@@ -876,25 +919,25 @@ extern "C" int sp_dev_w_out_to_nat(sp_dev *d, double *dev_w_nat)
 extern "C" int sp_dev_upload_w_out(sp_dev *d, const double *h_W_out)
 {
     double *tmp = nullptr;
-    SP_CK(cudaMalloc(&tmp, (size_t)d->n * d->dout * sizeof(double) + 8));
+    SP_CK(sp_cuda_malloc(&tmp, (size_t)d->n * d->dout * sizeof(double) + 8));
     cudaMemcpyAsync(tmp, h_W_out, (size_t)d->n * d->dout * sizeof(double),
                     cudaMemcpyHostToDevice, d->stream);
     int rc = sp_dev_w_out_from_nat(d, tmp);
     cudaStreamSynchronize(d->stream);
-    cudaFree(tmp);
+    sp_cuda_free(tmp);
     return rc ? rc : sp_dev_sync(d);
 }
 
 extern "C" int sp_dev_download_w_out(sp_dev *d, double *h_W_out)
 {
     double *tmp = nullptr;
-    SP_CK(cudaMalloc(&tmp, (size_t)d->n * d->dout * sizeof(double) + 8));
+    SP_CK(sp_cuda_malloc(&tmp, (size_t)d->n * d->dout * sizeof(double) + 8));
     int rc = sp_dev_w_out_to_nat(d, tmp);
     if (!rc)
         cudaMemcpyAsync(h_W_out, tmp, (size_t)d->n * d->dout * sizeof(double),
                         cudaMemcpyDeviceToHost, d->stream);
     cudaStreamSynchronize(d->stream);
-    cudaFree(tmp);
+    sp_cuda_free(tmp);
     return rc ? rc : sp_dev_sync(d);
 }
 
@@ -988,7 +1031,7 @@ static int snapshot(sp_dev *d, std::vector<sp_snap_item> &items, bool take)
         for (auto &it : items) {
             if (!it.ptr || !it.bytes)
                 continue;
-            if (cudaMalloc(&it.save, it.bytes) != cudaSuccess)
+            if (sp_cuda_malloc(&it.save, it.bytes) != cudaSuccess)
                 return SP_EALLOC;
             SP_CK(cudaMemcpyAsync(it.save, it.ptr, it.bytes, cudaMemcpyDeviceToDevice, d->stream));
         }
@@ -1080,7 +1123,7 @@ extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
     cudaStreamSynchronize(d->stream);
     for (auto &it : items)
         if (it.save)
-            cudaFree(it.save);
+            sp_cuda_free(it.save);
     if (rc) {
         d->launch = keep;
         return rc;
@@ -1149,7 +1192,7 @@ extern "C" int sp_dev_state_save(sp_dev *d, void *buf)
     return SP_OK;
 }
 
-extern "C" int sp_dev_state_load(sp_dev *d, const void *buf)
+extern "C" int sp_dev_state_check(sp_dev *d, const void *buf)
 {
     sp_state_header h, mine;
     memcpy(&h, buf, sizeof(h));
@@ -1157,8 +1200,19 @@ extern "C" int sp_dev_state_load(sp_dev *d, const void *buf)
     if (memcmp(h.magic, mine.magic, 8) != 0 || h.n != mine.n || h.rs != mine.rs ||
         h.ntype != mine.ntype || h.stype != mine.stype || h.ring_elems != mine.ring_elems ||
         h.nwords != mine.nwords || h.nnz != mine.nnz || h.frac_L != mine.frac_L ||
-        h.mexp_N != mine.mexp_N || (h.phase != 0 && h.phase != 1))
+        h.mexp_N != mine.mexp_N || (h.phase != 0 && h.phase != 1) || h.step < 0 ||
+        h.syn_step < 0)
         return SP_EINVAL;
+    return SP_OK;
+}
+
+extern "C" int sp_dev_state_load(sp_dev *d, const void *buf)
+{
+    sp_state_header h;
+    int rc = sp_dev_state_check(d, buf);
+    if (rc)
+        return rc;
+    memcpy(&h, buf, sizeof(h));
     SP_CK(cudaStreamSynchronize(d->stream));
     const char *p = (const char *)buf + sizeof(h);
     std::vector<sp_snap_item> items;

@@ -25,6 +25,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+#include "sp_alloc.h"
 #include "sp_dev.h"
 #include "sp_dev_internal.h"
 
@@ -228,7 +229,7 @@ static void mlp_free_work(sp_mlp *m)
     float *bufs[] = {m->X, m->y, m->Z1, m->H1, m->Z2, m->H2, m->O, m->dO, m->dH2, m->dH1, m->rl};
     for (float *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     m->X = m->y = m->Z1 = m->H1 = m->Z2 = m->H2 = m->O = m->dO = m->dH2 = m->dH1 = m->rl =
         nullptr;
     m->cap = 0;
@@ -240,17 +241,17 @@ static int mlp_reserve(sp_mlp *m, int rows)
         return SP_OK;
     mlp_free_work(m);
     const size_t r = (size_t)rows;
-    MK(cudaMalloc(&m->X, r * kIn * 4));
-    MK(cudaMalloc(&m->y, r * 4));
-    MK(cudaMalloc(&m->Z1, r * kHid * 4));
-    MK(cudaMalloc(&m->H1, r * kHid * 4));
-    MK(cudaMalloc(&m->Z2, r * kHid * 4));
-    MK(cudaMalloc(&m->H2, r * kHid * 4));
-    MK(cudaMalloc(&m->O, r * kOut * 4));
-    MK(cudaMalloc(&m->dO, r * kOut * 4));
-    MK(cudaMalloc(&m->dH2, r * kHid * 4));
-    MK(cudaMalloc(&m->dH1, r * kHid * 4));
-    MK(cudaMalloc(&m->rl, r * 4));
+    MK(sp_cuda_malloc(&m->X, r * kIn * 4));
+    MK(sp_cuda_malloc(&m->y, r * 4));
+    MK(sp_cuda_malloc(&m->Z1, r * kHid * 4));
+    MK(sp_cuda_malloc(&m->H1, r * kHid * 4));
+    MK(sp_cuda_malloc(&m->Z2, r * kHid * 4));
+    MK(sp_cuda_malloc(&m->H2, r * kHid * 4));
+    MK(sp_cuda_malloc(&m->O, r * kOut * 4));
+    MK(sp_cuda_malloc(&m->dO, r * kOut * 4));
+    MK(sp_cuda_malloc(&m->dH2, r * kHid * 4));
+    MK(sp_cuda_malloc(&m->dH1, r * kHid * 4));
+    MK(sp_cuda_malloc(&m->rl, r * 4));
     m->cap = rows;
     return SP_OK;
 }
@@ -318,7 +319,7 @@ extern "C" void sp_mlp_destroy(sp_mlp *m)
     float *bufs[] = {m->p, m->g, m->m1, m->m2, m->loss, m->pb};
     for (float *b : bufs)
         if (b)
-            cudaFree(b);
+            sp_cuda_free(b);
     if (m->stream)
         cudaStreamDestroy(m->stream);
     delete m;
@@ -331,10 +332,10 @@ extern "C" int sp_mlp_create(uint64_t seed, sp_mlp **out)
     sp_mlp *m = new sp_mlp();
     int rc = SP_OK;
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&m->p, kParams * 4) != cudaSuccess || cudaMalloc(&m->g, kParams * 4) != cudaSuccess ||
-        cudaMalloc(&m->m1, kParams * 4) != cudaSuccess ||
-        cudaMalloc(&m->m2, kParams * 4) != cudaSuccess || cudaMalloc(&m->loss, 4) != cudaSuccess ||
-        cudaMalloc(&m->pb, kParams * 4) != cudaSuccess)
+        sp_cuda_malloc(&m->p, kParams * 4) != cudaSuccess || sp_cuda_malloc(&m->g, kParams * 4) != cudaSuccess ||
+        sp_cuda_malloc(&m->m1, kParams * 4) != cudaSuccess ||
+        sp_cuda_malloc(&m->m2, kParams * 4) != cudaSuccess || sp_cuda_malloc(&m->loss, 4) != cudaSuccess ||
+        sp_cuda_malloc(&m->pb, kParams * 4) != cudaSuccess)
         rc = SP_EALLOC;
     if (!rc) {
         std::vector<float> h(kParams);

@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
+#include "sp_alloc.h"
 #include "sp_gram.h"
 #include "sp_model.h"
 #include "sp_dev.h"
@@ -118,9 +119,9 @@ extern "C" int sp_gram_split(cudaStream_t s, int mode, const double *X, int n, s
     void *hi = nullptr, *lo = nullptr;
     float *G = nullptr;
     int rc = SP_OK;
-    if (cudaMallocAsync(&hi, (cnt ? cnt : 1) * esz, s) != cudaSuccess ||
-        cudaMallocAsync(&lo, (cnt ? cnt : 1) * esz, s) != cudaSuccess ||
-        cudaMallocAsync(&G, (size_t)n * n * sizeof(float), s) != cudaSuccess) {
+    if (sp_cuda_malloc_async(&hi, (cnt ? cnt : 1) * esz, s) != cudaSuccess ||
+        sp_cuda_malloc_async(&lo, (cnt ? cnt : 1) * esz, s) != cudaSuccess ||
+        sp_cuda_malloc_async(&G, (size_t)n * n * sizeof(float), s) != cudaSuccess) {
         cudaGetLastError();
         rc = SP_EALLOC;
     }
@@ -160,11 +161,11 @@ extern "C" int sp_gram_split(cudaStream_t s, int mode, const double *X, int n, s
             rc = SP_EINTERNAL;
     }
     if (hi)
-        cudaFreeAsync(hi, s);
+        sp_cuda_free_async(hi, s);
     if (lo)
-        cudaFreeAsync(lo, s);
+        sp_cuda_free_async(lo, s);
     if (G)
-        cudaFreeAsync(G, s);
+        sp_cuda_free_async(G, s);
     return rc;
 }
 

@@ -73,6 +73,16 @@ int  sp_dev_autotune(sp_dev *d, size_t steps);
 size_t sp_dev_state_bytes(sp_dev *d);
 int  sp_dev_state_save(sp_dev *d, void *buf);
 int  sp_dev_state_load(sp_dev *d, const void *buf);
+/* Bounded waits of the step kernel: their limit in milliseconds (default
+ * 2000); a one-shot hook that makes CTA `cta` withhold its grid-barrier
+ * arrival at micro-step `micro_step` of the next launch (counted from that
+ * launch's start), so that every other CTA's wait runs out; the code and
+ * micro-step of the last device error the host read. */
+int  sp_dev_set_wait_limit(sp_dev *d, double ms);
+int  sp_dev_hold_arrival(sp_dev *d, int cta, long long micro_step);
+int  sp_dev_last_error(const sp_dev *d, int *code, long long *micro_step);
+/* SP_OK when buf's header matches this reservoir's sizes; touches nothing */
+int  sp_dev_state_check(sp_dev *d, const void *buf);
 size_t sp_dev_nwords(const sp_dev *d);
 long long sp_dev_kernel_launches(const sp_dev *d);
 

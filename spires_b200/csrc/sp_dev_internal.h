@@ -60,8 +60,17 @@ struct sp_dev {
     unsigned *d_ras_nat; // [chunk][nw] neuron-order spike words
     double *d_spkd;      // [n]
     double *h_stage;     // pinned [chunk][dout]
-    unsigned *bar;
-    int *err;
+    unsigned long long *bar;  // grid-barrier arrival counter
+    int *err;                 // [0] code, [1]/[2] micro-step low/high word
+
+    // bounded waits: limit (ns) of every wait in the step kernel; one-shot
+    // test hook (CTA hold_cta withholds its arrival at micro-step hold_b of
+    // the next launch, -1 = none); the last device error seen by the host
+    unsigned long long wait_ns;
+    int hold_cta;
+    long long hold_b;
+    int last_err_code;
+    long long last_err_step;
 
     // 2-D tiled tensor map over the FLIF_GL ring (variant 1), box BW x R
     CUtensorMap tmap;

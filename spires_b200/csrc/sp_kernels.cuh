@@ -30,12 +30,18 @@ __device__ __forceinline__ unsigned ld_volatile_u32(const unsigned *p)
     return *(const volatile unsigned *)p;
 }
 
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p)
+{
+    return *(const volatile unsigned long long *)p;
+}
+
 __device__ __forceinline__ int ld_volatile_i32(const int *p)
 {
     return *(const volatile int *)p;
 }
 
-// Error codes written to err[0] by device code; err[1] holds the micro-step.
+// Error codes written to err[0] by device code; err[1] (and, where the step
+// kernel records it, err[2]) hold the micro-step.
 enum : int { kErrNone = 0, kErrBarrierTimeout = 1, kErrAborted = 2 };
 
 // How long a CTA waits at a grid barrier before it gives up (the host then

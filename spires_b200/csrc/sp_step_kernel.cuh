@@ -68,8 +68,13 @@ struct KP {
     const double *u;
     double *phi;
     unsigned *raster;
-    unsigned *bar;
-    int *err;
+    unsigned long long *bar;  // grid-barrier arrival counter (64-bit: never wraps)
+    int *err;                 // [0] error code, [1] / [2] low / high word of the micro-step
+    unsigned long long tmo;   // limit of every wait, ns
+    // one-shot test hook: CTA hold_cta does not arrive at the barrier that
+    // opens micro-step hold_b (-1: none), so every wait on it runs out
+    int hold_cta;
+    long long hold_b;
     // variant 1: 2-D tiled map of the ring [L rows][rs columns] of doubles,
     // box = BW columns x R rows
     alignas(64) CUtensorMap tmap;
@@ -150,8 +155,17 @@ __device__ __forceinline__ void fence_proxy_async()
 }
 
 // Bounded mbarrier wait; false on timeout or when the launch is aborting.
+__device__ __forceinline__ void record_err(int *err, int code, long long step)
+{
+    if (atomicCAS(err, kErrNone, code) == kErrNone) {
+        err[1] = (int)(unsigned)(unsigned long long)step;
+        err[2] = (int)(unsigned)((unsigned long long)step >> 32);
+    }
+}
+
 __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity,
-                                          volatile int *s_abort, int *err)
+                                          volatile int *s_abort, int *err,
+                                          unsigned long long tmo, long long step)
 {
     if (mbar_test(b, parity))
         return true;
@@ -161,8 +175,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
         if ((++polls & 63u) == 0) {
             if (*s_abort || ld_volatile_i32(err) != kErrNone)
                 return false;
-            if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-                atomicCAS(err, kErrNone, kErrBarrierTimeout);
+            if (globaltimer_ns() - t0 > tmo) {
+                record_err(err, kErrBarrierTimeout, step);
                 *s_abort = 1;
                 return false;
             }
@@ -311,8 +325,8 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                             ok = false;
                             break;
                         }
-                        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-                            atomicCAS(p.err, kErrNone, kErrBarrierTimeout);
+                        if (globaltimer_ns() - t0 > p.tmo) {
+                            record_err(p.err, kErrBarrierTimeout, g);
                             s_abort = 1;
                             ok = false;
                             break;
@@ -336,7 +350,8 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                     cnt = rh + 1;
                 const int y0 = rh - cnt + 1;
                 if (rounds > 0 &&
-                    !mbar_wait(&empty[st], (unsigned)((rounds - 1) & 1), &s_abort, p.err)) {
+                    !mbar_wait(&empty[st], (unsigned)((rounds - 1) & 1), &s_abort, p.err,
+                               p.tmo, g)) {
                     ok = false;
                     break;
                 }
@@ -361,7 +376,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         for (long long qq = (q > p.NST ? q - p.NST : 0); qq < q; ++qq) {
             const int st = (int)(qq % p.NST);
             while (!mbar_test(&full[st], (unsigned)((qq / p.NST) & 1))) {
-                if (globaltimer_ns() - t0 > kBarrierTimeoutNs)
+                if (globaltimer_ns() - t0 > p.tmo)
                     break;
             }
         }
@@ -450,11 +465,12 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         }
     };
 
-    auto barrier_arrive = [&]() {
+    // arrival at the barrier that opens micro-step b
+    auto barrier_arrive = [&](long long b) {
         named_sync(NC);
-        if (tid == 0 && p.G > 1) {
+        if (tid == 0 && p.G > 1 && !(b == p.hold_b && (int)blockIdx.x == p.hold_cta)) {
             __threadfence();
-            atomicAdd(p.bar, 1u);
+            atomicAdd(p.bar, 1ull);
         }
     };
     // returns false when the launch must stop
@@ -462,20 +478,19 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         if (tid == 0) {
             int ok = 1;
             if (p.G > 1) {
-                const unsigned target = (unsigned)(b + 1) * (unsigned)p.G;
-                if (ld_volatile_u32(p.bar) < target) {
+                const unsigned long long target =
+                    (unsigned long long)(b + 1) * (unsigned long long)p.G;
+                if (ld_volatile_u64(p.bar) < target) {
                     unsigned long long t0 = globaltimer_ns();
                     unsigned long long polls = 0;
-                    while (ld_volatile_u32(p.bar) < target) {
+                    while (ld_volatile_u64(p.bar) < target) {
                         if ((++polls & 255ull) == 0) {
                             if (ld_volatile_i32(p.err) != kErrNone) {
                                 ok = 0;
                                 break;
                             }
-                            if (globaltimer_ns() - t0 > kBarrierTimeoutNs ||
-                                polls > kBarrierMaxPolls) {
-                                if (atomicCAS(p.err, kErrNone, kErrBarrierTimeout) == kErrNone)
-                                    p.err[1] = (int)(p.step0 + b);
+                            if (globaltimer_ns() - t0 > p.tmo || polls > kBarrierMaxPolls) {
+                                record_err(p.err, kErrBarrierTimeout, p.step0 + b);
                                 ok = 0;
                                 break;
                             }
@@ -498,7 +513,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     // prologue: drive of micro-step 0, then arrive at barrier 0
     if (ST != SP_SYN_SIMPLE && ST != SP_SYN_PSC_HET)
         prepare(0, cur);
-    barrier_arrive();
+    barrier_arrive(0);
 
     for (long long b = 0; b < B; ++b) {
         const long long g = p.step0 + b;
@@ -553,7 +568,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                         cnt = rh + 1;
                     // on a failed wait the launch aborts at the next barrier_wait;
                     // every consumer keeps the same control flow until then
-                    const bool landed = mbar_wait(&full[cst], (unsigned)cph, &s_abort, p.err);
+                    const bool landed = mbar_wait(&full[cst], (unsigned)cph, &s_abort, p.err, p.tmo, g);
                     const double *buf = s_stage + (size_t)cst * STAGE + boff;
                     if (landed && act && integ) {
                         if ((cnt & 15) == 0) {
@@ -731,7 +746,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         if (b + 1 < B) {
             if (ST != SP_SYN_SIMPLE && ST != SP_SYN_PSC_HET)
                 prepare(b + 1, cur ^ 1);
-            barrier_arrive();
+            barrier_arrive(b + 1);
             if (VAR == 1 && tid == 0)
                 st_release_cta(&s_done, (int)(b + 1));
         }

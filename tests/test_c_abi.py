@@ -12,7 +12,11 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "spires_b200", "lib")
 SRC = os.path.join(ROOT, "tests", "c", "relink_check.c")
-REF_INCLUDE = "/root/reference/include"
+# the original project's sources, when present: SPIRES_REF_DIR, else a
+# checkout named `reference` beside this repository
+REF_DIR = os.environ.get("SPIRES_REF_DIR",
+                         os.path.abspath(os.path.join(ROOT, "..", "reference")))
+REF_INCLUDE = os.path.join(REF_DIR, "include")
 
 pytestmark = pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
 
@@ -50,7 +54,7 @@ def test_c_caller_against_the_original_header(tmp_path):
     build_and_run(REF_INCLUDE, tmp_path)
 
 
-REF_EXAMPLES = "/root/reference/examples"
+REF_EXAMPLES = os.path.join(REF_DIR, "examples")
 
 
 @pytest.mark.parametrize("name", ["mackey_glass_prediction", "spoken_digit_recognition"])
