@@ -444,9 +444,10 @@ def run_search_workload(args):
         out[name] = (r, ev.stats)
     plain = out["plain"][0]
     target = plain.best_loss + math.log(1.02)
+    tt = out["surrogate"][0].time_to(target)
     line = {"metric": "AGILE wall-clock to plain AGILE's best NRMSE (within 2%)",
-            "unit": "s", "higher_is_better": False,
-            "value": out["surrogate"][0].time_to(target),
+            "unit": "s", "higher_is_better": False, "value": tt,
+            "ratio_to_plain_wall": (tt / plain.wall_s) if tt is not None else None,
             "plain_wall_s": plain.wall_s, "plain_best_nrmse": plain.best_nrmse,
             "plain_time_to_best_s": plain.time_to(plain.best_loss)}
     for name in [a for a in ("surrogate", "no_surrogate") if a in out]:
@@ -454,11 +455,13 @@ def run_search_workload(args):
         line[name] = {"best_nrmse": r.best_nrmse, "wall_s": r.wall_s,
                       "time_to_target_s": r.time_to(target), "evals": r.evals,
                       "neuron_steps": st.neuron_steps, "build_s": st.build_s,
+                      "build_wait_s": st.build_wait_s,
                       "construct_s": st.construct_s, "setup_s": st.setup_s,
                       "surrogate_rmse_logNRMSE": r.extra.get("surrogate_rmse"),
                       "low_fidelity_rmse_logNRMSE": r.extra.get("low_fidelity_rmse")}
     line["plain_neuron_steps"] = out["plain"][1].neuron_steps
     line["plain_build_s"] = out["plain"][1].build_s
+    line["plain_build_wait_s"] = out["plain"][1].build_wait_s
     line["plain_construct_s"] = out["plain"][1].construct_s
     line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
                       "rungs": list(rungs), "points": points, "chains": chains, "waves": 8}
@@ -596,13 +599,19 @@ def run_small_lif_workload(args):
 
 def run_ridge_workload(args):
     """FLIF_GL N=4000 L=512 Watts-Strogatz k=10, Mackey-Glass T=20000,
-    washout 1000: the ridge readout with the FP64 Gram and with the split
-    tensor-core Grams, errors against the FP64 solution on the same states."""
+    washout 1000, lambda 1e-6: the Gram X^T X of the 19000 fitted states in
+    every mode (FP64 CUDA cores; INT8 integer slices, 7 and 8, on the tensor
+    cores; BF16X3 / TF32X3 splits), timed with CUDA events through
+    spires_ext_gram_device, its error against the FP64 Gram, then the ridge
+    readout solved from the FP64 and INT8 Grams, with W_out and NRMSE errors
+    against an FP64 numpy solve on the same states."""
     import numpy as np
+    import torch
 
     import spires_b200 as sp
     from spires_b200.datasets import mackey_glass
 
+    lib = sp.load()
     n, T, w, lam = 4000, 20000, 1000, 1e-6
     cfg = sp.make_config(n, 1, 1, rho=0.95, ei=0.5, gamma=0.5, conn=10.0 / (n - 1),
                          topo=sp.CONN_SMALL_WORLD, neuron=sp.FLIF_GL,
@@ -612,23 +621,68 @@ def run_ridge_workload(args):
     r = sp.Reservoir(cfg, seed=42)
     phi, _, _ = r.run_record(u, phi=True, raster=False)
     r.close()
+    tw = T - w
+    dX = torch.from_numpy(phi).cuda()
+    dC = torch.empty((n, n), dtype=torch.float64, device="cuda")
     peak, kind = bf16_peak()
-    rows = []
-    W64 = None
-    for mode in (0, 1, 2, 1, 2):
-        W, rep = sp.ridge_fit(phi, y, lam, washout=w, gram_mode=mode, max_refine=300)
-        yhat = phi[w:] @ W.T
-        nr = float(np.sqrt(np.mean((yhat[:, 0] - y[w:, 0]) ** 2)) / y[w:, 0].std())
-        if mode == 0:
-            W64, n64 = W, nr
-        fl = (3 if mode else 1) * 2.0 * (T - w) * n * n
-        rows.append({"gram_mode": mode, "gram_ms": rep.gram_ms,
-                     "gram_tflops": fl / rep.gram_ms / 1e9, "factor_ms": rep.factor_ms,
-                     "refine_ms": rep.refine_ms, "refine_iters": rep.refine_iters,
-                     "rel_residual": rep.rel_residual,
-                     "w_rel_err": float(np.linalg.norm(W - W64) / np.linalg.norm(W64)),
-                     "nrmse": nr, "nrmse_rel_err": abs(nr - n64) / n64})
-    best = min((x for x in rows[3:] if x["gram_mode"] == 1), key=lambda x: x["gram_ms"])
+
+    def gram(mode, slices=0, reps=3):
+        times = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st = lib.spires_ext_gram_device(C.c_void_p(dX.data_ptr()), T, n, w, mode, slices,
+                                            C.c_void_p(dC.data_ptr()), None)
+            e1.record()
+            torch.cuda.synchronize()
+            assert st == sp.SPIRES_OK, st
+            times.append(e0.elapsed_time(e1))
+        return float(np.median(times)), dC.clone()
+
+    ms64, G64 = gram(0)
+    g64n = torch.linalg.norm(G64).item()
+    fl64 = 2.0 * tw * n * n
+    n_pad = (n + 127) // 128 * 128
+    tiles = (n_pad // 128) * (n_pad // 128 + 1)
+    t_pad = (tw + 63) // 64 * 64
+    modes = [{"mode": "fp64", "gram_ms": ms64, "fp64_equiv_tflops": fl64 / ms64 / 1e9}]
+    int8 = None
+    for mode, slices, name in ((3, 7, "int8x7"), (3, 8, "int8x8"), (1, 0, "bf16x3"),
+                               (2, 0, "tf32x3")):
+        ms, G = gram(mode, slices)
+        nprod = slices * (slices + 1) // 2 if mode == 3 else 3
+        issued = 2.0 * 128 * 64 * t_pad * nprod * tiles
+        row = {"mode": name, "gram_ms": ms, "fp64_equiv_tflops": fl64 / ms / 1e9,
+               "issued_tops": issued / ms / 1e9,
+               "gram_rel_err_vs_fp64": torch.linalg.norm(G - G64).item() / g64n}
+        modes.append(row)
+        if name == "int8x7":
+            int8 = row
+    del dC
+
+    # ridge from the FP64 and the INT8 Gram, against an FP64 numpy solve
+    Xw = phi[w:]
+    A = Xw.T @ Xw
+    A[np.diag_indices(n)] += lam
+    Wnp = np.linalg.solve(A, Xw.T @ y[w:]).T
+
+    def nrmse(W):
+        yh = Xw @ W.T
+        return float(np.sqrt(np.mean((yh[:, 0] - y[w:, 0]) ** 2)) / y[w:, 0].std())
+
+    n_np = nrmse(Wnp)
+    fits = {}
+    for mode, name in ((0, "fp64"), (3, "int8x7")):
+        t0 = time.perf_counter()
+        W, rep = sp.ridge_fit(phi, y, lam, washout=w, gram_mode=mode, max_refine=30)
+        el = time.perf_counter() - t0
+        nr = nrmse(W)
+        fits[name] = {"ridge_s": el, "gram_ms": rep.gram_ms, "factor_ms": rep.factor_ms,
+                      "refine_ms": rep.refine_ms, "refine_iters": rep.refine_iters,
+                      "rel_residual": rep.rel_residual,
+                      "w_rel_err_vs_numpy_fp64": float(np.linalg.norm(W - Wnp) / np.linalg.norm(Wnp)),
+                      "nrmse": nr, "nrmse_rel_err_vs_numpy_fp64": abs(nr - n_np) / n_np}
     # spires_train_ridge end to end (reset, T steps recording states, ridge),
     # the library on the GPU against the reference on all host cores
     r = sp.Reservoir(cfg, seed=42)
@@ -638,32 +692,35 @@ def run_ridge_workload(args):
     Wg = r.readout()
     r.close()
     cpu = None
-    try:
-        from tests import _oracle as O
+    if not args.no_cpu_baseline:
+        try:
+            from tests import _oracle as O
 
-        threads = os.cpu_count() or 1
-        os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-        rr = sp.Reservoir(cfg, lib=O.ref_lib("openblas"), seed=42)
-        t0 = time.perf_counter()
-        rr.train_ridge(u, y, lam)
-        cpu_s = time.perf_counter() - t0
-        Wr = rr.readout()
-        rr.close()
-        cpu = {"value": cpu_s, "unit": "s", "cores": threads, "kind": "reference",
-               "sample": "reference spires_train_ridge, N=4000 T=20000 (OpenBLAS build)",
-               "w_rel_diff_vs_library": float(np.linalg.norm(Wg - Wr) / np.linalg.norm(Wr))}
-    except Exception as exc:  # the reference build is optional on a GPU host
-        cpu = {"unavailable": str(exc)[:200]}
-    line = {"metric": "ridge Gram TFLOP/s (BF16X3 split, issued flops)",
-            "value": best["gram_tflops"], "unit": "TFLOP/s",
-            "roofline": {"bound": "tensor", "achieved": best["gram_tflops"], "peak": peak,
-                         "unit": "TFLOP/s", "frac": best["gram_tflops"] / peak,
-                         "peak_kind": kind},
-            "modes": rows, "lambda": lam, "dtype": "bf16x3 / tf32x3 / f64",
-            "train_ridge_e2e": {"value": gpu_s, "unit": "s", "api": "spires_train_ridge"},
-            "cpu_baseline": cpu,
-            "data": "synthetic (seeded Mackey-Glass)",
-            "config": {"workload": "FLIF_GL N=4000 L=512 WS ridge, T=20000 washout 1000"}}
+            threads = os.cpu_count() or 1
+            os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+            rr = sp.Reservoir(cfg, lib=O.ref_lib("openblas"), seed=42)
+            t0 = time.perf_counter()
+            rr.train_ridge(u, y, lam)
+            cpu_s = time.perf_counter() - t0
+            Wr = rr.readout()
+            rr.close()
+            cpu = {"value": cpu_s, "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": "reference spires_train_ridge, N=4000 T=20000 (OpenBLAS build)",
+                   "w_rel_diff_vs_library": float(np.linalg.norm(Wg - Wr) / np.linalg.norm(Wr))}
+        except Exception as exc:  # the reference build is optional on a GPU host
+            cpu = {"unavailable": str(exc)[:200]}
+    int8_peak = 2.0 * peak
+    line = {"metric": "ridge Gram FP64-equivalent TFLOP/s (INT8 slices x7 on tensor cores)",
+            "value": int8["fp64_equiv_tflops"], "unit": "TFLOP/s",
+            "roofline": {"bound": "tensor", "achieved": int8["issued_tops"], "peak": int8_peak,
+                         "unit": "TOP/s (int8 issued)", "frac": int8["issued_tops"] / int8_peak,
+                         "peak_kind": f"2 x bf16 {kind} (dense int8 rate is twice bf16's)"},
+            "gram_modes": modes, "fits": fits, "numpy_fp64_nrmse": n_np, "lambda": lam,
+            "dtype": "int8 slices / f64", "train_ridge_e2e": {"value": gpu_s, "unit": "s",
+                                                              "api": "spires_train_ridge"},
+            "cpu_baseline": cpu, "data": "synthetic (seeded Mackey-Glass)",
+            "config": {"workload": "FLIF_GL N=4000 L=512 WS ridge, T=20000 washout 1000",
+                       "fitted_rows": tw}}
     print(json.dumps(line))
 
 

@@ -84,6 +84,8 @@ typedef struct {
     int variant;      /* 0 = generic, 1 = bulk-copy ring pipeline (FLIF_GL) */
     int stages;       /* pipeline stages (variant 1) */
     int rows;         /* ring rows per stage (variant 1) */
+    int csr_global;   /* 1: walk the recurrent CSR rows in global memory even
+                         when the CTA's slice fits in shared memory (0 default) */
 } spires_ext_launch;
 
 spires_status spires_ext_get_launch(const spires_reservoir *r, spires_ext_launch *l);
@@ -169,18 +171,29 @@ spires_status spires_ext_spectral_radius(size_t n, const int64_t *row_ptr, const
                                          const double *w, int on_device, double *out);
 
 /* ---- ridge readout with options ------------------------------------------ */
+/* The Gram X^T X of the fitted states (the reference forms it with one
+ * cblas_dgemm, src/math_utils.c:154-162) in one of four ways; X^T Y, the
+ * factorisation and the refinement residuals are FP64 in every mode. */
 typedef enum {
     SPIRES_EXT_GRAM_FP64 = 0,      /* FP64 Gram (CUDA cores) */
-    SPIRES_EXT_GRAM_BF16X3 = 1,    /* BF16 hi/lo split on tensor cores, FP32
-                                      accumulate, FP64 Cholesky + refinement */
-    SPIRES_EXT_GRAM_TF32X3 = 2     /* the same with TF32 hi/lo */
+    SPIRES_EXT_GRAM_BF16X3 = 1,    /* BF16 hi/lo split on the tensor cores
+                                      (hi hi + hi lo + lo hi), FP32 accumulate;
+                                      solved by Cholesky-preconditioned CG on
+                                      the FP64 operator */
+    SPIRES_EXT_GRAM_TF32X3 = 2,    /* the same with TF32 hi/lo */
+    SPIRES_EXT_GRAM_INT8 = 3       /* error-free integer slices on the tensor
+                                      cores (int8 digits, exact int32 sums per
+                                      digit level, FP64 combination): a Gram as
+                                      accurate as the FP64 one with 7 slices,
+                                      then FP64 Cholesky and refinement */
 } spires_ext_gram_mode;
 
 typedef struct {
     int    gram_mode;        /* spires_ext_gram_mode */
-    int    max_refine;       /* iterative-refinement sweeps (BF16X3) */
+    int    max_refine;       /* iterative-refinement sweeps */
     double refine_tol;       /* relative residual target */
     size_t washout;          /* leading rows excluded from the fit */
+    int    gram_slices;      /* SPIRES_EXT_GRAM_INT8: slices, 2..8 (0 = 7) */
 } spires_ext_ridge_opts;
 
 typedef struct {
@@ -193,6 +206,14 @@ typedef struct {
     int    dual;             /* 1: fewer fitted rows than N/2, solved as
                                 W = Phi^T (Phi Phi^T + lambda I)^-1 Y */
 } spires_ext_ridge_report;
+
+/* The Gram C = X^T X (d_C [n x n], full matrix) of device states
+ * d_X [T x n] over rows [t0, T) in any spires_ext_gram_mode (slices: the
+ * INT8 mode's slice count, 0 = 7); `stream` is a cudaStream_t (NULL = default);
+ * returns once the work on it has finished. Work memory is allocated on the
+ * device (stream-ordered) and freed before the call returns. */
+spires_status spires_ext_gram_device(const double *d_X, size_t T, size_t n, size_t t0,
+                                     int mode, int slices, double *d_C, void *stream);
 
 spires_status spires_ext_train_ridge(spires_reservoir *r, const double *input_series,
                                      const double *target_series, size_t series_length,

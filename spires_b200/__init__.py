@@ -80,12 +80,12 @@ class ModelInfo(C.Structure):
 
 class Launch(C.Structure):
     _fields_ = [("ctas", C.c_int), ("warps_max", C.c_int), ("variant", C.c_int),
-                ("stages", C.c_int), ("rows", C.c_int)]
+                ("stages", C.c_int), ("rows", C.c_int), ("csr_global", C.c_int)]
 
 
 class RidgeOpts(C.Structure):
     _fields_ = [("gram_mode", C.c_int), ("max_refine", C.c_int), ("refine_tol", C.c_double),
-                ("washout", C.c_size_t)]
+                ("washout", C.c_size_t), ("gram_slices", C.c_int)]
 
 
 class RidgeReport(C.Structure):
@@ -160,6 +160,8 @@ EXT_SIGNATURES = {
     "spires_ext_set_launch": (C.c_int, [_VP, C.POINTER(Launch)]),
     "spires_ext_autotune": (C.c_int, [_VP, C.c_size_t]),
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),
+    "spires_ext_gram_device": (C.c_int, [_VP, C.c_size_t, C.c_size_t, C.c_size_t, C.c_int,
+                                         C.c_int, _VP, _VP]),
     "spires_ext_set_wait_limit": (C.c_int, [_VP, C.c_double]),
     "spires_ext_last_device_error": (C.c_int, [_VP, C.POINTER(C.c_int),
                                               C.POINTER(C.c_longlong)]),

@@ -491,6 +491,7 @@ SPIRES_EXPORT spires_status spires_ext_get_launch(const spires_reservoir *r,
     l->variant = s.variant;
     l->stages = s.stages;
     l->rows = s.rows;
+    l->csr_global = s.csr_global;
     return SPIRES_OK;
 }
 
@@ -499,7 +500,7 @@ SPIRES_EXPORT spires_status spires_ext_set_launch(spires_reservoir *r,
 {
     if (!r || !r->dev || !l)
         return SPIRES_ERR_INVALID_ARG;
-    sp_launch s = {l->ctas, l->warps_max, l->variant, l->stages, l->rows};
+    sp_launch s = {l->ctas, l->warps_max, l->variant, l->stages, l->rows, l->csr_global != 0};
     return to_status(sp_dev_set_launch(r->dev, &s));
 }
 
@@ -713,6 +714,7 @@ SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
         o.max_refine = opts->max_refine;
         o.refine_tol = opts->refine_tol;
         o.washout = opts->washout;
+        o.gram_slices = opts->gram_slices;
     }
     if (o.washout >= series_length)
         return SPIRES_ERR_INVALID_ARG;
@@ -899,6 +901,7 @@ SPIRES_EXPORT spires_status spires_ext_batch_train_ridge(spires_ext_batch *b,
         o.max_refine = opts->max_refine;
         o.refine_tol = opts->refine_tol;
         o.washout = opts->washout;
+        o.gram_slices = opts->gram_slices;
     }
     for (size_t k = 0; k < b->count; ++k)
         if (!y[k] || o.washout >= T[k])
@@ -932,6 +935,7 @@ SPIRES_EXPORT spires_status spires_ext_batch_fit_predict(
         o.max_refine = opts->max_refine;
         o.refine_tol = opts->refine_tol;
         o.washout = opts->washout;
+        o.gram_slices = opts->gram_slices;
     }
     for (size_t k = 0; k < b->count; ++k)
         if (!y[k] || T_fit[k] > T[k] || o.washout >= T_fit[k])
@@ -1077,6 +1081,7 @@ SPIRES_EXPORT spires_status spires_ext_ridge_fit(const double *states, size_t T,
         o.max_refine = opts->max_refine;
         o.refine_tol = opts->refine_tol;
         o.washout = opts->washout;
+        o.gram_slices = opts->gram_slices;
     }
     if (o.washout >= T)
         return SPIRES_ERR_INVALID_ARG;

@@ -946,8 +946,17 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
     {
         auto tg = std::chrono::steady_clock::now();
         int mode = o->gram_mode;
-        if ((mode == 1 || mode == 2) && sp_gram_bf16x3_available()) {
-            rc = sp_gram_split(s, mode, Phi, n, w0, T, A, n);
+        const int slices = o->gram_slices > 0 ? o->gram_slices : SP_GRAM_INT8_SLICES;
+        if ((mode == SP_GRAM_BF16X3 || mode == SP_GRAM_TF32X3 || mode == SP_GRAM_INT8) &&
+            sp_gram_tc_available()) {
+            rc = sp_gram_tc(s, mode, slices, Phi, n, w0, T, A, n);
+            if (rc == SP_EINVAL && mode == SP_GRAM_INT8) {
+                // a state that is not finite: the FP64 Gram, as the reference
+                rc = SP_OK;
+                mode = 0;
+                const int nt = (n + 63) / 64;
+                k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(Phi, n, w0, T, A, n);
+            }
             if (rc)
                 goto out;
         } else {
@@ -967,7 +976,9 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
         rep->gram_ms = ms_since(tg);
     }
 
-    if (rep->gram_mode_used != 0) {
+    if (rep->gram_mode_used == SP_GRAM_BF16X3 || rep->gram_mode_used == SP_GRAM_TF32X3) {
+        // an FP32-accumulated Gram is too coarse to factor directly at small
+        // lambda: Cholesky-preconditioned CG on the FP64 operator
         rc = ridge_mixed(s, Phi, n, T, w0, Y, dout, lambda, rep->gram_mode_used, o, rep, A, B, W,
                          R, E, part, parts, tmp, info);
         if (rc)
@@ -989,7 +1000,9 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
             rep->lu_fallback = 1;
             RK(cudaMemsetAsync(info, 0, sizeof(int), s));
             if (rep->gram_mode_used != 0) {
-                rc = sp_gram_split(s, rep->gram_mode_used, Phi, n, w0, T, A, n);
+                rc = sp_gram_tc(s, rep->gram_mode_used,
+                                o->gram_slices > 0 ? o->gram_slices : SP_GRAM_INT8_SLICES, Phi,
+                                n, w0, T, A, n);
                 if (rc)
                     goto out;
             } else {
@@ -1046,6 +1059,14 @@ out:
         if (b)
             sp_cuda_free(b);
     return rc;
+}
+
+extern "C" int sp_gram_fp64(cudaStream_t s, const double *X, int n, size_t t0, size_t t1,
+                            double *C, int ldc)
+{
+    const int nt = (n + 63) / 64;
+    k_syrk_f64<<<nt * (nt + 1) / 2, 256, 0, s>>>(X, n, t0, t1, C, ldc);
+    return cudaGetLastError() == cudaSuccess ? SP_OK : SP_EINTERNAL;
 }
 
 // Ridge on states already on the device: Phi [T x n] row-major (neuron order),

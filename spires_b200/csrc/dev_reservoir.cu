@@ -255,6 +255,37 @@ static void box_geometry(const sp_launch &l, int *bw, int *nbx)
     *nbx = (sw + *bw - 1) / *bw;
 }
 
+// SIMPLE synapse: the CTA's CSR slice (position-space row offsets, column
+// positions, weights) is copied to shared memory at the start of a launch
+// when its largest slice has at most kCsrSmemEdges edges, so the row pass
+// after each grid barrier reads no global memory. Returns the edge capacity
+// to reserve (0: rows are walked from global memory).
+constexpr long long kCsrSmemEdges = 2048;
+
+static long long csr_smem_edges(const sp_dev *d, const sp_launch &l)
+{
+    if (d->stype != SP_SYN_SIMPLE || !d->h_row_ptr || l.ctas < 1 || l.csr_global)
+        return 0;
+    const long long nw = (long long)d->nwords;
+    long long mx = 0;
+    for (long long b = 0; b < l.ctas; ++b) {
+        const long long w0 = b * nw / l.ctas, w1 = (b + 1) * nw / l.ctas;
+        const long long e = d->h_row_ptr[32 * w1] - d->h_row_ptr[32 * w0];
+        if (e > mx)
+            mx = e;
+    }
+    return mx <= kCsrSmemEdges ? (mx > 0 ? mx : 1) : 0;
+}
+
+static size_t csr_smem_bytes(long long cap, int warps_max)
+{
+    if (cap <= 0)
+        return 0;
+    const size_t rows = 32 * (size_t)warps_max + 1;
+    return ((size_t)cap * 8 + 127) / 128 * 128 + ((size_t)cap * 4 + 127) / 128 * 128 +
+           (rows * 4 + 127) / 128 * 128;
+}
+
 // variant 1 stages the coefficient table in shared memory up to 64 KB
 static size_t coef_smem_bytes(const sp_dev *d)
 {
@@ -266,7 +297,8 @@ static size_t coef_smem_bytes(const sp_dev *d)
 // ring-row stages and their full/empty mbarriers
 static size_t launch_smem(const sp_dev *d, const sp_launch &l)
 {
-    size_t spk = ((d->nwords * 4) + 127) & ~(size_t)127;
+    size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) +
+                 csr_smem_bytes(csr_smem_edges(d, l), l.warps_max);
     if (l.variant == 1) {
         int bw, nbx;
         box_geometry(l, &bw, &nbx);
@@ -346,7 +378,8 @@ static void default_launch(sp_dev *d)
             box_geometry(v, &bw, &nbx);
             const size_t stage = (size_t)v.rows * nbx * bw * sizeof(double);
             const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
-            const size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d);
+            const size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d) +
+                               csr_smem_bytes(csr_smem_edges(d, v), v.warps_max);
             long long st = budget > spk ? (long long)((budget - spk) / (stage + 16)) : 0;
             if (st > 16)
                 st = 16;
@@ -489,6 +522,10 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         TRY(dalloc(&d->bar, 4));
         TRY(dalloc(&d->err, 4));
         TRY(dupload(&d->row_ptr, rp.data(), rs + 1, s));
+        d->h_row_ptr = (long long *)malloc((rs + 1) * sizeof(long long));
+        if (!d->h_row_ptr)
+            TRY(SP_EALLOC);
+        memcpy(d->h_row_ptr, rp.data(), (rs + 1) * sizeof(long long));
         TRY(dupload(&d->col, col.data(), m->nnz, s));
         TRY(dupload(&d->w, w.data(), m->nnz, s));
         TRY(dupload(&d->W_in, win.data(), rs * din, s));
@@ -575,6 +612,7 @@ extern "C" void sp_dev_destroy(sp_dev *d)
             sp_cuda_free(b);
     if (d->stream)
         cudaStreamDestroy(d->stream);
+    free(d->h_row_ptr);
     free(d);
 }
 
@@ -618,6 +656,20 @@ static int check_err(sp_dev *d)
     }
     return SP_OK;
 }
+
+#ifdef SP_PHASE_STAMPS
+// Debug builds only: the phase stamps of the last launch (see SP_STAMP).
+extern "C" __attribute__((visibility("default"))) int spires_dbg_phase_stamps(void *host,
+                                                                             size_t bytes)
+{
+    if (bytes < sizeof(g_sp_stamps))
+        return -1;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpyFromSymbol(host, g_sp_stamps, sizeof(g_sp_stamps)) != cudaSuccess)
+        return -1;
+    return 0;
+}
+#endif
 
 extern "C" int sp_dev_set_wait_limit(sp_dev *d, double ms)
 {
@@ -710,6 +762,7 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     d->hold_cta = -1;
     d->hold_b = -1;
     p.nid_of = d->nid_of;
+    p.csr_cap = (int)csr_smem_edges(d, l);
 
     kfn_t fn = pick_kernel(d->ntype, d->stype, l.variant);
     if (!fn)
@@ -1079,7 +1132,9 @@ extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
                 int bw, nbx;
                 box_geometry(v, &bw, &nbx);
                 const size_t stage = (size_t)rows * nbx * bw * 8;
-                const size_t base = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d);
+                const size_t base = (((d->nwords * 4) + 127) & ~(size_t)127) +
+                                    coef_smem_bytes(d) +
+                                    csr_smem_bytes(csr_smem_edges(d, v), v.warps_max);
                 const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
                 long long st = budget > base ? (long long)((budget - base) / (stage + 16)) : 0;
                 if (st > 16)

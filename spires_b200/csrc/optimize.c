@@ -809,5 +809,7 @@ int sp_default_gram_mode(void)
         return 1;
     if (e && (!strcmp(e, "tf32x3") || !strcmp(e, "2")))
         return 2;
+    if (e && (!strcmp(e, "int8") || !strcmp(e, "3")))
+        return 3;
     return 0;
 }

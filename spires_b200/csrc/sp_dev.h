@@ -27,6 +27,8 @@ typedef struct {
     int variant;     /* 0 = generic ring loads, 1 = bulk-copy ring pipeline (FLIF_GL) */
     int stages;      /* pipeline depth of variant 1 */
     int rows;        /* ring rows per stage of variant 1 */
+    int csr_global;  /* 1: SIMPLE synapse rows walked in global memory even when
+                        the CTA's CSR slice fits in shared memory */
 } sp_launch;
 
 int  sp_dev_create(const sp_host_model *m, sp_dev **out);
@@ -88,10 +90,11 @@ long long sp_dev_kernel_launches(const sp_dev *d);
 
 /* Readouts on the device (dev_readout.cu). */
 typedef struct {
-    int gram_mode;      /* 0 = FP64 Gram, 1 = BF16x3 split tensor-core Gram */
-    int max_refine;     /* iterative-refinement sweeps (mode 1) */
+    int gram_mode;      /* SP_GRAM_*: 0 FP64 Gram, 1 BF16X3, 2 TF32X3, 3 INT8 slices */
+    int max_refine;     /* iterative-refinement sweeps */
     double refine_tol;  /* stop when ||r|| / ||b|| falls below */
     size_t washout;     /* rows of phi skipped before the Gram */
+    int gram_slices;    /* INT8 mode: integer slices (2..8), 0 = default (7) */
 } sp_ridge_opts;
 
 typedef struct {

@@ -47,6 +47,7 @@ struct sp_dev {
     double *scoef, *Iring;
     double *mx_decay, *mx_omd, *mx_c, *mx_tr;
     double *W_in, *W_out;  // rows / columns in position order
+    long long *h_row_ptr;  // host copy of row_ptr [rs + 1] (launch planning)
     int *pos_of;           // [n] position of neuron i
     int *nid_of;           // [rs] neuron at position q, or -1
 

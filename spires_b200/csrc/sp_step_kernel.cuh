@@ -38,6 +38,8 @@ struct KP {
     int BW, NBX;    // variant 1: box width (neurons) and boxes side by side per stage
     int RB;         // variant 1: rows per box = min(R, L)
     int coef_smem;  // variant 1: coefficient table staged in shared memory
+    int csr_cap;    // SIMPLE synapse: edges of the CTA's CSR slice kept in shared
+                    // memory for the launch (0: rows are walked in global memory)
     const int *nid_of;  // neuron at each position, -1 for an empty lane
     long long step0, syn_step0;
     double a, b, c, d, e, f, g, h, ci, cj, ck, cl, dt;
@@ -231,6 +233,62 @@ __device__ __forceinline__ double rowpass_simple_warp(const long long *__restric
     return acc;
 }
 
+// Per-phase timing of the last kSpStampSteps micro-steps of a launch
+// (compiled in only with -DSP_PHASE_STAMPS): thread 0 of each CTA records the
+// global timer at the phase boundaries of every step into g_sp_stamps
+// [cta][step][phase]; spires_dbg_phase_stamps (dev_reservoir.cu) copies them
+// out. Phases: 0 step start, 1 history summed, 2 barrier passed, 3 spike
+// words staged, 4 row pass done (warp 0), 5 update and spike word done,
+// 6 arrival made; 7 the producer issued the step's first stage.
+#ifdef SP_PHASE_STAMPS
+constexpr int kSpStampCtas = 160, kSpStampSteps = 32, kSpStampPhases = 8;
+__device__ unsigned long long g_sp_stamps[kSpStampCtas * kSpStampSteps * kSpStampPhases];
+#define SP_STAMP(cond, b, B, ph)                                                             \
+    do {                                                                                    \
+        if ((cond) && blockIdx.x < kSpStampCtas && (b) >= (B)-kSpStampSteps)                \
+            g_sp_stamps[((size_t)blockIdx.x * kSpStampSteps + ((b) - ((B)-kSpStampSteps))) * \
+                            kSpStampPhases +                                                \
+                        (ph)] = globaltimer_ns();                                           \
+    } while (0)
+#else
+#define SP_STAMP(cond, b, B, ph) \
+    do {                         \
+    } while (0)
+#endif
+
+// The same walk over the CTA's CSR slice in shared memory: rp = row offsets
+// relative to the slice (rows of the CTA in position order), col = column
+// positions, w = weights. Same terms, same order.
+__device__ __forceinline__ double rowpass_simple_smem(const int *rp, const int *col,
+                                                      const double *w, const unsigned *s_spk,
+                                                      int row0, int lane)
+{
+    const int e0 = rp[row0], e1 = rp[row0 + 32];
+    const int my_end = rp[row0 + lane + 1];
+    double acc = 0.0;
+    for (int base = e0; base < e1; base += 32) {
+        const int e = base + lane;
+        int c = -1;
+        double wv = 0.0;
+        if (e < e1) {
+            c = col[e];
+            wv = w[e];
+        }
+        const bool s = c >= 0 && ((s_spk[c >> 5] >> (c & 31)) & 1u);
+        unsigned m = __ballot_sync(kFull, s);
+        while (m) {
+            const int bpos = __ffs(m) - 1;
+            m &= m - 1;
+            const int eb = base + bpos;
+            const double wb = __shfl_sync(kFull, wv, bpos);
+            const unsigned owner = __ballot_sync(kFull, my_end > eb);
+            if (lane == __ffs(owner) - 1)
+                acc = add(acc, wb);
+        }
+    }
+    return acc;
+}
+
 template <int R>
 __device__ __forceinline__ double stage_sum(double hist, const double *coef_k, const double *buf,
                                             int bw)
@@ -272,7 +330,18 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     const long long B = (long long)p.n_macro * p.micro;
 
     unsigned *s_spk = (unsigned *)smem;
-    const size_t spk_bytes = (((size_t)p.nwords * 4) + 127) & ~(size_t)127;
+    const size_t spk_bytes0 = (((size_t)p.nwords * 4) + 127) & ~(size_t)127;
+    // CSR slice (SIMPLE synapse), between the spike words and the rest
+    double *s_csr_w = (double *)(smem + spk_bytes0);
+    const size_t csr_w_bytes = ((size_t)p.csr_cap * 8 + 127) / 128 * 128;
+    int *s_csr_col = (int *)(smem + spk_bytes0 + csr_w_bytes);
+    const size_t csr_c_bytes = ((size_t)p.csr_cap * 4 + 127) / 128 * 128;
+    int *s_csr_rp = (int *)(smem + spk_bytes0 + csr_w_bytes + csr_c_bytes);
+    const size_t csr_bytes =
+        p.csr_cap > 0 ? csr_w_bytes + csr_c_bytes +
+                            (((size_t)32 * p.warps + 1) * 4 + 127) / 128 * 128
+                      : 0;
+    const size_t spk_bytes = spk_bytes0 + csr_bytes;
     const size_t coef_bytes = p.coef_smem ? (((size_t)L * 8) + 127) & ~(size_t)127 : 0;
     double *s_coef = (double *)(smem + spk_bytes);
     double *s_stage = (double *)(smem + spk_bytes + coef_bytes);
@@ -290,6 +359,16 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     if (VAR == 1 && p.coef_smem)
         for (int k = tid; k < L; k += blockDim.x)
             s_coef[k] = p.coef[k];
+    if (ST == SP_SYN_SIMPLE && p.csr_cap > 0) {
+        const long long e_lo = __ldg(p.row_ptr + lo);
+        const int ne = (int)(__ldg(p.row_ptr + lo + S_b) - e_lo);  // <= csr_cap
+        for (int k = tid; k < ne; k += blockDim.x) {
+            s_csr_col[k] = __ldg(p.col + e_lo + k);
+            s_csr_w[k] = __ldg(p.w + e_lo + k);
+        }
+        for (int q = tid; q <= S_b; q += blockDim.x)
+            s_csr_rp[q] = (int)(__ldg(p.row_ptr + lo + q) - e_lo);
+    }
     if (VAR == 1) {
         if (tid == 0) {
             for (int s = 0; s < p.NST; ++s) {
@@ -339,6 +418,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             }
             // lags k..k+cnt-1 are rows rh down to rh-cnt+1: one contiguous
             // ascending row range per stage (split at the wrap)
+            SP_STAMP(true, b, B, 7);
             int rh = (int)(g % L) - 2;
             if (rh < 0)
                 rh += L;
@@ -517,6 +597,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
 
     for (long long b = 0; b < B; ++b) {
         const long long g = p.step0 + b;
+        SP_STAMP(tid == 0, b, B, 0);
         const int s = (int)(b / p.micro);
         const int m = (int)(b % p.micro);
         if (m == 0) {
@@ -602,20 +683,27 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         }
 
         // ---- barrier: spikes / eff of step g-1 are visible
+        SP_STAMP(tid == 0, b, B, 1);
         if (!barrier_wait(b))
             return;
+        SP_STAMP(tid == 0, b, B, 2);
         if (ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET) {
             for (int wi = tid; wi < p.nwords; wi += NC)
                 s_spk[wi] = __ldcg(p.spk + (size_t)cur * p.nwords + wi);
             named_sync(NC);
         }
+        SP_STAMP(tid == 0, b, B, 3);
 
         // ---- recurrent input
         double rec = 0.0;
         if (ST == SP_SYN_SIMPLE) {
             if (wact) {
                 // CSR rows are in position order; holes are empty rows
-                rec = rowpass_simple_warp(p.row_ptr, p.col, p.w, s_spk, gw * 32, 32, lane);
+                if (p.csr_cap > 0)
+                    rec = rowpass_simple_smem(s_csr_rp, s_csr_col, s_csr_w, s_spk,
+                                              (gw - wb0) * 32, lane);
+                else
+                    rec = rowpass_simple_warp(p.row_ptr, p.col, p.w, s_spk, gw * 32, 32, lane);
             }
         } else if (act) {
             const long long k0 = __ldg(p.row_ptr + i), k1 = __ldg(p.row_ptr + i + 1);
@@ -637,6 +725,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             }
         }
 
+        SP_STAMP(tid == 0, b, B, 4);
         // ---- neuron update (operation order of src/neurons/<model>.c)
         bool fired = false;
         if (act) {
@@ -737,6 +826,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             p.spk[(size_t)(cur ^ 1) * p.nwords + gw] = word;
         lastword = word;
         sprev = fired ? 1.0 : 0.0;
+        SP_STAMP(tid == 0, b, B, 5);
         if (m == p.micro - 1) {
             if (act && p.phi)
                 p.phi[(size_t)s * p.rs + i] = V;
@@ -750,6 +840,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             if (VAR == 1 && tid == 0)
                 st_release_cta(&s_done, (int)(b + 1));
         }
+        SP_STAMP(tid == 0, b, B, 6);
         cur ^= 1;
     }
 

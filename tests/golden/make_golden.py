@@ -11,8 +11,12 @@ Fixtures (all small):
                        (bit-packed), final membrane potentials, sha256 of the
                        state trajectory, readouts of spires_run
   long_horizon.npz  -- FLIF_GL reservoirs run for thousands of steps: sha256
-                       of the spike raster of every 500-step block and of the
-                       final state (full-horizon raster parity)
+                       of the spike raster of every 500-step block, the first
+                       32 bits of the sha256 of every step's raster row (so a
+                       mismatch is located to its step) and the sha256 of the
+                       final state (full-horizon raster parity). The N=20000,
+                       L=1024 pin covers the ring fill (1032 steps) plus
+                       25 launches of 256 steps: 7432 steps.
 Inputs are regenerated from their seeds by spires_b200.datasets / numpy; the
 sha256 of each input series is stored and checked before use.
 """
@@ -100,7 +104,7 @@ def make_small(ref):
 # long-horizon FLIF_GL pins: (name, n, L, topo, conn, din, rho, alpha, T, seed)
 LONG = [
     ("gl_n4000_l512_ws", 4000, 512, 1, 10 / 3999, 1, 0.95, 0.7, 20000, 42),
-    ("gl_n20000_l1024_ba", 20000, 1024, 2, 5 / 19999, 13, 0.9, 0.6, 1200, 1234),
+    ("gl_n20000_l1024_ba", 20000, 1024, 2, 5 / 19999, 13, 0.9, 0.6, 1032 + 25 * 256, 1234),
 ]
 BLOCK = 500
 
@@ -120,6 +124,11 @@ def long_inputs(c):
     return np.ascontiguousarray(np.concatenate(seqs, axis=0)[:T])
 
 
+def step_hash(packed_row):
+    """First 32 bits of the sha256 of one step's bit-packed raster row."""
+    return np.uint32(int(hashlib.sha256(packed_row.tobytes()).hexdigest()[:8], 16))
+
+
 def make_long(ref):
     out = {}
     for c in LONG:
@@ -131,11 +140,13 @@ def make_long(ref):
         spk = np.empty(n)
         ras = np.empty((BLOCK, n), np.uint8)
         hashes = []
+        steps = np.empty(T, np.uint32)
         rate = 0.0
         for t in range(T):
             r.step(u[t])
             r.lib.spires_read_spike_state(r.h, sp.dptr(spk))
             ras[t % BLOCK] = spk != 0.0
+            steps[t] = step_hash(np.packbits(ras[t % BLOCK]))
             if (t + 1) % BLOCK == 0 or t + 1 == T:
                 m = (t % BLOCK) + 1
                 blk = np.packbits(ras[:m], axis=1)
@@ -145,6 +156,7 @@ def make_long(ref):
         r.close()
         out[name + ":u_sha"] = np.array(sha(u))
         out[name + ":block_sha"] = np.array(hashes)
+        out[name + ":step_hash"] = steps
         out[name + ":V_final_sha"] = np.array(sha(V))
         out[name + ":V_final_head"] = V[:64]
         print(f"{name}: T={T} rate={rate / (T * n):.4f} ({time.time() - t0:.1f}s)")

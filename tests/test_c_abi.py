@@ -23,8 +23,8 @@ pytestmark = pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compil
 
 CUDA_LIB = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64")
 # the static archive's extra libraries, as the integration notes give them
-STATIC = [os.path.join(LIB, "libspires.a"), "-L" + CUDA_LIB, "-lcudart_static", "-lcublas",
-          "-Wl,-rpath," + CUDA_LIB, "-lstdc++", "-fopenmp", "-lpthread", "-ldl", "-lrt", "-lm"]
+STATIC = [os.path.join(LIB, "libspires.a"), "-L" + CUDA_LIB, "-lcudart_static",
+          "-lstdc++", "-fopenmp", "-lpthread", "-ldl", "-lrt", "-lm"]
 
 
 def build_and_run(include_dir, tmp_path, static=False):

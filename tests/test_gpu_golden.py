@@ -1,7 +1,7 @@
 """The CUDA library against the golden fixtures generated from the reference
 compiled from source: small cases bit for bit, and the FP64 FLIF_GL
 configurations over their full horizon (spike-raster sha256 per 500-step block
-and the final state)."""
+and per step, so that a mismatch names its step, and the final state)."""
 import hashlib
 import os
 
@@ -49,13 +49,19 @@ def test_full_horizon_rasters_match_golden(case):
     assert sha(u) == str(LONG[name + ":u_sha"])
     r = sp.Reservoir(cfg, seed=seed)
     hashes = []
+    steps = np.empty(T, np.uint32)
     for b0 in range(0, T, G.BLOCK):
         _, R, _ = r.run_record(u[b0:b0 + G.BLOCK], phi=False)
-        hashes.append(sha(np.packbits(sp.unpack_raster(R, n), axis=1)))
+        packed = np.packbits(sp.unpack_raster(R, n), axis=1)
+        hashes.append(sha(packed))
+        for j in range(packed.shape[0]):
+            steps[b0 + j] = G.step_hash(packed[j])
     V = r.state()
     r.close()
     want = [str(h) for h in LONG[name + ":block_sha"]]
-    bad = [i for i, (a, b) in enumerate(zip(hashes, want)) if a != b]
-    assert not bad, f"first differing 500-step block: {bad[0]} (steps {bad[0] * G.BLOCK}..)"
+    assert len(want) == len(hashes)
+    bad = np.flatnonzero(steps != LONG[name + ":step_hash"])
+    assert bad.size == 0, f"first step whose spike raster differs: {int(bad[0])} (of {T})"
+    assert hashes == want
     assert np.array_equal(V[:64], LONG[name + ":V_final_head"])
     assert sha(V) == str(LONG[name + ":V_final_sha"])

@@ -62,3 +62,57 @@ def test_split_gram_small_lambda_stated_error(mode):
           f"refine {rep.refine_iters}, residual {rep.rel_residual:.1e}")
     # ill-conditioned: the readout's NRMSE must still agree to 1 %
     assert np.isfinite(nr) and abs(nr - n64) <= 1e-2 * n64
+
+
+@pytest.mark.parametrize("lam", [1e-3, 1e-6])
+def test_int8_gram_ridge_is_the_fp64_ridge(lam):
+    """INT8 integer-slice Gram (7 slices): as accurate as the FP64 Gram, so the
+    same FP64 Cholesky and refinement give the FP64 path's solution."""
+    W64, n64, r64 = fit(0, lam)
+    W, nr, rep = fit(3, lam)
+    assert rep.gram_mode_used == 3 and r64.gram_mode_used == 0
+    werr = np.linalg.norm(W - W64) / np.linalg.norm(W64)
+    print(f"int8 lambda {lam:g}: W rel err {werr:.2e}, NRMSE {nr:.9f} vs {n64:.9f}, "
+          f"refine {rep.refine_iters} (fp64 {r64.refine_iters}), residual "
+          f"{rep.rel_residual:.1e} (fp64 {r64.rel_residual:.1e})")
+    assert rep.factor_failed == 0
+    assert rep.rel_residual <= max(10 * r64.rel_residual, 1e-12)
+    assert werr < (1e-8 if lam >= 1e-3 else 1e-4)
+    assert abs(nr - n64) <= 1e-8 * n64
+
+
+def test_int8_gram_ridge_at_full_size_against_fp64():
+    """FLIF_GL N=4000, L=512, Watts-Strogatz k=10, Mackey-Glass T=20000,
+    washout 1000, lambda 1e-6: W_out and NRMSE of the INT8-Gram ridge and of
+    the FP64-Gram ridge, each against an FP64 solve (numpy, LAPACK) of the
+    same normal equations on the same states. Stated, and bounded by the
+    FP64-Gram path's own distance to that solve."""
+    n, T, w, lam = 4000, 20000, 1000, 1e-6
+    cfg = sp.make_config(n, 1, 1, rho=0.95, ei=0.5, gamma=0.5, conn=10.0 / (n - 1),
+                         topo=sp.CONN_SMALL_WORLD, neuron=sp.FLIF_GL,
+                         nparams=(1.0, 0.0, 0.0, 20.0, 0.7, 512.0, 0.1, 2.0))
+    x = mackey_glass(T + 1, seed=0)
+    u, y = np.ascontiguousarray(x[:-1, None]), np.ascontiguousarray(x[1:, None])
+    r = sp.Reservoir(cfg, seed=42)
+    phi, _, _ = r.run_record(u, phi=True, raster=False)
+    r.close()
+    Xw = phi[w:]
+    A = Xw.T @ Xw
+    A[np.diag_indices(n)] += lam
+    Wnp = np.linalg.solve(A, Xw.T @ y[w:]).T
+
+    def nrmse(W):
+        e = Xw @ W.T - y[w:]
+        return float(np.sqrt(np.mean(e * e)) / y[w:, 0].std())
+
+    out = {}
+    for mode in (0, 3):
+        W, rep = sp.ridge_fit(phi, y, lam, washout=w, gram_mode=mode, max_refine=30)
+        out[mode] = (float(np.linalg.norm(W - Wnp) / np.linalg.norm(Wnp)),
+                     abs(nrmse(W) - nrmse(Wnp)) / nrmse(Wnp), rep.refine_iters,
+                     rep.rel_residual, rep.gram_ms)
+        print(f"mode {mode}: W rel err vs numpy FP64 {out[mode][0]:.2e}, NRMSE rel err "
+              f"{out[mode][1]:.2e}, refine {out[mode][2]}, residual {out[mode][3]:.1e}, "
+              f"Gram {out[mode][4]:.1f} ms")
+    assert out[3][0] <= max(2 * out[0][0], 1e-6)
+    assert out[3][1] <= max(2 * out[0][1], 1e-9)
