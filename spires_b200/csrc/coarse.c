@@ -2,9 +2,10 @@
  * coarse.c -- spires_coarse_grain (src/reservoir.c:782-967, src/spires_api.c:226-245).
  *
  * Pair-merging of neurons joined by a strong weight, repeated until a full
- * pass merges nothing, then a new reservoir over the survivors. This is a
- * one-shot, O(n^2)-per-pass host algorithm in the reference and stays on the
- * host here; the new reservoir gets its own device state. As in the reference
+ * pass merges nothing, then a new reservoir over the survivors. The merge
+ * loop runs on the device (dev_coarse.cu, bit-identical to the reference's
+ * loop); the dense matrices are assembled and compacted here and the new
+ * reservoir gets its own device state. As in the reference
  * the merged matrix is installed without a spectral rescale and without new
  * W_in/W_out draws (PSC_HETEROGENEOUS still draws per-edge tau for it).
  */
@@ -56,39 +57,12 @@ SPIRES_EXPORT spires_status spires_coarse_grain(const spires_reservoir *r, doubl
     for (size_t i = 0; i < n; i++)
         alive[i] = 1;
 
-    int merged = 1;
-    while (merged) {
-        merged = 0;
-        for (size_t i = 0; i < n; i++) {
-            for (size_t j = i + 1; j < n; j++) {
-                if (W[i * n + j] <= weight_threshold && W[j * n + i] <= weight_threshold)
-                    continue;
-                merged = 1;
-                V[i] = (V[i] + V[j]) / 2.0;
-                V[j] = 0.0;
-                alive[j] = 0;
-                for (size_t k = 0; k < n; k++) {
-                    if (k == i || k == j)
-                        continue;
-                    double a = W[i * n + k], b = W[j * n + k];
-                    double nw = (a * b == 0.0) ? a + b : (a + b) / 2.0;
-                    W[i * n + k] = nw;
-                    W[k * n + i] = nw;
-                }
-                for (size_t k = 0; k < nin; k++) {
-                    double a = Win[i * nin + k], b = Win[j * nin + k];
-                    Win[i * nin + k] = (a * b == 0.0) ? a + b : (a + b) / 2.0;
-                    Win[j * nin + k] = 0.0;
-                }
-                for (size_t o = 0; o < nout; o++) {
-                    Wout[o * n + i] += Wout[o * n + j];
-                    Wout[o * n + j] = 0.0;
-                }
-                for (size_t k = 0; k < n; k++) {
-                    W[j * n + k] = 0.0;
-                    W[k * n + j] = 0.0;
-                }
-            }
+    /* the merge loop (src/reservoir.c:822-915) runs on the device */
+    {
+        int rc0 = sp_coarse_merge_device(n, nin, nout, weight_threshold, W, Win, Wout, V, alive);
+        if (rc0) {
+            st = (rc0 == SP_EALLOC) ? SPIRES_ERR_ALLOC : SPIRES_ERR_INTERNAL;
+            goto done;
         }
     }
 

@@ -88,6 +88,11 @@ int  sp_dev_state_check(sp_dev *d, const void *buf);
 size_t sp_dev_nwords(const sp_dev *d);
 long long sp_dev_kernel_launches(const sp_dev *d);
 
+/* Merge loop of spires_coarse_grain on the device (dev_coarse.cu), in place
+ * on host arrays W [n][n], Win [n][nin], Wout [nout][n], V [n], alive [n]. */
+int sp_coarse_merge_device(size_t n, size_t nin, size_t nout, double thr, double *W,
+                           double *Win, double *Wout, double *V, int *alive);
+
 /* Readouts on the device (dev_readout.cu). */
 typedef struct {
     int gram_mode;      /* SP_GRAM_*: 0 FP64 Gram, 1 BF16X3, 2 TF32X3, 3 INT8 slices */
