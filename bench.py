@@ -393,6 +393,8 @@ def run_sweep_workload(args):
     build_s = time.perf_counter() - t0
     us, ys = sweep.series_for(insts)
     ns = float(sum(i.n * i.T for i in insts))
+    # the autotuner picks the schedule on the first 400 steps of every series
+    tuned = b.autotune([u[:400] for u in us])
     b.run(us, rasters=False, states=False)  # warm-up (plans, captures the graph)
     times = [b.run(us, rasters=False, states=False)[2] for _ in range(max(1, args.steps // 10))]
     ms = float(np.median(times))
@@ -407,7 +409,25 @@ def run_sweep_workload(args):
         solo_ms += (time.perf_counter() - t) * 1e3
         solo_ns += inst.n * inst.T
         r.close()
+    # algorithmic bytes of one run: per FLIF_GL neuron-step 8 min(g, L-1)
+    # history + 8 ring write, per neuron-step of either model 8 din input
+    # weights + 16 state (recurrent CSR walks not counted: a lower bound)
+    byt = 0.0
+    for i in insts:
+        per = 8 * 1 + 16
+        byt += float(i.n) * i.T * per
+        if i.neuron == sp.FLIF_GL:
+            L1 = i.L - 1
+            hist = L1 * (L1 + 1) / 2 + max(0, i.T - i.L) * L1 if i.T >= i.L else i.T * (i.T - 1) / 2
+            byt += 8.0 * i.n * (hist + i.T)
+    peak, kind = peaks()
+    gbs = byt / (ms * 1e-3) / 1e9
     line = {"metric": "batched sweep neuron-steps/s", "value": ns / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / peak, "peak_kind": kind,
+                         "algorithmic_bytes_per_run": byt,
+                         "note": "history, ring writes, input weights and state; CSR walks not counted"},
+            "autotune": tuned,
             "unit": "neuron-steps/s", "n_gpus": 1, "ms_per_run": ms, "instances": len(insts),
             "neuron_steps_per_run": ns, "build_s": build_s, "fit_score_all_s": res["fit_score_s"], "nrmse_median": float(np.median(res["nrmse"])),
             "nrmse_min": float(np.min(res["nrmse"])), "schedule": b.info(),

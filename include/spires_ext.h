@@ -370,6 +370,17 @@ spires_status spires_ext_batch_fit_predict(spires_ext_batch *b, const double *co
 spires_status spires_ext_batch_timing(const spires_ext_batch *b, double *construct_ms,
                                       double *setup_ms);
 
+/* Autotuner of the batched launch: runs the batch over u / T (lengths of a
+ * representative sample, every instance from reset) once per candidate
+ * schedule -- four families of CTA groups (size classes with power-of-two
+ * widths, with exact minimum widths, with doubled widths; list scheduling
+ * heaviest first) on a grid of full occupancy and on one CTA per SM -- and
+ * keeps the one with the shortest device time for later runs. Returns the
+ * chosen family (0..3), grid size and its time (any pointer may be NULL). */
+spires_status spires_ext_batch_autotune(spires_ext_batch *b, const double *const *u,
+                                        const size_t *T, int *schedule, int *ctas,
+                                        double *best_ms);
+
 /* Schedule of the last run: CTAs of the grid, CTA groups, and whether the
  * launch sequence runs as a CUDA graph (1) or as direct launches (-1). */
 spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas, int *groups,

@@ -160,6 +160,8 @@ EXT_SIGNATURES = {
     "spires_ext_set_launch": (C.c_int, [_VP, C.POINTER(Launch)]),
     "spires_ext_autotune": (C.c_int, [_VP, C.c_size_t]),
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),
+    "spires_ext_batch_autotune": (C.c_int, [_VP, _VP, _VP, C.POINTER(C.c_int),
+                                            C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "spires_ext_gram_device": (C.c_int, [_VP, C.c_size_t, C.c_size_t, C.c_size_t, C.c_int,
                                          C.c_int, _VP, _VP]),
     "spires_ext_set_wait_limit": (C.c_int, [_VP, C.c_double]),
@@ -579,6 +581,18 @@ class Batch:
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         self.lib.spires_ext_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c))
         return {"ctas": a.value, "groups": b.value, "graph": c.value}
+
+    def autotune(self, us=None, T=None):
+        """spires_ext_batch_autotune over a sample of the series: returns the
+        chosen schedule family, grid size and device ms."""
+        up, T, keep = self._inputs(us, T)
+        Ts = (C.c_size_t * self.count)(*T)
+        mode, ctas, ms = C.c_int(), C.c_int(), C.c_double()
+        st = self.lib.spires_ext_batch_autotune(self.h, up, Ts, C.byref(mode), C.byref(ctas),
+                                                C.byref(ms))
+        if st != SPIRES_OK:
+            raise RuntimeError(f"spires_ext_batch_autotune failed: {st}")
+        return {"schedule": mode.value, "ctas": ctas.value, "ms": ms.value}
 
 
 def ridge_fit(states, targets, lam, washout=0, gram_mode=0, max_refine=30, lib=None):

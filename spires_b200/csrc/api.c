@@ -944,6 +944,18 @@ SPIRES_EXPORT spires_status spires_ext_batch_fit_predict(
         sp_batch_fit_predict(b->b, u, y, T, T_fit, lambda, &o, y_out, w_out, elapsed_ms));
 }
 
+SPIRES_EXPORT spires_status spires_ext_batch_autotune(spires_ext_batch *b,
+                                                     const double *const *u, const size_t *T,
+                                                     int *schedule, int *ctas, double *best_ms)
+{
+    if (!b || !T)
+        return SPIRES_ERR_INVALID_ARG;
+    for (size_t k = 0; k < b->count; ++k)
+        if (T[k] == 0)
+            return SPIRES_ERR_INVALID_ARG;
+    return to_status(sp_batch_autotune(b->b, u, T, schedule, ctas, best_ms));
+}
+
 SPIRES_EXPORT spires_status spires_ext_batch_info(const spires_ext_batch *b, int *ctas,
                                                   int *groups, int *graph)
 {

@@ -519,6 +519,8 @@ __global__ void k_batch_gather(const BInst *inst)
 
 struct sp_batch {
     int device = 0, num_sms = 0, P = 0;
+    int P_max = 0;      // CTAs of the grid at full occupancy (P <= P_max)
+    int plan_mode = 0;  // schedule family (plan()): set by sp_batch_autotune
     size_t smem = 0;
     int lmax = 0;
     int max_nw = 1, list_cap = 0;
@@ -689,7 +691,7 @@ static bool plan_order(sp_batch *b, const std::vector<int> &order, const std::ve
 // class's instances are dealt heaviest first to its least busy group.
 // Many narrow groups keep every SM busy with instances that each run at their
 // own per-step latency. Returns false when the classes do not fit the grid.
-static bool plan_classes(sp_batch *b, const std::vector<long long> &T)
+static bool plan_classes(sp_batch *b, const std::vector<long long> &T, int widen, bool pow2)
 {
     const int P = b->P;
     const size_t cnt = b->inst.size();
@@ -697,8 +699,13 @@ static bool plan_classes(sp_batch *b, const std::vector<long long> &T)
     std::vector<int> classes;
     for (size_t k = 0; k < cnt; ++k) {
         int w = 1;
-        while (w < min_ctas(b->inst[k]))
-            w <<= 1;
+        if (pow2) {
+            while (w < min_ctas(b->inst[k]))
+                w <<= 1;
+        } else {
+            w = min_ctas(b->inst[k]);
+        }
+        w *= widen;
         if (w > P)
             w = min_ctas(b->inst[k]);
         width[k] = w;
@@ -791,9 +798,18 @@ static bool plan_classes(sp_batch *b, const std::vector<long long> &T)
     return true;
 }
 
+// Schedule families (b->plan_mode): 0 size classes of power-of-two widths,
+// 1 size classes of the exact minimum widths, 2 size classes of twice the
+// power-of-two widths (fewer, wider groups), 3 list scheduling heaviest first.
+// Each falls back to list scheduling when its classes do not fit the grid.
 static void plan(sp_batch *b, const std::vector<long long> &T)
 {
-    if (plan_classes(b, T))
+    const int mode = b->plan_mode;
+    if (mode == 0 && plan_classes(b, T, 1, true))
+        return;
+    if (mode == 1 && plan_classes(b, T, 1, false))
+        return;
+    if (mode == 2 && plan_classes(b, T, 2, true))
         return;
     const size_t cnt = b->inst.size();
     std::vector<int> order(cnt);
@@ -916,6 +932,7 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         if (per_sm < 1)
             rc = SP_EINVAL;
         b->P = per_sm * b->num_sms;
+        b->P_max = b->P;
     }
     for (size_t k = 0; !rc && k < count; ++k)
         if (min_ctas(b->inst[k]) > b->P)
@@ -944,7 +961,7 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
         if (I.dense) {
             // column blocks read spike lists in neuron order: identity layout;
             // W_out and the readout sums keep the single path's layout
-            sp_make_layout(&m, I.nw, pos_ro, nid_ro);
+            sp_make_layout(&m, I.nw, nullptr, pos_ro, nid_ro);
             pos[k].resize(m.n);
             nid[k].assign(rs, -1);
             for (size_t i = 0; i < m.n; ++i) {
@@ -952,7 +969,7 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
                 nid[k][i] = (int)i;
             }
         } else {
-            sp_make_layout(&m, I.nw, pos[k], nid[k]);
+            sp_make_layout(&m, I.nw, nullptr, pos[k], nid[k]);
         }
         // CSR in position order, as the single-reservoir path lays it out
         // (column-block instances keep only empty rows here)
@@ -1484,6 +1501,58 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
         *elapsed_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
+}
+
+// Autotuner: times every schedule family on a grid of full occupancy and
+// on one CTA per SM, with the caller's series (the run starts every instance
+// from reset, so no state needs saving), keeps the fastest and returns its
+// device time. Later runs plan with the chosen family and grid.
+extern "C" int sp_batch_autotune(sp_batch *b, const double *const *u, const size_t *T,
+                                 int *best_mode, int *best_ctas, double *best_ms)
+{
+    std::vector<int> grids = {b->P_max};
+    if (b->P_max > b->num_sms)
+        grids.push_back(b->num_sms);
+    const int mode0 = b->plan_mode, P0 = b->P;
+    int bm = mode0, bp = P0;
+    float best = 3.4e38f;
+    for (int P : grids) {
+        bool fits = true;
+        for (const BInst &I : b->inst)
+            fits = fits && min_ctas(I) <= P;
+        if (!fits)
+            continue;
+        for (int mode = 0; mode < 4; ++mode) {
+            b->P = P;
+            b->plan_mode = mode;
+            b->T.clear();  // re-plan and re-capture
+            int rc = batch_prepare(b, T, 0);
+            float ms = 0.f;
+            if (!rc)
+                rc = batch_simulate(b, u, &ms);
+            if (rc) {
+                b->P = P0;
+                b->plan_mode = mode0;
+                b->T.clear();
+                return rc;
+            }
+            if (ms < best) {
+                best = ms;
+                bm = mode;
+                bp = P;
+            }
+        }
+    }
+    b->P = bp;
+    b->plan_mode = bm;
+    b->T.clear();
+    if (best_mode)
+        *best_mode = bm;
+    if (best_ctas)
+        *best_ctas = bp;
+    if (best_ms)
+        *best_ms = best;
+    return SP_OK;
 }
 
 extern "C" int sp_batch_info(const sp_batch *b, int *ctas, int *groups, int *graph)

@@ -157,11 +157,13 @@ __global__ void k_wout_to_pos(const double *__restrict__ w_nat, const int *__res
     }
 }
 
-// spike words in neuron order from position-space words: bit i%32 of word i/32
-__global__ void k_gather_bits(const unsigned *__restrict__ in, int nw, const int *__restrict__ pos,
-                              int n, size_t T, unsigned *__restrict__ out)
+// spike words in neuron order (nw_out words per step) from position-space
+// words (nw_in per step): bit i%32 of word i/32
+__global__ void k_gather_bits(const unsigned *__restrict__ in, int nw_in,
+                              const int *__restrict__ pos, int n, size_t T,
+                              unsigned *__restrict__ out, int nw_out)
 {
-    const size_t words = (size_t)nw;
+    const size_t words = (size_t)nw_out;
     const size_t total = T * words * 32;
     for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
          k += (size_t)gridDim.x * blockDim.x) {
@@ -170,7 +172,7 @@ __global__ void k_gather_bits(const unsigned *__restrict__ in, int nw, const int
         bool b = false;
         if (i < n) {
             const int q = pos[i];
-            b = (in[t * words + (q >> 5)] >> (q & 31)) & 1u;
+            b = (in[t * (size_t)nw_in + (q >> 5)] >> (q & 31)) & 1u;
         }
         const unsigned m = __ballot_sync(kFull, b);
         if ((threadIdx.x & 31) == 0)
@@ -248,11 +250,24 @@ static unsigned gather_blocks(size_t total)
     return (unsigned)(b > 8192 ? 8192 : (b ? b : 1));
 }
 
-static void box_geometry(const sp_launch &l, int *bw, int *nbx)
+// Ring columns a CTA of this launch streams: all its positions, or -- on the
+// balanced layout launched over the grid it was made for -- its active
+// positions only (the first n / G (+1) of its range; the rest are holes).
+static int cta_span(const sp_dev *d, const sp_launch &l)
 {
-    const int sw = 32 * l.warps_max;
-    *bw = sw < 256 ? sw : 256;
-    *nbx = (sw + *bw - 1) / *bw;
+    if (d->bal_G > 0 && l.ctas == d->bal_G)
+        return (d->n + l.ctas - 1) / l.ctas;
+    return 32 * l.warps_max;
+}
+
+// TMA box of the ring pipeline: at most 256 columns (the box limit), an even
+// count (16-byte rows), NBX boxes side by side covering the CTA's span.
+static void box_geometry(const sp_dev *d, const sp_launch &l, int *bw, int *nbx)
+{
+    const int sw = cta_span(d, l);
+    *nbx = (sw + 255) / 256;
+    int w = (sw + *nbx - 1) / *nbx;
+    *bw = (w + 1) & ~1;
 }
 
 // SIMPLE synapse: the CTA's CSR slice (position-space row offsets, column
@@ -301,7 +316,7 @@ static size_t launch_smem(const sp_dev *d, const sp_launch &l)
                  csr_smem_bytes(csr_smem_edges(d, l), l.warps_max);
     if (l.variant == 1) {
         int bw, nbx;
-        box_geometry(l, &bw, &nbx);
+        box_geometry(d, l, &bw, &nbx);
         return spk + coef_smem_bytes(d) + (size_t)l.stages * nbx * l.rows * bw * sizeof(double) +
                2 * (size_t)l.stages * sizeof(unsigned long long);
     }
@@ -375,7 +390,7 @@ static void default_launch(sp_dev *d)
             v.variant = 1;
             v.rows = rows;
             int bw, nbx;
-            box_geometry(v, &bw, &nbx);
+            box_geometry(d, v, &bw, &nbx);
             const size_t stage = (size_t)v.rows * nbx * bw * sizeof(double);
             const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
             const size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d) +
@@ -400,8 +415,8 @@ static void default_launch(sp_dev *d)
 // (longest-processing-time assignment), lanes filled from 0. Every warp, and
 // so every CTA, ends up with about the same number of edges to walk.
 // pos_of[i] = position of neuron i, nid_of[q] = neuron at position q or -1.
-void sp_make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
-                    std::vector<int> &nid_of)
+void sp_make_layout(const sp_host_model *m, int nw, const std::vector<int> *cap,
+                    std::vector<int> &pos_of, std::vector<int> &nid_of)
 {
     const int n = (int)m->n;
     std::vector<int> order(n);
@@ -415,7 +430,8 @@ void sp_make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
     std::vector<ent> heap;
     heap.reserve(nw);
     for (int w = 0; w < nw; ++w)
-        heap.push_back(ent(0, w));
+        if (!cap || (*cap)[w] > 0)
+            heap.push_back(ent(0, w));
     std::vector<int> fill(nw, 0);
     auto cmp = [](const ent &a, const ent &b) { return a > b; };
     std::make_heap(heap.begin(), heap.end(), cmp);
@@ -427,7 +443,7 @@ void sp_make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
         const int q = w * 32 + fill[w]++;
         pos_of[order[r]] = q;
         nid_of[q] = order[r];
-        if (fill[w] < 32) {
+        if (fill[w] < (cap ? (*cap)[w] : 32)) {
             heap.push_back(ent(e.first + deg(order[r]), w));
             std::push_heap(heap.begin(), heap.end(), cmp);
         }
@@ -467,7 +483,23 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
     d->n = (int)m->n;
     d->din = (int)m->din;
     d->dout = (int)m->dout;
-    d->nwords = (m->n + 31) / 32;
+    d->nwords_nat = (m->n + 31) / 32;
+    d->nwords = d->nwords_nat;
+    // Balanced layout (FLIF_GL with at least two warps of neurons per SM):
+    // every one of the SMs' CTAs gets n / SMs (+1) neurons and whole warps of
+    // positions with the holes at the end of its range, so no CTA streams more
+    // history than another and none streams a neighbour's columns.
+    d->bal_G = 0;
+    {
+        const long long G = d->num_sms;
+        if (m->neuron_type == SP_FLIF_GL && G > 0 && (long long)m->n >= 64 * G) {
+            const long long wpc = ((long long)m->n + 32 * G - 1) / (32 * G);
+            if (wpc <= 16 && G * wpc > (long long)d->nwords_nat) {
+                d->bal_G = (int)G;
+                d->nwords = (size_t)(G * wpc);
+            }
+        }
+    }
     d->nw = (int)d->nwords;
     d->rs = d->nw * 32;
     d->micro = m->micro_steps;
@@ -483,7 +515,21 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         const size_t n = m->n, rs = (size_t)d->rs, din = m->din, dout = m->dout;
         cudaStream_t s = d->stream;
         std::vector<int> pos_of, nid_of;
-        sp_make_layout(m, d->nw, pos_of, nid_of);
+        std::vector<int> cap;
+        if (d->bal_G > 0) {
+            // CTA b: n / G (+1 for the first n % G) neurons on its first lanes
+            const int G = d->bal_G, wpc = d->nw / G, n = (int)m->n;
+            cap.assign(d->nw, 0);
+            for (int b = 0; b < G; ++b) {
+                int c = n / G + (b < n % G ? 1 : 0);
+                for (int w = 0; w < wpc; ++w) {
+                    const int k = c < 32 ? c : 32;
+                    cap[b * wpc + w] = k;
+                    c -= k;
+                }
+            }
+        }
+        sp_make_layout(m, d->nw, d->bal_G > 0 ? &cap : nullptr, pos_of, nid_of);
         // CSR in position order: row q = neuron nid_of[q], edges in their original
         // order, column index mapped to the presynaptic neuron's position
         std::vector<long long> rp(rs + 1, 0);
@@ -581,7 +627,7 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         TRY(dalloc(&d->d_y, rows * (dout ? dout : 1) + 2 * (dout ? dout : 1)));
         TRY(dalloc(&d->d_spkd, n));
         TRY(dalloc(&d->d_ras, rows * d->nwords));
-        TRY(dalloc(&d->d_ras_nat, rows * d->nwords));
+        TRY(dalloc(&d->d_ras_nat, rows * d->nwords_nat));
         SP_CK(cudaStreamSynchronize(s));  // host vectors above go out of scope
     }
     default_launch(d);
@@ -723,7 +769,8 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.R = l.variant == 1 ? l.rows : 0;
     p.NST = l.variant == 1 ? l.stages : 0;
     if (l.variant == 1) {
-        box_geometry(l, &p.BW, &p.NBX);
+        box_geometry(d, l, &p.BW, &p.NBX);
+        p.bal = (d->bal_G > 0 && l.ctas == d->bal_G) ? 1 : 0;
         p.RB = p.R < d->nc.L ? p.R : d->nc.L;
         p.coef_smem = coef_smem_bytes(d) > 0;
         int rc = encode_ring_map(d, p.BW, p.RB);
@@ -874,14 +921,14 @@ extern "C" int sp_dev_run(sp_dev *d, const sp_run_args *a)
         if (rc)
             return rc;
         if (want_ras) {
-            unsigned *dst = a->d_raster ? a->d_raster + t0 * d->nwords : d->d_ras_nat;
-            k_gather_bits<<<gather_blocks(tc * d->nwords * 32), 256, 0, d->stream>>>(
-                d->d_ras, d->nw, d->pos_of, d->n, tc, dst);
+            unsigned *dst = a->d_raster ? a->d_raster + t0 * d->nwords_nat : d->d_ras_nat;
+            k_gather_bits<<<gather_blocks(tc * d->nwords_nat * 32), 256, 0, d->stream>>>(
+                d->d_ras, d->nw, d->pos_of, d->n, tc, dst, (int)d->nwords_nat);
             SP_CK(cudaGetLastError());
             if (a->h_raster)
-                SP_CK(cudaMemcpyAsync(a->h_raster + t0 * d->nwords, dst,
-                                      tc * d->nwords * sizeof(unsigned), cudaMemcpyDeviceToHost,
-                                      d->stream));
+                SP_CK(cudaMemcpyAsync(a->h_raster + t0 * d->nwords_nat, dst,
+                                      tc * d->nwords_nat * sizeof(unsigned),
+                                      cudaMemcpyDeviceToHost, d->stream));
         }
         if (want_phi) {
             double *dst = a->d_phi ? a->d_phi + t0 * n : d->d_nat;
@@ -1013,7 +1060,7 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
             l->rows > 256)
             return SP_EINVAL;
         int bw, nbx;
-        box_geometry(*l, &bw, &nbx);
+        box_geometry(d, *l, &bw, &nbx);
         if (encode_ring_map(d, bw, l->rows < d->nc.L ? l->rows : d->nc.L) != SP_OK)
             return SP_EINTERNAL;
     } else if (l->variant != 0) {
@@ -1041,7 +1088,7 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
     return SP_OK;
 }
 
-extern "C" size_t sp_dev_nwords(const sp_dev *d) { return d->nwords; }
+extern "C" size_t sp_dev_nwords(const sp_dev *d) { return d->nwords_nat; }
 extern "C" long long sp_dev_kernel_launches(const sp_dev *d) { return d->launches; }
 
 // ------------------------------------------------------------- autotuner --
@@ -1130,7 +1177,7 @@ extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
                 v.variant = 1;
                 v.rows = rows;
                 int bw, nbx;
-                box_geometry(v, &bw, &nbx);
+                box_geometry(d, v, &bw, &nbx);
                 const size_t stage = (size_t)rows * nbx * bw * 8;
                 const size_t base = (((d->nwords * 4) + 127) & ~(size_t)127) +
                                     coef_smem_bytes(d) +

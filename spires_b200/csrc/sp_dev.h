@@ -162,6 +162,8 @@ int  sp_batch_fit_predict(sp_batch *b, const double *const *u, const double *con
                           const sp_ridge_opts *o, double *const *y_out, double *const *w_out,
                           double *elapsed_ms);
 int  sp_batch_info(const sp_batch *b, int *ctas, int *groups, int *graph);
+int  sp_batch_autotune(sp_batch *b, const double *const *u, const size_t *T, int *best_mode,
+                       int *best_ctas, double *best_ms);
 
 #ifdef __cplusplus
 }

@@ -20,10 +20,12 @@ struct sp_dev {
     int device, num_sms, coop;
     cudaStream_t stream;
     int n, din, dout, micro;
-    int nw;              // warps of neurons = ceil(n / 32)
+    int nw;              // warps of positions (= spike words in position space)
     int rs;              // positions = 32 * nw (device arrays are in position order)
     size_t ring_elems;
-    size_t nwords, nnz;
+    size_t nwords, nnz;  // nwords = nw (position-space spike words)
+    size_t nwords_nat;   // spike words of a neuron-order raster, ceil(n / 32)
+    int bal_G;           // layout balanced over this many CTAs (0: dense layout)
     double dt, gamma;
     int ntype, stype;
     sp_neuron_consts nc;
@@ -87,7 +89,8 @@ extern "C" int sp_dev_w_out_from_nat(sp_dev *d, const double *dev_w_nat);
 extern "C" int sp_dev_w_out_to_nat(sp_dev *d, double *dev_w_nat);
 
 // Position layout shared by the single and batched paths (dev_reservoir.cu).
-void sp_make_layout(const sp_host_model *m, int nw, std::vector<int> &pos_of,
+void sp_make_layout(const sp_host_model *m, int nw, const std::vector<int> *cap,
+                    std::vector<int> &pos_of,
                     std::vector<int> &nid_of);
 
 // Ridge on a device Phi [T x n] (neuron order) and targets Y [T x dout];

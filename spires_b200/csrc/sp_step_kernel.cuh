@@ -36,6 +36,8 @@ struct KP {
     int warps;      // consumer warps per CTA
     int R, NST;     // variant 1: ring rows per stage, stages
     int BW, NBX;    // variant 1: box width (neurons) and boxes side by side per stage
+    int bal;        // balanced layout: CTA b's active positions are the first
+                    // n / G (+1 for b < n % G) of its range, the rest holes
     int RB;         // variant 1: rows per box = min(R, L)
     int coef_smem;  // variant 1: coefficient table staged in shared memory
     int csr_cap;    // SIMPLE synapse: edges of the CTA's CSR slice kept in shared
@@ -388,7 +390,8 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         int st = 0;       // q % NST
         long long rounds = 0;  // q / NST
         bool ok = true;
-        const int nbox = (S_b + p.BW - 1) / p.BW;
+        const int S_act = p.bal ? p.n / p.G + (blockIdx.x < p.n % p.G ? 1 : 0) : S_b;
+        const int nbox = (S_act + p.BW - 1) / p.BW;
         for (long long b = 0; b < B && ok; ++b) {
             const long long g = p.step0 + b;
             const int lim = (int)(g < L ? g : L - 1);

@@ -168,3 +168,22 @@ def test_fit_predict_equals_train_then_predict():
     Y2, _ = b2.predict(us)
     for k in range(len(cfgs)):
         assert same_bits(Y[k][:, :2], Y2[k][:, :2]), f"instance {k}"
+
+
+def test_autotuned_schedule_keeps_results():
+    """spires_ext_batch_autotune times every schedule family and grid size on
+    a sample of the series and keeps the fastest; whichever it keeps, every
+    instance's raster and final state stay bit-identical to the same
+    reservoir run on its own."""
+    cfgs, seeds, us = mixed_batch(12, seed=77)
+    b = sp.Batch(cfgs, seeds)
+    sample = [u[:30] for u in us]
+    tuned = b.autotune(sample)
+    assert 0 <= tuned["schedule"] <= 3 and tuned["ctas"] > 0 and tuned["ms"] > 0
+    R, V, _ = b.run(us)
+    assert b.info()["ctas"] == tuned["ctas"]
+    b.close()
+    for k in range(len(cfgs)):
+        Rs, Vs = solo(cfgs[k], seeds[k], us[k])
+        assert np.array_equal(R[k], Rs), k
+        assert same_bits(V[k], Vs), k
