@@ -1321,8 +1321,10 @@ extern "C" int sp_batch_train_ridge(sp_batch *b, const double *const *u, const d
         max_wn = std::max(max_wn, (size_t)b->inst[k].n * b->models[k].dout);
     }
     double *nat = nullptr, *Y = nullptr, *W = nullptr;
+    sp_ridge_ws *ws = sp_ridge_ws_new();  // one set of solver buffers for every instance
     auto cleanup = [&]() {
         cudaStreamSynchronize(b->stream);
+        sp_ridge_ws_free(ws);
         if (nat)
             sp_cuda_free(nat);
         if (Y)
@@ -1354,7 +1356,7 @@ extern "C" int sp_batch_train_ridge(sp_batch *b, const double *const *u, const d
             break;
         sp_ridge_report rep;
         memset(&rep, 0, sizeof(rep));
-        rc = sp_ridge_phi(b->stream, nat, I.n, T[k], Y, dout, lambda[k], o, &rep, W);
+        rc = sp_ridge_phi_ws(b->stream, nat, I.n, T[k], Y, dout, lambda[k], o, &rep, W, ws);
         if (rc == SP_RIDGE_SINGULAR) {
             // singular: W_out of this instance stays as it was (dgesv failure)
             rc = SP_OK;
@@ -1456,6 +1458,7 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
         return SP_EALLOC;
     }
     size_t po = 0;
+    sp_ridge_ws *ws = sp_ridge_ws_new();  // one set of solver buffers for every instance
     for (size_t k = 0; k < b->inst.size() && !rc; ++k) {
         const BInst &I = b->inst[k];
         const int dout = (int)b->models[k].dout;
@@ -1473,7 +1476,7 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
             break;
         sp_ridge_report rep;
         memset(&rep, 0, sizeof(rep));
-        rc = sp_ridge_phi(b->stream, nat, I.n, T_fit[k], Y, dout, lambda[k], o, &rep, W);
+        rc = sp_ridge_phi_ws(b->stream, nat, I.n, T_fit[k], Y, dout, lambda[k], o, &rep, W, ws);
         if (rc == SP_RIDGE_SINGULAR) {
             rc = SP_OK; /* this instance keeps its previous W_out */
         } else if (!rc) {
@@ -1494,6 +1497,7 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
             rc = SP_EINTERNAL;
     }
     cudaStreamSynchronize(b->stream);
+    sp_ridge_ws_free(ws);
     sp_cuda_free(nat);
     sp_cuda_free(Y);
     sp_cuda_free(W);

@@ -894,11 +894,72 @@ out:
     return rc;
 }
 
-// One group of at most 16 outputs of sp_ridge_phi (below). Work buffers are
-// allocated per call.
+// Work buffers of the primal solve, kept across calls by a caller that fits
+// many readouts in a row (the batched fits): grown to the largest sizes seen,
+// freed by sp_ridge_ws_free.
+struct sp_ridge_ws {
+    double *A = nullptr, *B = nullptr, *W = nullptr, *R = nullptr, *E = nullptr,
+           *part = nullptr, *tmp = nullptr;
+    int *info = nullptr, *piv = nullptr;
+    size_t cap_nn = 0, cap_nd = 0, cap_td = 0, cap_n = 0;
+};
+
+extern "C" sp_ridge_ws *sp_ridge_ws_new(void) { return new sp_ridge_ws(); }
+
+static void ws_release(sp_ridge_ws *w)
+{
+    void *bufs[] = {w->A, w->B, w->W, w->R, w->E, w->part, w->tmp, w->info, w->piv};
+    for (void *b : bufs)
+        if (b)
+            sp_cuda_free(b);
+    *w = sp_ridge_ws();
+}
+
+extern "C" void sp_ridge_ws_free(sp_ridge_ws *w)
+{
+    if (!w)
+        return;
+    ws_release(w);
+    delete w;
+}
+
+// Buffers for n neurons, T rows and dout (<= 16) outputs, reusing what is
+// large enough. The caller's stream must be idle (the batched fits wait for
+// each instance before the next).
+static int ws_ensure(sp_ridge_ws *w, int n, size_t T, int dout, int parts)
+{
+    const size_t nn = (size_t)n * n, nd = (size_t)n * dout, td = (T ? T : 1) * (size_t)dout;
+    if (nn <= w->cap_nn && nd <= w->cap_nd && td <= w->cap_td && (size_t)n <= w->cap_n)
+        return SP_OK;
+    const size_t cnn = nn > w->cap_nn ? nn : w->cap_nn, cnd = nd > w->cap_nd ? nd : w->cap_nd,
+                 ctd = td > w->cap_td ? td : w->cap_td,
+                 cn = (size_t)n > w->cap_n ? (size_t)n : w->cap_n;
+    ws_release(w);
+    int rc = SP_OK;
+    RK(sp_cuda_malloc(&w->A, cnn * sizeof(double)));
+    RK(sp_cuda_malloc(&w->B, cnd * sizeof(double)));
+    RK(sp_cuda_malloc(&w->W, cnd * sizeof(double)));
+    RK(sp_cuda_malloc(&w->R, cnd * sizeof(double)));
+    RK(sp_cuda_malloc(&w->E, ctd * sizeof(double)));
+    RK(sp_cuda_malloc(&w->part, (size_t)parts * cnd * sizeof(double)));
+    RK(sp_cuda_malloc(&w->tmp, 4 * sizeof(double)));
+    RK(sp_cuda_malloc(&w->info, sizeof(int)));
+    RK(sp_cuda_malloc(&w->piv, cn * sizeof(int)));
+    w->cap_nn = cnn;
+    w->cap_nd = cnd;
+    w->cap_td = ctd;
+    w->cap_n = cn;
+    return SP_OK;
+out:
+    ws_release(w);
+    return rc;
+}
+
+// One group of at most 16 outputs of sp_ridge_phi (below). Work buffers come
+// from `ws` when given, else are allocated for the call.
 static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
                            const double *Y, int dout, double lambda, const sp_ridge_opts *o,
-                           sp_ridge_report *rep, double *d_W_out)
+                           sp_ridge_report *rep, double *d_W_out, sp_ridge_ws *ws)
 {
     int rc = SP_OK;
     double *A = nullptr, *Aw = nullptr, *B = nullptr, *W = nullptr, *R = nullptr, *E = nullptr,
@@ -910,15 +971,30 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
         return SP_OK;
     if (dout > 16)
         return SP_EINVAL; /* per-thread accumulators below hold up to 16 outputs */
-    RK(sp_cuda_malloc(&A, (size_t)n * n * sizeof(double)));
-    RK(sp_cuda_malloc(&B, (size_t)n * dout * sizeof(double)));
-    RK(sp_cuda_malloc(&W, (size_t)n * dout * sizeof(double)));
-    RK(sp_cuda_malloc(&R, (size_t)n * dout * sizeof(double)));
-    RK(sp_cuda_malloc(&E, (T ? T : 1) * (size_t)dout * sizeof(double)));
-    RK(sp_cuda_malloc(&part, (size_t)parts * n * dout * sizeof(double)));
-    RK(sp_cuda_malloc(&tmp, 4 * sizeof(double)));
-    RK(sp_cuda_malloc(&info, sizeof(int)));
-    RK(sp_cuda_malloc(&piv, (size_t)n * sizeof(int)));
+    if (ws) {
+        rc = ws_ensure(ws, n, T, dout, parts);
+        if (rc)
+            return rc;
+        A = ws->A;
+        B = ws->B;
+        W = ws->W;
+        R = ws->R;
+        E = ws->E;
+        part = ws->part;
+        tmp = ws->tmp;
+        info = ws->info;
+        piv = ws->piv;
+    } else {
+        RK(sp_cuda_malloc(&A, (size_t)n * n * sizeof(double)));
+        RK(sp_cuda_malloc(&B, (size_t)n * dout * sizeof(double)));
+        RK(sp_cuda_malloc(&W, (size_t)n * dout * sizeof(double)));
+        RK(sp_cuda_malloc(&R, (size_t)n * dout * sizeof(double)));
+        RK(sp_cuda_malloc(&E, (T ? T : 1) * (size_t)dout * sizeof(double)));
+        RK(sp_cuda_malloc(&part, (size_t)parts * n * dout * sizeof(double)));
+        RK(sp_cuda_malloc(&tmp, 4 * sizeof(double)));
+        RK(sp_cuda_malloc(&info, sizeof(int)));
+        RK(sp_cuda_malloc(&piv, (size_t)n * sizeof(int)));
+    }
     RK(cudaMemsetAsync(info, 0, sizeof(int), s));
 
     if (lambda > 0.0 && 2 * (T - w0) <= (size_t)n) {
@@ -1054,10 +1130,14 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
     }
 out:
     cudaStreamSynchronize(s);
-    void *bufs[] = {A, Aw, B, W, R, E, part, tmp, info, piv};
-    for (void *b : bufs)
-        if (b)
-            sp_cuda_free(b);
+    if (!ws) {
+        void *bufs[] = {A, Aw, B, W, R, E, part, tmp, info, piv};
+        for (void *b : bufs)
+            if (b)
+                sp_cuda_free(b);
+    } else if (Aw) {
+        sp_cuda_free(Aw);
+    }
     return rc;
 }
 
@@ -1079,10 +1159,23 @@ extern "C" int sp_gram_fp64(cudaStream_t s, const double *X, int n, size_t t0, s
 // d_W_out only when every group has succeeded.
 extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
                             const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                            sp_ridge_report *rep, double *d_W_out);
+
+extern "C" int sp_ridge_phi_ws(cudaStream_t s, const double *Phi, int n, size_t T,
+                               const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                               sp_ridge_report *rep, double *d_W_out, sp_ridge_ws *ws)
+{
+    if (dout <= 16)
+        return ridge_phi_group(s, Phi, n, T, Y, dout, lambda, o, rep, d_W_out, ws);
+    return sp_ridge_phi(s, Phi, n, T, Y, dout, lambda, o, rep, d_W_out);
+}
+
+extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
+                            const double *Y, int dout, double lambda, const sp_ridge_opts *o,
                             sp_ridge_report *rep, double *d_W_out)
 {
     if (dout <= 16)
-        return ridge_phi_group(s, Phi, n, T, Y, dout, lambda, o, rep, d_W_out);
+        return ridge_phi_group(s, Phi, n, T, Y, dout, lambda, o, rep, d_W_out, nullptr);
     int rc = SP_OK;
     double *Yg = nullptr, *Wall = nullptr;
     sp_ridge_report sum;
@@ -1097,7 +1190,8 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
                                  cudaMemcpyDeviceToDevice, s));
         sp_ridge_report r1;
         memset(&r1, 0, sizeof(r1));
-        rc = ridge_phi_group(s, Phi, n, T, Yg, dg, lambda, o, &r1, Wall + (size_t)g0 * n);
+        rc = ridge_phi_group(s, Phi, n, T, Yg, dg, lambda, o, &r1, Wall + (size_t)g0 * n,
+                             nullptr);
         sum.gram_mode_used = r1.gram_mode_used;
         sum.dual = r1.dual;
         sum.refine_iters = r1.refine_iters > sum.refine_iters ? r1.refine_iters : sum.refine_iters;

@@ -352,7 +352,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_gram_tc(const __grid_constant__
             const int i = I * kTileM + r;
             const int ei = (MODE == SP_GRAM_INT8 && i < p.n_pad) ? __ldg(p.exps + i) : 0;
             for (int sg = 0; sg < segs && ok; ++sg, ++sc) {
-                if (!wait_bar(tfull, (unsigned)(sc & 1), p.err, &s_abort, 4)) {
+                // one lane polls; the warp then reads TMEM together (.sync.aligned)
+                int okw = 1;
+                if (lane == 0)
+                    okw = wait_bar(tfull, (unsigned)(sc & 1), p.err, &s_abort, 4) ? 1 : 0;
+                okw = __shfl_sync(0xffffffffu, okw, 0);
+                if (!okw) {
                     ok = false;
                     break;
                 }

@@ -98,6 +98,13 @@ void sp_make_layout(const sp_host_model *m, int nw, const std::vector<int> *cap,
 extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
                             const double *Y, int dout, double lambda, const sp_ridge_opts *o,
                             sp_ridge_report *rep, double *d_W_out);
+// The same with reusable work buffers (primal solves of up to 16 outputs).
+struct sp_ridge_ws;
+extern "C" sp_ridge_ws *sp_ridge_ws_new(void);
+extern "C" void sp_ridge_ws_free(sp_ridge_ws *w);
+extern "C" int sp_ridge_phi_ws(cudaStream_t s, const double *Phi, int n, size_t T,
+                               const double *Y, int dout, double lambda, const sp_ridge_opts *o,
+                               sp_ridge_report *rep, double *d_W_out, sp_ridge_ws *ws);
 
 // Layout kernels on raw device pointers (dev_reservoir.cu).
 extern "C" int sp_launch_readout(cudaStream_t s, const double *W_pos, const double *X, int rs,
