@@ -380,7 +380,7 @@ static void default_launch(sp_dev *d)
         if (l.warps_max > 32)
             l.warps_max = 32;
     }
-    if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 16) {
+    if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= kPipeWarps) {
         // long rings: 64-row stages (fewer, larger copies per step; 34.1 against
         // 35.2 us per step at N=20000, L=1024), else 32-row stages
         for (int rows : {64, 32}) {
@@ -494,7 +494,7 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         const long long G = d->num_sms;
         if (m->neuron_type == SP_FLIF_GL && G > 0 && (long long)m->n >= 64 * G) {
             const long long wpc = ((long long)m->n + 32 * G - 1) / (32 * G);
-            if (wpc <= 16 && G * wpc > (long long)d->nwords_nat) {
+            if (wpc <= kPipeWarps && G * wpc > (long long)d->nwords_nat) {
                 d->bal_G = (int)G;
                 d->nwords = (size_t)(G * wpc);
             }
@@ -1056,7 +1056,7 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
     if ((long long)l->ctas * l->warps_max < (long long)d->nwords)
         return SP_EINVAL;
     if (l->variant == 1) {
-        if (d->ntype != SP_FLIF_GL || l->warps_max > 16 || l->rows < 1 || l->stages < 2 ||
+        if (d->ntype != SP_FLIF_GL || l->warps_max > kPipeWarps || l->rows < 1 || l->stages < 2 ||
             l->rows > 256)
             return SP_EINVAL;
         int bw, nbx;
@@ -1171,7 +1171,7 @@ extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
         if (l.warps_max > 32)
             continue;
         cand.push_back(l);
-        if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= 16) {
+        if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= kPipeWarps) {
             for (int rows : {16, 32, 64}) {
                 sp_launch v = l;
                 v.variant = 1;

@@ -13,6 +13,13 @@
 //   shared memory. The producer runs up to one step ahead of the consumers:
 //   the rows of step g are the states of steps <= g-2 (lag 1 is the register
 //   copy of the previous state), so they only wait for step g-2 to finish.
+//   Lags 2..33 are the thread's own last 32 states, kept in a register shift
+//   register, so the producer streams lags 34.. only (3 % fewer ring bytes per
+//   step at L = 1024) and the sum of a step starts as soon as its lag 1 exists.
+//   The grid is sized so that each CTA streams about the same number of ring
+//   columns (balanced layout, dev_reservoir.cu), and the CTA's CSR slice sits
+//   in shared memory for the launch, so the row pass after each grid barrier
+//   reads no global memory but the spike words.
 //
 // Per micro-step (both variants), with a split-phase grid barrier:
 //   history sum of step g      (overlaps the barrier wait)
@@ -307,16 +314,25 @@ __device__ __forceinline__ double stage_sum(double hist, const double *coef_k, c
     return hist;
 }
 
-// Variant 1 runs at most 16 consumer warps + 1 producer warp per CTA, which
-// leaves registers for a whole stage of lags in flight per thread.
+// Variant 1 runs at most kPipeWarps consumer warps + 1 producer warp per CTA,
+// which leaves registers for a stage of lags in flight and the register lags
+// per thread.
+constexpr int kPipeWarps = 8;
+
 template <int VAR>
 struct Bounds {
-    static constexpr int threads = VAR == 1 ? 544 : 1024;
+    static constexpr int threads = VAR == 1 ? 32 * (kPipeWarps + 1) : 1024;
 };
+
+// Variant 1 keeps lags 2..kRegLags+1 of its own neuron in registers: they are
+// the thread's own last states, so they are neither written to nor read back
+// from the ring for the sum, and the producer streams lags kRegLags+2.. only.
+constexpr int kRegLags = 32;
 
 template <int NT, int ST, int VAR>
 __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_constant__ KP p)
 {
+    constexpr int RL = (VAR == 1 && NT == SP_FLIF_GL) ? kRegLags : 0;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_flag;
     __shared__ volatile int s_abort;
@@ -395,7 +411,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         for (long long b = 0; b < B && ok; ++b) {
             const long long g = p.step0 + b;
             const int lim = (int)(g < L ? g : L - 1);
-            if (lim < 2)
+            if (lim < 2 + RL)
                 continue;
             if (b >= 2) {
                 // rows of step g are states of steps <= g-2
@@ -422,10 +438,8 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             // lags k..k+cnt-1 are rows rh down to rh-cnt+1: one contiguous
             // ascending row range per stage (split at the wrap)
             SP_STAMP(true, b, B, 7);
-            int rh = (int)(g % L) - 2;
-            if (rh < 0)
-                rh += L;
-            for (int k = 2; k <= lim && ok;) {
+            int rh = (int)(((g - 2 - RL) % L + L) % L);
+            for (int k = 2 + RL; k <= lim && ok;) {
                 int cnt = lim - k + 1;
                 if (cnt > p.R)
                     cnt = p.R;
@@ -486,6 +500,20 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 pr += L;
             vlast = p.ring[(size_t)pr * p.rs + i];
         }
+    }
+    // lag 2 + j of the next step: the state of micro-step step0 - 2 - j
+    double hreg[RL > 0 ? RL : 1];
+#pragma unroll
+    for (int j = 0; j < (RL > 0 ? RL : 1); ++j)
+        hreg[j] = 0.0;
+    if (RL > 0 && act) {
+#pragma unroll
+        for (int j = 0; j < RL; ++j) {
+            const long long pr = ((p.step0 - 2 - j) % L + L) % L;
+            hreg[j] = p.ring[(size_t)pr * p.rs + i];
+        }
+    }
+    if (act) {
         if (NT == SP_FLIF_CAPUTO)
             cpos = p.cap_pos[i];
         if (NT == SP_FLIF_DIFFUSIVE) {
@@ -641,10 +669,15 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             } else {
                 const int boff = (tid / p.BW) * p.R * p.BW + (tid % p.BW);
                 const double *cf = p.coef_smem ? s_coef : p.coef;
-                int rh = head - 2;
-                if (rh < 0)
-                    rh += L;
-                for (int k = 2; k <= lim && S_b > 0;) {
+                if (act && integ) {
+                    // lags 2 .. RL+1 from registers, in ascending order
+#pragma unroll
+                    for (int j = 0; j < RL; ++j)
+                        if (2 + j <= lim)
+                            hist = add(hist, mul(cf[2 + j], hreg[j]));
+                }
+                int rh = (int)(((long long)head - 2 - RL) % L + L) % L;
+                for (int k = 2 + RL; k <= lim && S_b > 0;) {
                     int cnt = lim - k + 1;
                     if (cnt > p.R)
                         cnt = p.R;
@@ -759,6 +792,12 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                     V = p.b;
                 }
                 p.ring[(size_t)head * p.rs + i] = V;
+                if (RL > 0) {
+#pragma unroll
+                    for (int j = (RL > 0 ? RL : 1) - 1; j > 0; --j)
+                        hreg[j] = hreg[j - 1];
+                    hreg[0] = vlast;
+                }
                 vlast = V;
                 tprev = add(tprev, p.dt);
             } else if (NT == SP_FLIF_CAPUTO) {
