@@ -365,6 +365,34 @@ def run_profile_case(args):
     print("profile case done")
 
 
+def run_profile_gram(args):
+    """The ridge workload's states (FLIF_GL N=4000 L=512 WS, T=20000), then
+    exactly one tensor-core Gram of rows [1000, 20000) in the INT8 mode with
+    7 slices: the launch an ncu capture with -k regex:k_gram_tc -c 1 sees."""
+    import numpy as np
+    import torch
+
+    import spires_b200 as sp
+    from spires_b200.datasets import mackey_glass
+
+    lib = sp.load()
+    n, T, w = 4000, 20000, 1000
+    cfg = sp.make_config(n, 1, 1, rho=0.95, ei=0.5, gamma=0.5, conn=10.0 / (n - 1),
+                         topo=sp.CONN_SMALL_WORLD, neuron=sp.FLIF_GL,
+                         nparams=(1.0, 0.0, 0.0, 20.0, 0.7, 512.0, 0.1, 2.0))
+    x = mackey_glass(T + 1, seed=0)
+    r = sp.Reservoir(cfg, seed=42)
+    phi, _, _ = r.run_record(np.ascontiguousarray(x[:-1, None]), phi=True, raster=False)
+    r.close()
+    dX = torch.from_numpy(phi).cuda()
+    dC = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    st = lib.spires_ext_gram_device(C.c_void_p(dX.data_ptr()), T, n, w, args.gram_mode,
+                                    args.gram_slices, C.c_void_p(dC.data_ptr()), None)
+    assert st == sp.SPIRES_OK, st
+    print("profile gram done")
+
+
 # ------------------------------------------------- additional workloads --
 # Printed only when asked for with --workload; the default line above is the
 # headline measurement.
@@ -758,6 +786,10 @@ def main():
     ap.add_argument("--variant", type=int, default=-1, help="force step-kernel variant")
     ap.add_argument("--profile-case", action="store_true",
                     help="fill the ring, then one launch of --chunk steps (for ncu -s 1 -c 1)")
+    ap.add_argument("--profile-gram", action="store_true",
+                    help="the ridge workload's states, then one tensor-core Gram (for ncu)")
+    ap.add_argument("--gram-mode", type=int, default=3)
+    ap.add_argument("--gram-slices", type=int, default=7)
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
     ap.add_argument("--workload", default="step",
@@ -793,6 +825,9 @@ def main():
         return
     if args.profile_case:
         run_profile_case(args)
+        return
+    if args.profile_gram:
+        run_profile_gram(args)
         return
 
     if world > 1:

@@ -410,8 +410,9 @@ spires_status spires_ext_mlp_loss_grad(spires_ext_mlp *m, const float *X, const 
 spires_status spires_ext_mlp_train(spires_ext_mlp *m, const float *X, const float *y, size_t n,
                                    int epochs, int batch, float lr, uint64_t seed,
                                    float *final_loss);
-/* mean / logvar per row (either may be NULL); bf16 = 1: BF16 weights and
- * activations with FP32 accumulation */
+/* mean / logvar per row (either may be NULL); bf16 = 1: weights and
+ * activations rounded to BF16, products and sums in FP32 on the CUDA cores
+ * (the network is too small for the tensor cores to pay) */
 spires_status spires_ext_mlp_predict(spires_ext_mlp *m, const float *X, size_t n, int bf16,
                                      float *mean, float *logvar);
 long long     spires_ext_mlp_kernel_launches(const spires_ext_mlp *m);

@@ -471,7 +471,9 @@ extern "C" int sp_mlp_train(sp_mlp *m, const float *X, const float *y, int n, in
 }
 
 // Predicted (mean, log-variance) for n host rows; bf16 = 1 runs the BF16
-// inference path (weights and activations rounded to BF16, FP32 sums).
+// inference path (weights and activations rounded to BF16, products and sums
+// in FP32 on the CUDA cores: a 10 -> 128 -> 128 -> 2 network is too small for
+// tensor-core tiles to pay).
 extern "C" int sp_mlp_predict(sp_mlp *m, const float *X, int n, int bf16, float *mean,
                               float *logvar)
 {
