@@ -381,10 +381,14 @@ static void default_launch(sp_dev *d)
             l.warps_max = 32;
     }
     if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= kPipeWarps) {
-        // long rings: 64-row stages (fewer, larger copies per step; 34.1 against
-        // 35.2 us per step at N=20000, L=1024), else 32-row stages
-        for (int rows : {64, 32}) {
-            if (rows == 64 && d->nc.L < 512)
+        // The ring stream is paced by the bytes in flight per SM (the stages
+        // the consumers are not reading): long rings take the stage height of
+        // 64, 56 or 48 rows that puts the most rows in flight (ties: taller),
+        // shorter rings 32-row stages.
+        sp_launch best = l;
+        long long best_rows = 0;
+        for (int rows : {64, 56, 48, 32}) {
+            if ((rows > 32) != (d->nc.L >= 512))
                 continue;
             sp_launch v = l;
             v.variant = 1;
@@ -392,18 +396,24 @@ static void default_launch(sp_dev *d)
             int bw, nbx;
             box_geometry(d, v, &bw, &nbx);
             const size_t stage = (size_t)v.rows * nbx * bw * sizeof(double);
-            const size_t budget = (size_t)(max_smem(d) - 8 * 1024);
+            const size_t budget = (size_t)(max_smem(d) - 2 * 1024);
             const size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d) +
                                csr_smem_bytes(csr_smem_edges(d, v), v.warps_max);
             long long st = budget > spk ? (long long)((budget - spk) / (stage + 16)) : 0;
             if (st > 16)
                 st = 16;
-            if (st >= 2 &&
+            if (st >= 2 && st * rows > best_rows &&
                 encode_ring_map(d, bw, v.rows < d->nc.L ? v.rows : d->nc.L) == SP_OK) {
                 v.stages = (int)st;
-                l = v;
-                break;
+                best = v;
+                best_rows = st * rows;
             }
+        }
+        if (best_rows > 0) {
+            l = best;
+            int bw, nbx;
+            box_geometry(d, l, &bw, &nbx);
+            encode_ring_map(d, bw, l.rows < d->nc.L ? l.rows : d->nc.L);
         }
     }
     d->launch = l;

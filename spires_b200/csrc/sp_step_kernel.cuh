@@ -695,8 +695,15 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                             for (int h = 0; h < cnt; h += 16)
                                 hist = stage_sum<16>(hist, cf + k + h,
                                                      buf + (size_t)(cnt - 16 - h) * p.BW, p.BW);
-                        } else if (cnt == 8) {
-                            hist = stage_sum<8>(hist, cf + k, buf, p.BW);
+                        } else if ((cnt & 7) == 0) {
+                            // stages of 24, 40, 48 or 56 rows: 16 at a time, then 8
+                            int h = 0;
+                            for (; h + 16 <= cnt; h += 16)
+                                hist = stage_sum<16>(hist, cf + k + h,
+                                                     buf + (size_t)(cnt - 16 - h) * p.BW, p.BW);
+                            for (; h < cnt; h += 8)
+                                hist = stage_sum<8>(hist, cf + k + h,
+                                                    buf + (size_t)(cnt - 8 - h) * p.BW, p.BW);
                         } else {
                             for (int jr = 0; jr < cnt; ++jr)
                                 hist = add(hist, mul(cf[k + jr],
