@@ -576,6 +576,8 @@ extern "C" int sp_dev_create(const sp_host_model *m, sp_dev **out)
         TRY(dalloc(&d->tprev, rs));
         TRY(dalloc(&d->spk, 2 * d->nwords));
         TRY(dalloc(&d->bar, 4));
+        d->flag_cap = 8 * (d->num_sms > 0 ? d->num_sms : 1);
+        TRY(dalloc(&d->flags, (size_t)d->flag_cap * kFlagStride));
         TRY(dalloc(&d->err, 4));
         TRY(dupload(&d->row_ptr, rp.data(), rs + 1, s));
         d->h_row_ptr = (long long *)malloc((rs + 1) * sizeof(long long));
@@ -662,7 +664,8 @@ extern "C" void sp_dev_destroy(sp_dev *d)
                     d->row_ptr, d->col, d->w, d->coef, d->eff, d->trace, d->edge_decay,
                     d->edge_omd, d->edge_trace, d->scoef, d->Iring, d->mx_decay, d->mx_omd,
                     d->mx_c, d->mx_tr, d->W_in, d->W_out, d->d_u, d->d_phi, d->d_nat, d->d_y,
-                    d->d_spkd, d->d_ras, d->d_ras_nat, d->bar, d->err, d->pos_of, d->nid_of};
+                    d->d_spkd, d->d_ras, d->d_ras_nat, d->bar, d->err, d->pos_of, d->nid_of,
+                    d->flags};
     for (void *b : bufs)
         if (b)
             sp_cuda_free(b);
@@ -808,7 +811,7 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.mx_tr = d->mx_tr;
     p.W_in = d->W_in; p.gamma = d->gamma; p.u = u;
     p.phi = phi; p.raster = raster;
-    p.bar = d->bar; p.err = d->err;
+    p.bar = d->bar; p.err = d->err; p.flags = d->flags;
     p.tmo = d->wait_ns ? d->wait_ns : kBarrierTimeoutNs;
     p.hold_cta = -1;
     p.hold_b = -1;
@@ -830,7 +833,9 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
         SP_CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     if (l.ctas > 1) {
-        SP_CK(cudaMemsetAsync(d->bar, 0, sizeof(unsigned long long), d->stream));
+        SP_CK(cudaMemsetAsync(d->flags, 0,
+                              (size_t)l.ctas * kFlagStride * sizeof(unsigned long long),
+                              d->stream));
         void *args[] = {&p};
         SP_CK(cudaLaunchCooperativeKernel((const void *)fn, grid, block, args, smem, d->stream));
     } else {
@@ -1063,7 +1068,7 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
 {
     if (l->ctas < 1 || l->warps_max < 1 || l->warps_max > 32)
         return SP_EINVAL;
-    if ((long long)l->ctas * l->warps_max < (long long)d->nwords)
+    if ((long long)l->ctas * l->warps_max < (long long)d->nwords || l->ctas > d->flag_cap)
         return SP_EINVAL;
     if (l->variant == 1) {
         if (d->ntype != SP_FLIF_GL || l->warps_max > kPipeWarps || l->rows < 1 || l->stages < 2 ||

@@ -64,6 +64,8 @@ struct sp_dev {
     double *d_spkd;      // [n]
     double *h_stage;     // pinned [chunk][dout]
     unsigned long long *bar;  // grid-barrier arrival counter
+    unsigned long long *flags; // per-CTA arrival flags of the step kernel (flag_cap CTAs)
+    int flag_cap;
     int *err;                 // [0] code, [1]/[2] micro-step low/high word
 
     // bounded waits: limit (ns) of every wait in the step kernel; one-shot

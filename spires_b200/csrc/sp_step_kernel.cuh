@@ -80,6 +80,9 @@ struct KP {
     double *phi;
     unsigned *raster;
     unsigned long long *bar;  // grid-barrier arrival counter (64-bit: never wraps)
+    // arrival flags, one per CTA on its own 128-byte line: CTA c stores b + 1
+    // once its spike words and drive of micro-step b - 1 are published
+    unsigned long long *flags;
     int *err;                 // [0] error code, [1] / [2] low / high word of the micro-step
     unsigned long long tmo;   // limit of every wait, ns
     // one-shot test hook: CTA hold_cta does not arrive at the barrier that
@@ -328,6 +331,7 @@ struct Bounds {
 // the thread's own last states, so they are neither written to nor read back
 // from the ring for the sum, and the producer streams lags kRegLags+2.. only.
 constexpr int kRegLags = 32;
+constexpr int kFlagStride = 16;  // u64 per CTA arrival flag (one 128-byte line)
 
 template <int NT, int ST, int VAR>
 __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_constant__ KP p)
@@ -577,46 +581,67 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     };
 
     // arrival at the barrier that opens micro-step b
+    // Grid barrier as per-CTA flags: arriving at barrier b publishes b + 1 in
+    // the CTA's own flag (after its spike words); waiting, consumer thread t
+    // watches the flags of CTAs t, t + NC, ... and, as soon as one is up, copies
+    // that CTA's spike words into shared memory -- so the copy of the early
+    // CTAs' words overlaps the wait for the late ones, and no two CTAs write
+    // the same line.
     auto barrier_arrive = [&](long long b) {
         named_sync(NC);
         if (tid == 0 && p.G > 1 && !(b == p.hold_b && (int)blockIdx.x == p.hold_cta)) {
             __threadfence();
-            atomicAdd(p.bar, 1ull);
+            *(volatile unsigned long long *)(p.flags + (size_t)blockIdx.x * kFlagStride) =
+                (unsigned long long)(b + 1);
         }
     };
     // returns false when the launch must stop
     auto barrier_wait = [&](long long b) -> bool {
-        if (tid == 0) {
-            int ok = 1;
-            if (p.G > 1) {
-                const unsigned long long target =
-                    (unsigned long long)(b + 1) * (unsigned long long)p.G;
-                if (ld_volatile_u64(p.bar) < target) {
-                    unsigned long long t0 = globaltimer_ns();
+        constexpr bool kWords = ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET;
+        const unsigned long long want = (unsigned long long)(b + 1);
+        if (p.G > 1) {
+            for (int c = tid; c < p.G; c += NC) {
+                const unsigned long long *f = p.flags + (size_t)c * kFlagStride;
+                if (ld_volatile_u64(f) < want) {
+                    const unsigned long long t0 = globaltimer_ns();
                     unsigned long long polls = 0;
-                    while (ld_volatile_u64(p.bar) < target) {
+                    bool ok = true;
+                    while (ld_volatile_u64(f) < want) {
                         if ((++polls & 255ull) == 0) {
-                            if (ld_volatile_i32(p.err) != kErrNone) {
-                                ok = 0;
+                            if (s_abort || ld_volatile_i32(p.err) != kErrNone) {
+                                ok = false;
                                 break;
                             }
                             if (globaltimer_ns() - t0 > p.tmo || polls > kBarrierMaxPolls) {
                                 record_err(p.err, kErrBarrierTimeout, p.step0 + b);
-                                ok = 0;
+                                ok = false;
                                 break;
                             }
                         }
                         __nanosleep(32);
                     }
+                    if (!ok) {
+                        s_abort = 1;
+                        break;
+                    }
                 }
                 __threadfence();
+                if (kWords) {
+                    const int w0 = (int)(((long long)c * p.nwords) / p.G);
+                    const int w1 = (int)(((long long)(c + 1) * p.nwords) / p.G);
+                    for (int wi = w0; wi < w1; ++wi)
+                        s_spk[wi] = __ldcg(p.spk + (size_t)cur * p.nwords + wi);
+                }
             }
-            if (s_abort)
-                ok = 0;
-            s_flag = ok;
-            if (!ok)
-                s_abort = 1;
+        } else if (kWords) {
+            for (int wi = tid; wi < p.nwords; wi += NC)
+                s_spk[wi] = __ldcg(p.spk + (size_t)cur * p.nwords + wi);
         }
+        named_sync(NC);
+        // one verdict for the whole CTA (another CTA may record an error at any
+        // moment; every consumer must take the same branch)
+        if (tid == 0)
+            s_flag = (!s_abort && ld_volatile_i32(p.err) == kErrNone) ? 1 : 0;
         named_sync(NC);
         return s_flag != 0;
     };
@@ -730,11 +755,6 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         if (!barrier_wait(b))
             return;
         SP_STAMP(tid == 0, b, B, 2);
-        if (ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET) {
-            for (int wi = tid; wi < p.nwords; wi += NC)
-                s_spk[wi] = __ldcg(p.spk + (size_t)cur * p.nwords + wi);
-            named_sync(NC);
-        }
         SP_STAMP(tid == 0, b, B, 3);
 
         // ---- recurrent input
