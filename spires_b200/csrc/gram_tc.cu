@@ -416,8 +416,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gram_tc(const __grid_constant__
 // ------------------------------------------------------ operand preparation
 
 // e[i] = exponent with max_t |x_ti| < 2^e[i] (0 for a zero column); e starts
-// at INT_MIN and is raised by atomicMax from row parts; bad[0] = 1 when any
-// fitted state is not finite.
+// very negative and is raised by atomicMax from row parts; bad[0] = 1 when
+// any fitted state is not finite.
 __global__ void k_col_exp(const double *__restrict__ X, int n, size_t t0, size_t tw, int parts,
                           int *__restrict__ e, int *__restrict__ bad)
 {
@@ -443,38 +443,60 @@ __global__ void k_col_exp(const double *__restrict__ X, int n, size_t t0, size_t
     }
 }
 
+// exponents start as the memset pattern 0x80808080 (far below any frexp
+// exponent); a column that stayed there is all zeros
 __global__ void k_exp_fix(int *e, int n_pad)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n_pad && e[i] == INT_MIN)
+    if (i < n_pad && e[i] < -100000)
         e[i] = 0;
 }
 
 // Integer slices of rows [t0, t0 + tw) of X, written K-major:
-// S[s][i][t] (n_pad x T_pad per slice; padding is zero).
-__global__ void k_slice_i8(const double *__restrict__ X, int n, size_t t0, size_t tw, int n_pad,
-                           size_t T_pad, const int *__restrict__ e, int k, signed char *__restrict__ S)
+// S[s][i][t] (n_pad x T_pad per slice; padding is zero). A block takes 128
+// rows x 32 columns through shared memory; each thread then cuts 4
+// consecutive rows of one column and writes 4 digits of a slice as one
+// 32-bit word (a warp writes 128 contiguous bytes per slice).
+__global__ void __launch_bounds__(256) k_slice_i8(const double *__restrict__ X, int n, size_t t0,
+                                                  size_t tw, int n_pad, size_t T_pad,
+                                                  const int *__restrict__ e, int k,
+                                                  signed char *__restrict__ S)
 {
-    __shared__ double tile[32][33];
-    const size_t tb = (size_t)blockIdx.y * 32;
+    __shared__ double tile[128][33];
+    const size_t tb = (size_t)blockIdx.y * 128;
     const int ib = blockIdx.x * 32;
-    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int rr = ty; rr < 128; rr += 8) {
         const size_t t = tb + rr;
-        const int i = ib + threadIdx.x;
-        tile[rr][threadIdx.x] = (t < tw && i < n) ? X[(t0 + t) * n + i] : 0.0;
+        const int i = ib + tx;
+        tile[rr][tx] = (t < tw && i < n) ? X[(t0 + t) * n + i] : 0.0;
     }
     __syncthreads();
     const size_t slice = (size_t)n_pad * T_pad;
-    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
-        const int i = ib + rr;
-        const size_t t = tb + threadIdx.x;
-        const double x = ldexp(tile[threadIdx.x][rr], -e[i]);
-        double v = __dmul_rn(x, 64.0);
-        for (int s = 0; s < k; ++s) {
-            const double d = rint(v);
-            S[s * slice + (size_t)i * T_pad + t] = (signed char)(int)d;
-            v = __dmul_rn(__dsub_rn(v, d), 128.0);
+    for (int r = 0; r < 4; ++r) {
+        const int il = ty + 8 * r;
+        const int i = ib + il;
+        const int ex = e[i];
+        unsigned w[kMaxSlices];
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q)
+            w[q] = 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double v = __dmul_rn(ldexp(tile[4 * tx + j][il], -ex), 64.0);
+#pragma unroll
+            for (int q = 0; q < kMaxSlices; ++q) {
+                if (q < k) {
+                    const double d = rint(v);
+                    w[q] |= ((unsigned)(int)d & 0xffu) << (8 * j);
+                    v = __dmul_rn(__dsub_rn(v, d), 128.0);
+                }
+            }
         }
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q)
+            if (q < k)
+                *(unsigned *)(S + q * slice + (size_t)i * T_pad + tb + 4 * tx) = w[q];
     }
 }
 
@@ -591,9 +613,9 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
         return SP_EINTERNAL;
     const size_t tw = t1 - t0;
     const int esz = mode == SP_GRAM_INT8 ? 1 : (mode == SP_GRAM_BF16X3 ? 2 : 4);
-    // rows padded to a multiple of 64 elements (whole K chunks in every mode,
-    // whole 32-row tiles for the split kernels)
-    const size_t T_pad = ((tw ? tw : 1) + 63) / 64 * 64;
+    // rows padded to a multiple of 128 elements (whole K chunks in every mode,
+    // whole row tiles for the split kernels)
+    const size_t T_pad = ((tw ? tw : 1) + 127) / 128 * 128;
     if (T_pad * esz / kChunk > (size_t)INT_MAX)
         return SP_EINVAL;
     const int n_pad = (n + kTileM - 1) / kTileM * kTileM;
@@ -674,19 +696,15 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
     if (!rc) {
         const dim3 g(n_pad / 32, (unsigned)(T_pad / 32)), blk(32, 8);
         if (mode == SP_GRAM_INT8) {
-            // exponents start at INT_MIN (bytes 0x80000000 are not a memset value)
-            std::vector<int> init(n_pad, INT_MIN);
-            if (cudaMemcpyAsync(ex, init.data(), (size_t)n_pad * sizeof(int),
-                                cudaMemcpyHostToDevice, s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess)
+            if (cudaMemsetAsync(ex, 0x80, (size_t)n_pad * sizeof(int), s) != cudaSuccess)
                 rc = SP_EINTERNAL;
             if (!rc) {
                 const int parts = 64;
                 k_col_exp<<<dim3((n + 31) / 32, parts), 256, 0, s>>>(X, n, t0, tw, parts, ex,
                                                                       flags + 2);
                 k_exp_fix<<<(n_pad + 255) / 256, 256, 0, s>>>(ex, n_pad);
-                k_slice_i8<<<g, blk, 0, s>>>(X, n, t0, tw, n_pad, T_pad, ex, slices,
-                                             (signed char *)S);
+                k_slice_i8<<<dim3(n_pad / 32, (unsigned)(T_pad / 128)), 256, 0, s>>>(
+                    X, n, t0, tw, n_pad, T_pad, ex, slices, (signed char *)S);
             }
         } else if (mode == SP_GRAM_BF16X3) {
             k_split_hl<__nv_bfloat16><<<g, blk, 0, s>>>(X, n, t0, tw, n_pad, T_pad,
@@ -696,15 +714,6 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
         }
         if (!rc && cudaGetLastError() != cudaSuccess)
             rc = SP_EINTERNAL;
-    }
-    if (!rc && mode == SP_GRAM_INT8) {
-        // a state that is not finite: leave the Gram to the FP64 path
-        if (cudaMemcpyAsync(hflags, flags, 4 * sizeof(int), cudaMemcpyDeviceToHost, s) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess)
-            rc = SP_EINTERNAL;
-        else if (hflags[2])
-            rc = SP_EINVAL;
     }
     if (!rc) {
         const CUtensorMapDataType dt = mode == SP_GRAM_INT8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
@@ -730,7 +739,14 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
             rc = launch_gram<SP_GRAM_TF32X3>(s, p, smem);
     }
     if (!rc) {
-        if (cudaMemcpyAsync(hflags, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, s) !=
+        k_mirror<<<1024, 256, 0, s>>>(C, n, ldc);
+        if (cudaGetLastError() != cudaSuccess)
+            rc = SP_EINTERNAL;
+    }
+    // one wait for everything: a wait that ran out in the kernel, or (INT8) a
+    // state that is not finite, in which case the caller takes the FP64 Gram
+    if (!rc) {
+        if (cudaMemcpyAsync(hflags, flags, 4 * sizeof(int), cudaMemcpyDeviceToHost, s) !=
                 cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
             rc = SP_EINTERNAL;
@@ -738,12 +754,9 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
             if (getenv("SPIRES_DEBUG"))
                 fprintf(stderr, "spires: Gram kernel wait ran out (role %d)\n", hflags[1]);
             rc = SP_EINTERNAL;
+        } else if (mode == SP_GRAM_INT8 && hflags[2]) {
+            rc = SP_EINVAL;
         }
-    }
-    if (!rc) {
-        k_mirror<<<1024, 256, 0, s>>>(C, n, ldc);
-        if (cudaGetLastError() != cudaSuccess)
-            rc = SP_EINTERNAL;
     }
     if (S)
         sp_cuda_free_async(S, s);
