@@ -413,6 +413,254 @@ __global__ void __launch_bounds__(kThreads, 1) k_gram_tc(const __grid_constant__
     }
 }
 
+// ------------------------------------------------ level-by-level variant
+// 128 x 256 output tiles (N = 256: the shape at which a tcgen05.mma keeps the
+// tensor pipe full) and one level at a time: the MMA warp accumulates every
+// digit pair of level lv over the rows into one of two 256-column TMEM
+// buffers, then the next level into the other while the epilogue drains the
+// first. The FP64 combination of the levels runs through the output (or a
+// scratch for later row segments) in memory: the first level written, each
+// smaller one added, the last scaled by 2^(e_i+e_j-12) -- the same operations
+// in the same order as the all-levels kernel, so the two give the same bits.
+constexpr int kTileNL = 256;
+
+struct GPL {
+    int mode, nlev, nst, n, n_pad, tiles_i, ntiles, chunks, seg_chunks;
+    unsigned idesc;
+    signed char pa[kMaxProd], pb[kMaxProd];
+    int lv_first[kMaxSlices + 1];  // products of level lv: [lv_first[lv], lv_first[lv + 1])
+    const int *exps;
+    double *C, *V;                 // output; per-segment sums of later row segments
+    int ldc;
+    int *err;
+    alignas(64) CUtensorMap map;
+};
+
+// tile t -> (I, J): row block I (128 rows) has floor(I / 2) + 1 column blocks
+// of 256 in the lower triangle
+__device__ __forceinline__ void tile_ij_l(int t, int *I, int *J)
+{
+    int i = 0, base = 0;
+    while (base + i / 2 + 1 <= t) {
+        base += i / 2 + 1;
+        ++i;
+    }
+    *I = i;
+    *J = t - base;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1) k_gram_lv(const __grid_constant__ GPL p)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem =
+        (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    constexpr int stage_bytes = 6 * kBox;  // A: 2 boxes (128 rows), B: 4 boxes (256 rows)
+    unsigned long long *full = (unsigned long long *)(smem + (size_t)p.nst * stage_bytes);
+    unsigned long long *empty = full + p.nst;
+    unsigned long long *tfull = empty + p.nst;   // [2]
+    unsigned long long *tempty = tfull + 2;      // [2]
+    unsigned long long *mdone = tempty + 2;
+    unsigned *tmem_slot = (unsigned *)(mdone + 1);
+    __shared__ volatile int s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        for (int s = 0; s < p.nst; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);
+        }
+        mbar_init(mdone, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                         smem_u32(tmem_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tmem_slot;
+    const int segs = (p.chunks + p.seg_chunks - 1) / p.seg_chunks;
+    const int xstep = kChunk / (MODE == SP_GRAM_INT8 ? 1 : (MODE == SP_GRAM_BF16X3 ? 2 : 4));
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- producer
+        if (lane == 0) {
+            long long q = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+                int I, J;
+                tile_ij_l(t, &I, &J);
+                for (int sg = 0; sg < segs && ok; ++sg) {
+                    const int c0 = sg * p.seg_chunks;
+                    const int c1 = (c0 + p.seg_chunks < p.chunks) ? c0 + p.seg_chunks : p.chunks;
+                    for (int lv = p.nlev - 1; lv >= 0 && ok; --lv) {
+                        for (int k = p.lv_first[lv]; k < p.lv_first[lv + 1] && ok; ++k) {
+                            const int rowA = p.pa[k] * p.n_pad + I * kTileM;
+                            const int rowB = p.pb[k] * p.n_pad + J * kTileNL;
+                            for (int c = c0; c < c1; ++c, ++q) {
+                                const int st = (int)(q % p.nst);
+                                const long long round = q / p.nst;
+                                if (round > 0 &&
+                                    !wait_bar(&empty[st], (unsigned)((round - 1) & 1), p.err,
+                                              &s_abort, 1)) {
+                                    ok = false;
+                                    break;
+                                }
+                                unsigned char *A = smem + (size_t)st * stage_bytes;
+                                mbar_expect_tx(&full[st], (unsigned)stage_bytes);
+                                for (int b = 0; b < 2; ++b)
+                                    tma_load_2d(A + b * kBox, &p.map, c * xstep, rowA + 64 * b,
+                                                &full[st]);
+                                for (int b = 0; b < 4; ++b)
+                                    tma_load_2d(A + (2 + b) * kBox, &p.map, c * xstep,
+                                                rowB + 64 * b, &full[st]);
+                            }
+                        }
+                    }
+                }
+            }
+            const unsigned long long t0 = gtimer();
+            for (long long qq = (q > p.nst ? q - p.nst : 0); qq < q; ++qq) {
+                const int st = (int)(qq % p.nst);
+                while (!mbar_try(&full[st], (unsigned)((qq / p.nst) & 1)))
+                    if (gtimer() - t0 > kWaitNs)
+                        break;
+            }
+        }
+    } else if (warp == 1) {
+        // -------------------------------------------------------------- MMA
+        if (lane == 0) {
+            long long q = 0, pass = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+                for (int sg = 0; sg < segs && ok; ++sg) {
+                    const int c0 = sg * p.seg_chunks;
+                    const int c1 = (c0 + p.seg_chunks < p.chunks) ? c0 + p.seg_chunks : p.chunks;
+                    for (int lv = p.nlev - 1; lv >= 0 && ok; --lv, ++pass) {
+                        const int buf = (int)(pass & 1);
+                        if (pass >= 2 && !wait_bar(&tempty[buf], (unsigned)(((pass >> 1) - 1) & 1),
+                                                   p.err, &s_abort, 2)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const unsigned td = tmem + (unsigned)(buf * kTileNL);
+                        for (int k = p.lv_first[lv]; k < p.lv_first[lv + 1] && ok; ++k) {
+                            for (int c = c0; c < c1; ++c, ++q) {
+                                const int st = (int)(q % p.nst);
+                                if (!wait_bar(&full[st], (unsigned)((q / p.nst) & 1), p.err,
+                                              &s_abort, 3)) {
+                                    ok = false;
+                                    break;
+                                }
+                                tc_fence_after();
+                                const unsigned a0 = smem_u32(smem + (size_t)st * stage_bytes);
+                                const unsigned b0 = a0 + 2 * kBox;
+                                const bool first = (k == p.lv_first[lv]) && (c == c0);
+#pragma unroll
+                                for (int kk = 0; kk < 2; ++kk)
+                                    mma<MODE>(td, sdesc(a0 + kk * 32), sdesc(b0 + kk * 32),
+                                              p.idesc, !(first && kk == 0));
+                                tc_commit(&empty[st]);
+                            }
+                        }
+                        if (ok)
+                            tc_commit(&tfull[buf]);
+                    }
+                }
+            }
+            tc_commit(mdone);
+            const unsigned long long t0 = gtimer();
+            while (!mbar_try(mdone, 0))
+                if (gtimer() - t0 > kWaitNs)
+                    break;
+        }
+        __syncwarp();
+    } else {
+        // --------------------------------------------------------- epilogue
+        const int qd = warp & 3;
+        const int r = qd * 32 + lane;
+        long long pass = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+            int I, J;
+            tile_ij_l(t, &I, &J);
+            const int i = I * kTileM + r;
+            const int ei = (MODE == SP_GRAM_INT8 && i < p.n_pad) ? __ldg(p.exps + i) : 0;
+            for (int sg = 0; sg < segs && ok; ++sg) {
+                double *vb = sg == 0 ? p.C : p.V;
+                for (int lv = p.nlev - 1; lv >= 0 && ok; --lv, ++pass) {
+                    const int buf = (int)(pass & 1);
+                    int okw = 1;
+                    if (lane == 0)
+                        okw = wait_bar(&tfull[buf], (unsigned)((pass >> 1) & 1), p.err, &s_abort,
+                                       4)
+                                  ? 1
+                                  : 0;
+                    okw = __shfl_sync(0xffffffffu, okw, 0);
+                    if (!okw) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const double sl = MODE == SP_GRAM_INT8 ? ldexp(1.0, -7 * lv) : 1.0;
+                    const bool firstlv = lv == p.nlev - 1, lastlv = lv == 0;
+                    for (int cc = 0; cc < kTileNL / 16; ++cc) {
+                        unsigned a[16];
+                        tmem_ld16(tmem + ((unsigned)(qd * 32) << 16) +
+                                      (unsigned)(buf * kTileNL + cc * 16),
+                                  a);
+                        if (i >= p.n)
+                            continue;
+                        double *vrow = vb + (size_t)i * p.ldc;
+                        double *crow = p.C + (size_t)i * p.ldc;
+#pragma unroll
+                        for (int c = 0; c < 16; ++c) {
+                            const int j = J * kTileNL + cc * 16 + c;
+                            if (j >= p.n)
+                                continue;
+                            double v;
+                            if (MODE == SP_GRAM_INT8) {
+                                const double x = __dmul_rn((double)(int)a[c], sl);
+                                v = firstlv ? x : __dadd_rn(vrow[j], x);
+                            } else {
+                                v = (double)__uint_as_float(a[c]);
+                            }
+                            if (!lastlv) {
+                                vrow[j] = v;
+                            } else {
+                                if (MODE == SP_GRAM_INT8)
+                                    v = ldexp(v, ei + __ldg(p.exps + j) - 12);
+                                crow[j] = sg == 0 ? v : __dadd_rn(crow[j], v);
+                            }
+                        }
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0)
+                        mbar_arrive(&tempty[buf]);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem)
+                     : "memory");
+    }
+}
+
 // ------------------------------------------------------ operand preparation
 
 // e[i] = exponent with max_t |x_ti| < 2^e[i] (0 for a zero column); e starts
@@ -595,6 +843,21 @@ int launch_gram(cudaStream_t s, GP &p, size_t smem)
     return cudaGetLastError() == cudaSuccess ? SP_OK : SP_EINTERNAL;
 }
 
+template <int MODE>
+int launch_gram_lv(cudaStream_t s, GPL &q, size_t smem)
+{
+    auto fn = k_gram_lv<MODE>;
+    if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return SP_EINTERNAL;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = q.ntiles < sms ? q.ntiles : sms;
+    fn<<<grid, kThreads, smem, s>>>(q);
+    return cudaGetLastError() == cudaSuccess ? SP_OK : SP_EINTERNAL;
+}
+
 }  // namespace
 
 extern "C" int sp_gram_tc_available(void) { return device_ok(); }
@@ -618,7 +881,12 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
     const size_t T_pad = ((tw ? tw : 1) + 127) / 128 * 128;
     if (T_pad * esz / kChunk > (size_t)INT_MAX)
         return SP_EINVAL;
-    const int n_pad = (n + kTileM - 1) / kTileM * kTileM;
+    // the level-by-level kernel (128 x 256 tiles) unless the all-levels one
+    // (128 x 64 tiles) is asked for
+    const char *kv = getenv("SPIRES_GRAM_KERNEL");
+    const bool lvk = !(kv && !strcmp(kv, "wide"));
+    const int n_pad = lvk ? (n + kTileNL - 1) / kTileNL * kTileNL
+                          : (n + kTileM - 1) / kTileM * kTileM;
     const int ns = mode == SP_GRAM_INT8 ? slices : 2;
 
     GP p;
@@ -667,22 +935,53 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
     p.idesc = (cfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((unsigned)(kTileN >> 3) << 17) |
               ((unsigned)(kTileM >> 4) << 24);
 
-    const size_t stage_bytes = (size_t)ns * 3 * kBox;
+    // the level kernel's parameters: the same products, by level
+    GPL q;
+    memset(&q, 0, sizeof(q));
+    q.mode = mode;
+    q.nlev = p.nlev;
+    q.n = n;
+    q.n_pad = n_pad;
+    q.tiles_i = n_pad / kTileM;
+    for (int I = 0; I < q.tiles_i; ++I)
+        q.ntiles += I / 2 + 1;
+    q.chunks = p.chunks;
+    q.seg_chunks = p.seg_chunks;
+    for (int k = 0; k < np; ++k) {
+        q.pa[k] = p.pa[k];
+        q.pb[k] = p.pb[k];
+    }
+    for (int lv = 0; lv <= p.nlev; ++lv)
+        q.lv_first[lv] = mode == SP_GRAM_INT8 ? lv * (lv + 1) / 2 : (lv == 0 ? 0 : 3);
+    q.idesc = (cfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((unsigned)(kTileNL >> 3) << 17) |
+              ((unsigned)(kTileM >> 4) << 24);
+    q.C = C;
+    q.ldc = ldc;
+    const int segs = (p.chunks + p.seg_chunks - 1) / p.seg_chunks;
+
+    const size_t stage_bytes = lvk ? (size_t)6 * kBox : (size_t)ns * 3 * kBox;
     int dev = 0, smem_max = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t fixed = 1024 + 256;
     long long nst = ((long long)smem_max - (long long)fixed) / (long long)stage_bytes;
-    if (nst > 6)
-        nst = 6;
+    if (nst > (lvk ? 8 : 6))
+        nst = lvk ? 8 : 6;
     if (nst < 2)
         return SP_EINVAL;
     p.nst = (int)nst;
+    q.nst = (int)nst;
     const size_t smem = fixed + (size_t)nst * stage_bytes;
 
     void *S = nullptr;
     int *ex = nullptr, *flags = nullptr;
+    double *V = nullptr;
     int rc = SP_OK;
+    if (lvk && segs > 1 &&
+        sp_cuda_malloc_async(&V, (size_t)n * ldc * sizeof(double), s) != cudaSuccess) {
+        cudaGetLastError();
+        return SP_EALLOC;
+    }
     const size_t sbytes = (size_t)ns * n_pad * T_pad * esz;
     if (sp_cuda_malloc_async(&S, sbytes, s) != cudaSuccess ||
         sp_cuda_malloc_async(&ex, (size_t)n_pad * sizeof(int), s) != cudaSuccess ||
@@ -727,8 +1026,19 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
                       CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             rc = SP_EINTERNAL;
+        q.map = p.map;
     }
-    if (!rc) {
+    if (!rc && lvk) {
+        q.exps = ex;
+        q.err = flags;
+        q.V = V;
+        if (mode == SP_GRAM_INT8)
+            rc = launch_gram_lv<SP_GRAM_INT8>(s, q, smem);
+        else if (mode == SP_GRAM_BF16X3)
+            rc = launch_gram_lv<SP_GRAM_BF16X3>(s, q, smem);
+        else
+            rc = launch_gram_lv<SP_GRAM_TF32X3>(s, q, smem);
+    } else if (!rc) {
         p.exps = ex;
         p.err = flags;
         if (mode == SP_GRAM_INT8)
@@ -764,6 +1074,8 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
         sp_cuda_free_async(ex, s);
     if (flags)
         sp_cuda_free_async(flags, s);
+    if (V)
+        sp_cuda_free_async(V, s);
     return rc;
 }
 
