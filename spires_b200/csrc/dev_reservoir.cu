@@ -312,7 +312,7 @@ static size_t coef_smem_bytes(const sp_dev *d)
 // ring-row stages and their full/empty mbarriers
 static size_t launch_smem(const sp_dev *d, const sp_launch &l)
 {
-    size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) +
+    size_t spk = (l.variant == 1 ? 2 : 1) * (((d->nwords * 4) + 127) & ~(size_t)127) +
                  csr_smem_bytes(csr_smem_edges(d, l), l.warps_max);
     if (l.variant == 1) {
         int bw, nbx;
@@ -391,11 +391,14 @@ static void default_launch(sp_dev *d)
     if (d->ntype == SP_FLIF_GL && d->nc.L >= 32 && l.warps_max <= kPipeWarps) {
         // The ring stream is paced by the bytes in flight per SM (the stages
         // the consumers are not reading): long rings take the stage height of
-        // 64, 56 or 48 rows that puts the most rows in flight (ties: taller),
-        // shorter rings 32-row stages.
+        // 64 or 48 rows that puts the most rows in flight (ties: taller),
+        // shorter rings 32-row stages. (N=20000, L=1024 on 148 SMs: 3 x 48
+        // rows, 31.7 us per step, against 31.9 for 2 x 64 and 33.0 for 3 x 56,
+        // whose extra bytes in flight slow the serial phase's loads more than
+        // they speed the stream.)
         sp_launch best = l;
         long long best_rows = 0;
-        for (int rows : {64, 56, 48, 32}) {
+        for (int rows : {64, 48, 32}) {
             if ((rows > 32) != (d->nc.L >= 512))
                 continue;
             sp_launch v = l;
@@ -405,7 +408,8 @@ static void default_launch(sp_dev *d)
             box_geometry(d, v, &bw, &nbx);
             const size_t stage = (size_t)v.rows * nbx * bw * sizeof(double);
             const size_t budget = (size_t)(max_smem(d) - 2 * 1024);
-            const size_t spk = (((d->nwords * 4) + 127) & ~(size_t)127) + coef_smem_bytes(d) +
+            const size_t spk = 2 * (((d->nwords * 4) + 127) & ~(size_t)127) +
+                               coef_smem_bytes(d) +
                                csr_smem_bytes(csr_smem_edges(d, v), v.warps_max);
             long long st = budget > spk ? (long long)((budget - spk) / (stage + 16)) : 0;
             if (st > 16)
@@ -836,7 +840,8 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     if (!fn)
         return SP_EINVAL;
     const size_t smem = launch_smem(d, l);
-    dim3 grid(l.ctas), block(32 * (l.warps_max + (l.variant == 1 ? 1 : 0)));
+    // variant 1: consumer warps, the producer warp and the gather warp
+    dim3 grid(l.ctas), block(32 * (l.warps_max + (l.variant == 1 ? 2 : 0)));
     if (smem > 48 * 1024)
         SP_CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
@@ -1100,7 +1105,7 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
             SP_CK(cudaFuncSetAttribute((const void *)fn,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        const int threads = 32 * (l->warps_max + (l->variant == 1 ? 1 : 0));
+        const int threads = 32 * (l->warps_max + (l->variant == 1 ? 2 : 0));
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, threads,
                                                           smem) != cudaSuccess)
             return SP_EINTERNAL;
@@ -1202,7 +1207,7 @@ extern "C" int sp_dev_autotune(sp_dev *d, size_t steps)
                 int bw, nbx;
                 box_geometry(d, v, &bw, &nbx);
                 const size_t stage = (size_t)rows * nbx * bw * 8;
-                const size_t base = (((d->nwords * 4) + 127) & ~(size_t)127) +
+                const size_t base = 2 * (((d->nwords * 4) + 127) & ~(size_t)127) +
                                     coef_smem_bytes(d) +
                                     csr_smem_bytes(csr_smem_edges(d, v), v.warps_max);
                 const size_t budget = (size_t)(max_smem(d) - 8 * 1024);

@@ -324,7 +324,7 @@ constexpr int kPipeWarps = 8;
 
 template <int VAR>
 struct Bounds {
-    static constexpr int threads = VAR == 1 ? 32 * (kPipeWarps + 1) : 1024;
+    static constexpr int threads = VAR == 1 ? 32 * (kPipeWarps + 2) : 1024;
 };
 
 // Variant 1 keeps lags 2..kRegLags+1 of its own neuron in registers: they are
@@ -341,6 +341,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     __shared__ int s_flag;
     __shared__ volatile int s_abort;
     __shared__ volatile int s_done;
+    __shared__ volatile int s_gather;  // variant 1: barriers whose words are staged
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -351,8 +352,11 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     const int L = p.L;
     const long long B = (long long)p.n_macro * p.micro;
 
-    unsigned *s_spk = (unsigned *)smem;
-    const size_t spk_bytes0 = (((size_t)p.nwords * 4) + 127) & ~(size_t)127;
+    // spike words of the barrier: one buffer, or two (variant 1: the gather
+    // warp fills barrier b + 1's while the row pass reads barrier b's)
+    const size_t spk_one = (((size_t)p.nwords * 4) + 127) & ~(size_t)127;
+    unsigned *s_spkb = (unsigned *)smem;
+    const size_t spk_bytes0 = (VAR == 1 ? 2 : 1) * spk_one;
     // CSR slice (SIMPLE synapse), between the spike words and the rest
     double *s_csr_w = (double *)(smem + spk_bytes0);
     const size_t csr_w_bytes = ((size_t)p.csr_cap * 8 + 127) / 128 * 128;
@@ -377,6 +381,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     if (tid == 0) {
         s_abort = 0;
         s_done = 0;
+        s_gather = 0;
     }
     if (VAR == 1 && p.coef_smem)
         for (int k = tid; k < L; k += blockDim.x)
@@ -403,6 +408,62 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     __syncthreads();
 
     // ------------------------------------------------------------ producer
+    // ------------------------------------------------------------ gatherer
+    // Variant 1, one warp: for barrier b it watches the arrival flags of all
+    // CTAs (lane l: CTAs l, l + 32, ...), copies each CTA's spike words into
+    // s_spkb[b & 1] as soon as that CTA's flag is up, and announces the
+    // barrier in s_gather -- while the consumers are still summing history.
+    // Buffer b & 1 is free by then: a flag can reach b + 1 only after this
+    // CTA's arrival at barrier b - 1, which follows its row pass of b - 2.
+    if (VAR == 1 && tid >= NC + 32) {
+        constexpr bool kWords = ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET;
+        if (p.G <= 1)
+            return;
+        for (long long b = 0; b < B; ++b) {
+            const unsigned long long want = (unsigned long long)(b + 1);
+            const int curb = p.phase0 ^ (int)(b & 1);
+            unsigned *dst = s_spkb + (size_t)(b & 1) * (spk_one / 4);
+            bool ok = true;
+            for (int c = lane; c < p.G && ok; c += 32) {
+                const unsigned long long *f = p.flags + (size_t)c * kFlagStride;
+                if (ld_volatile_u64(f) < want) {
+                    const unsigned long long t0 = globaltimer_ns();
+                    unsigned long long polls = 0;
+                    while (ld_volatile_u64(f) < want) {
+                        if ((++polls & 255ull) == 0) {
+                            if (s_abort || ld_volatile_i32(p.err) != kErrNone) {
+                                ok = false;
+                                break;
+                            }
+                            if (globaltimer_ns() - t0 > p.tmo || polls > kBarrierMaxPolls) {
+                                record_err(p.err, kErrBarrierTimeout, p.step0 + b);
+                                s_abort = 1;
+                                ok = false;
+                                break;
+                            }
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                if (!ok)
+                    break;
+                __threadfence();
+                if (kWords) {
+                    const int w0 = (int)(((long long)c * p.nwords) / p.G);
+                    const int w1 = (int)(((long long)(c + 1) * p.nwords) / p.G);
+                    for (int wi = w0; wi < w1; ++wi)
+                        dst[wi] = __ldcg(p.spk + (size_t)curb * p.nwords + wi);
+                }
+            }
+            if (__any_sync(kFull, !ok))
+                return;
+            __syncwarp();
+            if (lane == 0)
+                st_release_cta(&s_gather, (int)(b + 1));
+        }
+        return;
+    }
+
     if (VAR == 1 && tid >= NC) {
         if (lane != 0 || S_b == 0)
             return;
@@ -599,7 +660,29 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     auto barrier_wait = [&](long long b) -> bool {
         constexpr bool kWords = ST == SP_SYN_SIMPLE || ST == SP_SYN_PSC_HET;
         const unsigned long long want = (unsigned long long)(b + 1);
-        if (p.G > 1) {
+        unsigned *s_spk = s_spkb + (size_t)(VAR == 1 ? (b & 1) : 0) * (spk_one / 4);
+        if (VAR == 1 && p.G > 1) {
+            // the gather warp has the words: wait for its announcement
+            if (tid == 0) {
+                if (ld_acquire_cta(&s_gather) < (int)(b + 1)) {
+                    const unsigned long long t0 = globaltimer_ns();
+                    unsigned polls = 0;
+                    while (ld_acquire_cta(&s_gather) < (int)(b + 1)) {
+                        if ((++polls & 63u) == 0) {
+                            if (s_abort || ld_volatile_i32(p.err) != kErrNone)
+                                break;
+                            if (globaltimer_ns() - t0 > p.tmo) {
+                                record_err(p.err, kErrBarrierTimeout, p.step0 + b);
+                                s_abort = 1;
+                                break;
+                            }
+                        }
+                    }
+                }
+                if (!kWords)
+                    __threadfence();  // the drive in global memory is read next
+            }
+        } else if (p.G > 1) {
             for (int c = tid; c < p.G; c += NC) {
                 const unsigned long long *f = p.flags + (size_t)c * kFlagStride;
                 if (ld_volatile_u64(f) < want) {
@@ -756,6 +839,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
             return;
         SP_STAMP(tid == 0, b, B, 2);
         SP_STAMP(tid == 0, b, B, 3);
+        const unsigned *s_spk = s_spkb + (size_t)(VAR == 1 ? (b & 1) : 0) * (spk_one / 4);
 
         // ---- recurrent input
         double rec = 0.0;

@@ -83,7 +83,9 @@ def test_int8_gram_accuracy_matches_fp64():
     assert e8 <= e64 + 1e-17
 
 
-@pytest.mark.parametrize("mode,tol", [(1, 2e-4), (2, 2e-5)])
+# FP32 accumulation over 1500 rows: the split products' rounding (2^-16 for
+# BF16 hi/lo, 2^-22 for TF32) plus the sums' own, relative to |X|^T |X|
+@pytest.mark.parametrize("mode,tol", [(1, 2e-4), (2, 1e-4)])
 def test_split_grams_within_fp32_bound(mode, tol):
     X = states(1500, 190, seed=3)
     G = gram_dev(X, mode)
