@@ -86,9 +86,18 @@ typedef struct {
     int rows;         /* ring rows per stage (variant 1) */
     int csr_global;   /* 1: walk the recurrent CSR rows in global memory even
                          when the CTA's slice fits in shared memory (0 default) */
+    int l2_pin;       /* variant 1: ring slots [0, l2_pin) are loaded and stored
+                         with L2 evict-last priority and the other slots with
+                         evict-first, so that part of a ring larger than the L2
+                         stays resident from step to step; 0 = no cache hints,
+                         -1 = automatic (default: half of the L2 when the ring
+                         is larger than three quarters of it, else 0) */
 } spires_ext_launch;
 
 spires_status spires_ext_get_launch(const spires_reservoir *r, spires_ext_launch *l);
+/* Ring slots the current launch keeps L2-resident (l2_pin with -1 resolved;
+ * 0 for variant 0 or without cache hints). */
+int           spires_ext_l2_pin_rows(const spires_reservoir *r);
 spires_status spires_ext_set_launch(spires_reservoir *r, const spires_ext_launch *l);
 /* Time candidate launch shapes on this reservoir (state is saved and restored)
  * and keep the fastest. `steps` macro steps per candidate. */
@@ -205,6 +214,8 @@ typedef struct {
     int    lu_fallback;
     int    dual;             /* 1: fewer fitted rows than N/2, solved as
                                 W = Phi^T (Phi Phi^T + lambda I)^-1 Y */
+    double solve_ms;         /* the first triangular solve; factor_ms is the
+                                factorisation alone */
 } spires_ext_ridge_report;
 
 /* The Gram C = X^T X (d_C [n x n], full matrix) of device states

@@ -80,7 +80,8 @@ class ModelInfo(C.Structure):
 
 class Launch(C.Structure):
     _fields_ = [("ctas", C.c_int), ("warps_max", C.c_int), ("variant", C.c_int),
-                ("stages", C.c_int), ("rows", C.c_int), ("csr_global", C.c_int)]
+                ("stages", C.c_int), ("rows", C.c_int), ("csr_global", C.c_int),
+                ("l2_pin", C.c_int)]
 
 
 class RidgeOpts(C.Structure):
@@ -93,7 +94,7 @@ class RidgeReport(C.Structure):
                 ("rel_residual", C.c_double), ("collect_ms", C.c_double),
                 ("gram_ms", C.c_double), ("factor_ms", C.c_double),
                 ("refine_ms", C.c_double), ("factor_failed", C.c_int),
-                ("lu_fallback", C.c_int), ("dual", C.c_int)]
+                ("lu_fallback", C.c_int), ("dual", C.c_int), ("solve_ms", C.c_double)]
 
 
 class AgileOpts(C.Structure):
@@ -157,6 +158,7 @@ EXT_SIGNATURES = {
     "spires_ext_kernel_launches": (C.c_longlong, [_VP]),
     "spires_ext_read_w_in": (C.c_int, [_VP, _dp]),
     "spires_ext_get_launch": (C.c_int, [_VP, C.POINTER(Launch)]),
+    "spires_ext_l2_pin_rows": (C.c_int, [_VP]),
     "spires_ext_set_launch": (C.c_int, [_VP, C.POINTER(Launch)]),
     "spires_ext_autotune": (C.c_int, [_VP, C.c_size_t]),
     "spires_ext_set_seed": (C.c_int, [_VP, C.c_uint64]),

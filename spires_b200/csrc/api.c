@@ -492,7 +492,15 @@ SPIRES_EXPORT spires_status spires_ext_get_launch(const spires_reservoir *r,
     l->stages = s.stages;
     l->rows = s.rows;
     l->csr_global = s.csr_global;
+    l->l2_pin = s.l2_pin;
     return SPIRES_OK;
+}
+
+SPIRES_EXPORT int spires_ext_l2_pin_rows(const spires_reservoir *r)
+{
+    if (!r || !r->dev)
+        return 0;
+    return sp_dev_l2_pin_rows(r->dev);
 }
 
 SPIRES_EXPORT spires_status spires_ext_set_launch(spires_reservoir *r,
@@ -500,7 +508,8 @@ SPIRES_EXPORT spires_status spires_ext_set_launch(spires_reservoir *r,
 {
     if (!r || !r->dev || !l)
         return SPIRES_ERR_INVALID_ARG;
-    sp_launch s = {l->ctas, l->warps_max, l->variant, l->stages, l->rows, l->csr_global != 0};
+    sp_launch s = {l->ctas,   l->warps_max,          l->variant, l->stages,
+                   l->rows,   l->csr_global != 0,    l->l2_pin};
     return to_status(sp_dev_set_launch(r->dev, &s));
 }
 
@@ -736,6 +745,7 @@ SPIRES_EXPORT spires_status spires_ext_train_ridge(spires_reservoir *r,
         report->factor_failed = rep.factor_failed;
         report->lu_fallback = rep.lu_fallback;
         report->dual = rep.dual;
+        report->solve_ms = rep.solve_ms;
     }
     return to_status(rc);
 }
@@ -1110,6 +1120,7 @@ SPIRES_EXPORT spires_status spires_ext_ridge_fit(const double *states, size_t T,
         report->factor_failed = rep.factor_failed;
         report->lu_fallback = rep.lu_fallback;
         report->dual = rep.dual;
+        report->solve_ms = rep.solve_ms;
     }
     if (rc == SP_RIDGE_SINGULAR)
         return SPIRES_ERR_INTERNAL;

@@ -186,76 +186,100 @@ __global__ void k_add_diag(double *A, int n, int lda, double lam)
 
 // ------------------------------------------------------- blocked Cholesky
 // A (n x n, row-major, lower triangle used) -> L in place.
-__global__ void k_potrf_diag(double *A, int n, int lda, int k0, int kb, int *info)
+// Diagonal block of panel [k0, k0 + kb), one CTA of 256 threads: thread t
+// owns row t % 64 and the 16 columns t / 64 + 4 m of the trailing update, so
+// each column step is 16 predicated FMAs per thread between two barriers.
+__global__ void __launch_bounds__(256) k_potrf_diag(double *A, int n, int lda, int k0, int kb,
+                                                    int *info)
 {
     __shared__ double s[NB][NB + 1];
+    __shared__ int bad;
     if (*info)
         return;
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
-        int r = q / kb, c = q % kb;
+        const int r = q / kb, c = q % kb;
         s[r][c] = A[(size_t)(k0 + r) * lda + k0 + c];
     }
-    __syncthreads();
-    __shared__ int bad;
     if (threadIdx.x == 0)
         bad = 0;
     __syncthreads();
+    const int r = threadIdx.x & (NB - 1), c0 = threadIdx.x >> 6;
     for (int j = 0; j < kb; ++j) {
         if (threadIdx.x == 0) {
-            double d = s[j][j];
+            const double d = s[j][j];
             if (!(d > 0.0) || !isfinite(d)) {
-                bad = k0 + j + 1;
+                if (!bad)
+                    bad = k0 + j + 1;
                 s[j][j] = 1.0;
             } else {
                 s[j][j] = sqrt(d);
             }
         }
         __syncthreads();
-        const double djj = s[j][j];
-        for (int r = j + 1 + threadIdx.x; r < kb; r += blockDim.x)
-            s[r][j] /= djj;
+        if (threadIdx.x < NB && r > j && r < kb)
+            s[r][j] /= s[j][j];
         __syncthreads();
-        // trailing update of the diagonal block, lower part
-        for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
-            int r = q / kb, c = q % kb;
-            if (r > j && c > j && c <= r)
-                s[r][c] -= s[r][j] * s[c][j];
+        if (r > j && r < kb) {
+            const double lrj = s[r][j];
+#pragma unroll
+            for (int m = 0; m < NB / 4; ++m) {
+                const int c = c0 + 4 * m;
+                if (c > j && c <= r)
+                    s[r][c] -= lrj * s[c][j];
+            }
         }
         __syncthreads();
     }
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
-        int r = q / kb, c = q % kb;
-        if (c <= r)
-            A[(size_t)(k0 + r) * lda + k0 + c] = s[r][c];
+        const int rr = q / kb, cc = q % kb;
+        if (cc <= rr)
+            A[(size_t)(k0 + rr) * lda + k0 + cc] = s[rr][cc];
     }
     if (threadIdx.x == 0 && bad)
         atomicCAS(info, 0, bad);
 }
 
-// rows r >= k0+kb: L[r][k0:k0+kb] = A[r][k0:k0+kb] * Lkk^{-T}
-__global__ void k_trsm_panel(double *A, int n, int lda, int k0, int kb, const int *info)
+// Rows r >= k0 + kb: L[r][k0:k0+kb] = A[r][k0:k0+kb] L_kk^-T. One warp per
+// row, lane l holding columns l and l + 32; columns are eliminated in order
+// (x_c = a_c / L_cc, then a_q -= x_c L_qc for q > c). 32 rows per CTA.
+__global__ void __launch_bounds__(256) k_trsm_panel(double *A, int n, int lda, int k0, int kb,
+                                                    const int *info)
 {
-    __shared__ double L[NB][NB + 1];
+    __shared__ double sL[NB][NB + 1];
     if (*info)
         return;
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
-        int r = q / kb, c = q % kb;
-        L[r][c] = (c <= r) ? A[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
+        const int r = q / kb, c = q % kb;
+        sL[r][c] = (c <= r) ? A[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
     }
     __syncthreads();
-    const int r = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n)
-        return;
-    double x[NB];
-    double *row = A + (size_t)r * lda + k0;
-    for (int c = 0; c < kb; ++c) {
-        double v = row[c];
-        for (int q = 0; q < c; ++q)
-            v -= x[q] * L[c][q];
-        x[c] = v / L[c][c];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = 0; k < 4; ++k) {
+        const int r = k0 + kb + blockIdx.x * 32 + k * 8 + warp;
+        if (r >= n)
+            return;
+        double *row = A + (size_t)r * lda + k0;
+        double a0 = lane < kb ? row[lane] : 0.0;
+        double a1 = lane + 32 < kb ? row[lane + 32] : 0.0;
+        for (int c = 0; c < kb; ++c) {
+            const double ac = __shfl_sync(kFull, c < 32 ? a0 : a1, c & 31);
+            const double xc = ac / sL[c][c];
+            if (lane == (c & 31)) {
+                if (c < 32)
+                    a0 = xc;
+                else
+                    a1 = xc;
+            }
+            if (lane > c && lane < kb)
+                a0 = fma(-xc, sL[lane][c], a0);
+            if (lane + 32 > c && lane + 32 < kb)
+                a1 = fma(-xc, sL[lane + 32][c], a1);
+        }
+        if (lane < kb)
+            row[lane] = a0;
+        if (lane + 32 < kb)
+            row[lane + 32] = a1;
     }
-    for (int c = 0; c < kb; ++c)
-        row[c] = x[c];
 }
 
 // trailing update A22 -= L21 L21^T on lower tiles of the trailing matrix
@@ -309,48 +333,106 @@ __global__ void __launch_bounds__(256) k_syrk_update(double *A, int n, int lda, 
 }
 
 // ----------------------------------------------------- triangular solves
-// Forward L Z = B in place on Z (n x dout), panel by panel.
-__global__ void k_fwd_diag(const double *L, int lda, int k0, int kb, double *Z, int dout)
+// Forward L Z = B in place on Z (n x dout), panel by panel: the diagonal
+// block by one CTA (warp w takes outputs w, w + 8, ...; lane l holds rows l
+// and l + 32; columns eliminated in order), then the rows below it.
+__global__ void __launch_bounds__(256) k_fwd_diag(const double *L, int lda, int k0, int kb,
+                                                  double *Z, int dout)
 {
-    const int o = threadIdx.x;
-    if (o >= dout)
-        return;
-    for (int r = 0; r < kb; ++r) {
-        double v = Z[(size_t)(k0 + r) * dout + o];
-        for (int c = 0; c < r; ++c)
-            v -= L[(size_t)(k0 + r) * lda + k0 + c] * Z[(size_t)(k0 + c) * dout + o];
-        Z[(size_t)(k0 + r) * dout + o] = v / L[(size_t)(k0 + r) * lda + k0 + r];
+    __shared__ double sL[NB][NB + 1];
+    for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+        const int r = q / kb, c = q % kb;
+        sL[r][c] = (c <= r) ? L[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int o = warp; o < dout; o += 8) {
+        double z0 = lane < kb ? Z[(size_t)(k0 + lane) * dout + o] : 0.0;
+        double z1 = lane + 32 < kb ? Z[(size_t)(k0 + lane + 32) * dout + o] : 0.0;
+        for (int j = 0; j < kb; ++j) {
+            const double zj = __shfl_sync(kFull, j < 32 ? z0 : z1, j & 31) / sL[j][j];
+            if (lane == (j & 31)) {
+                if (j < 32)
+                    z0 = zj;
+                else
+                    z1 = zj;
+            }
+            if (lane > j && lane < kb)
+                z0 = fma(-zj, sL[lane][j], z0);
+            if (lane + 32 > j && lane + 32 < kb)
+                z1 = fma(-zj, sL[lane + 32][j], z1);
+        }
+        if (lane < kb)
+            Z[(size_t)(k0 + lane) * dout + o] = z0;
+        if (lane + 32 < kb)
+            Z[(size_t)(k0 + lane + 32) * dout + o] = z1;
     }
 }
 
-__global__ void k_fwd_update(const double *L, int n, int lda, int k0, int kb, double *Z, int dout)
+// Rows r >= k0 + kb: Z[r] -= L[r][k0:k0+kb] Z[k0:k0+kb]; one warp per row.
+__global__ void __launch_bounds__(256) k_fwd_update(const double *L, int n, int lda, int k0,
+                                                    int kb, double *Z, int dout)
 {
-    const int r = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = k0 + kb + blockIdx.x * 8 + warp;
     if (r >= n)
         return;
+    const double *Lr = L + (size_t)r * lda + k0;
+    const double l0 = lane < kb ? Lr[lane] : 0.0;
+    const double l1 = lane + 32 < kb ? Lr[lane + 32] : 0.0;
     for (int o = 0; o < dout; ++o) {
         double v = 0.0;
-        for (int c = 0; c < kb; ++c)
-            v = fma(L[(size_t)r * lda + k0 + c], Z[(size_t)(k0 + c) * dout + o], v);
-        Z[(size_t)r * dout + o] -= v;
+        if (lane < kb)
+            v = l0 * Z[(size_t)(k0 + lane) * dout + o];
+        if (lane + 32 < kb)
+            v = fma(l1, Z[(size_t)(k0 + lane + 32) * dout + o], v);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            v += __shfl_xor_sync(kFull, v, off);
+        if (lane == 0)
+            Z[(size_t)r * dout + o] -= v;
     }
 }
 
-// Backward L^T X = Z, panels from the last one.
-__global__ void k_bwd_diag(const double *L, int lda, int k0, int kb, double *Z, int dout)
+// Backward L^T X = Z, panels from the last one: the diagonal block (rows
+// eliminated from the last, x_j = z_j / L_jj, z_r -= L_jr x_j for r < j).
+__global__ void __launch_bounds__(256) k_bwd_diag(const double *L, int lda, int k0, int kb,
+                                                  double *Z, int dout)
 {
-    const int o = threadIdx.x;
-    if (o >= dout)
-        return;
-    for (int r = kb - 1; r >= 0; --r) {
-        double v = Z[(size_t)(k0 + r) * dout + o];
-        for (int c = r + 1; c < kb; ++c)
-            v -= L[(size_t)(k0 + c) * lda + k0 + r] * Z[(size_t)(k0 + c) * dout + o];
-        Z[(size_t)(k0 + r) * dout + o] = v / L[(size_t)(k0 + r) * lda + k0 + r];
+    __shared__ double sL[NB][NB + 1];
+    for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+        const int r = q / kb, c = q % kb;
+        sL[r][c] = (c <= r) ? L[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int o = warp; o < dout; o += 8) {
+        double z0 = lane < kb ? Z[(size_t)(k0 + lane) * dout + o] : 0.0;
+        double z1 = lane + 32 < kb ? Z[(size_t)(k0 + lane + 32) * dout + o] : 0.0;
+        for (int j = kb - 1; j >= 0; --j) {
+            const double xj = __shfl_sync(kFull, j < 32 ? z0 : z1, j & 31) / sL[j][j];
+            if (lane == (j & 31)) {
+                if (j < 32)
+                    z0 = xj;
+                else
+                    z1 = xj;
+            }
+            if (lane < j)
+                z0 = fma(-xj, sL[j][lane], z0);
+            if (lane + 32 < j)
+                z1 = fma(-xj, sL[j][lane + 32], z1);
+        }
+        if (lane < kb)
+            Z[(size_t)(k0 + lane) * dout + o] = z0;
+        if (lane + 32 < kb)
+            Z[(size_t)(k0 + lane + 32) * dout + o] = z1;
     }
 }
 
-__global__ void k_bwd_update(const double *L, int lda, int k0, int kb, double *Z, int dout)
+// Rows i < k0: Z[i] -= L[k0:k0+kb][i]^T X[k0:k0+kb]; one thread per row
+// (coalesced along the rows of L).
+__global__ void __launch_bounds__(256) k_bwd_update(const double *L, int lda, int k0, int kb,
+                                                    double *Z, int dout)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;  // rows i < k0
     if (i >= k0)
@@ -648,7 +730,7 @@ static int cholesky_inplace(cudaStream_t s, double *A, int n, int *d_info)
         k_potrf_diag<<<1, 256, 0, s>>>(A, n, n, k0, kb, d_info);
         const int rest = n - k0 - kb;
         if (rest > 0) {
-            k_trsm_panel<<<(rest + 63) / 64, 64, 0, s>>>(A, n, n, k0, kb, d_info);
+            k_trsm_panel<<<(rest + 31) / 32, 256, 0, s>>>(A, n, n, k0, kb, d_info);
             const int nt = (rest + 63) / 64;
             k_syrk_update<<<nt * (nt + 1) / 2, 256, 0, s>>>(A, n, n, k0, kb, d_info);
         }
@@ -663,17 +745,17 @@ static void chol_solve(cudaStream_t s, const double *L, int n, double *Z, int do
 {
     for (int k0 = 0; k0 < n; k0 += NB) {
         const int kb = (n - k0 < NB) ? n - k0 : NB;
-        k_fwd_diag<<<1, 32, 0, s>>>(L, n, k0, kb, Z, dout);
+        k_fwd_diag<<<1, 256, 0, s>>>(L, n, k0, kb, Z, dout);
         const int rest = n - k0 - kb;
         if (rest > 0)
-            k_fwd_update<<<(rest + 127) / 128, 128, 0, s>>>(L, n, n, k0, kb, Z, dout);
+            k_fwd_update<<<(rest + 7) / 8, 256, 0, s>>>(L, n, n, k0, kb, Z, dout);
     }
     const int last = ((n - 1) / NB) * NB;
     for (int k0 = last; k0 >= 0; k0 -= NB) {
         const int kb = (n - k0 < NB) ? n - k0 : NB;
-        k_bwd_diag<<<1, 32, 0, s>>>(L, n, k0, kb, Z, dout);
+        k_bwd_diag<<<1, 256, 0, s>>>(L, n, k0, kb, Z, dout);
         if (k0 > 0)
-            k_bwd_update<<<(k0 + 127) / 128, 128, 0, s>>>(L, n, k0, kb, Z, dout);
+            k_bwd_update<<<(k0 + 255) / 256, 256, 0, s>>>(L, n, k0, kb, Z, dout);
     }
 }
 
@@ -1091,12 +1173,17 @@ static int ridge_phi_group(cudaStream_t s, const double *Phi, int n, size_t T,
                 rc = SP_RIDGE_SINGULAR;
                 goto out;
             }
+            rep->factor_ms = ms_since(tf);
         } else {
+            // cholesky_inplace has waited for the factorisation
+            rep->factor_ms = ms_since(tf);
+            auto ts = std::chrono::steady_clock::now();
             chol_solve(s, A, n, W, dout);
+            RK(cudaStreamSynchronize(s));
+            rep->solve_ms = ms_since(ts);
         }
         RK(cudaStreamSynchronize(s));
         RK(cudaGetLastError());
-        rep->factor_ms = ms_since(tf);
     }
 
     {
@@ -1198,6 +1285,7 @@ extern "C" int sp_ridge_phi(cudaStream_t s, const double *Phi, int n, size_t T,
         sum.rel_residual = r1.rel_residual > sum.rel_residual ? r1.rel_residual : sum.rel_residual;
         sum.gram_ms += r1.gram_ms;
         sum.factor_ms += r1.factor_ms;
+        sum.solve_ms += r1.solve_ms;
         sum.refine_ms += r1.refine_ms;
         sum.factor_failed |= r1.factor_failed;
         sum.lu_fallback |= r1.lu_fallback;

@@ -17,6 +17,30 @@ bool injected_failure()
     }
     return false;
 }
+
+// Stream-ordered allocations come from the device's default pool. Its release
+// threshold is 0 by default, so every synchronisation hands freed blocks back
+// to the driver and the next call maps them again (milliseconds for the
+// hundreds of MB of Gram slices). Keep up to 8 GiB cached in the pool.
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_pool_set[kMaxDevices];
+
+void keep_pool(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return;
+    }
+    if (g_pool_set[dev].exchange(1))
+        return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long thr = 8ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+}
 }  // namespace
 
 extern "C" cudaError_t sp_cuda_malloc_bytes(void **p, size_t bytes)
@@ -37,6 +61,7 @@ extern "C" cudaError_t sp_cuda_malloc_async_bytes(void **p, size_t bytes, cudaSt
         *p = nullptr;
         return cudaErrorMemoryAllocation;
     }
+    keep_pool();
     cudaError_t e = cudaMallocAsync(p, bytes, s);
     if (e == cudaSuccess)
         ++g_live;

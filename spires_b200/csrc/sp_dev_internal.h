@@ -18,6 +18,7 @@
 
 struct sp_dev {
     int device, num_sms, coop;
+    int l2_bytes;  // device L2 cache size
     cudaStream_t stream;
     int n, din, dout, micro;
     int nw;              // warps of positions (= spike words in position space)

@@ -19,7 +19,12 @@
 //   The grid is sized so that each CTA streams about the same number of ring
 //   columns (balanced layout, dev_reservoir.cu), and the CTA's CSR slice sits
 //   in shared memory for the launch, so the row pass after each grid barrier
-//   reads no global memory but the spike words.
+//   reads no global memory but the spike words. A gather warp watches the
+//   other CTAs' arrival flags and copies their spike words into a
+//   double-buffered shared array while the consumers are still summing.
+//   A ring larger than the L2 is read with cache hints: slots [0, l2_pin)
+//   are loaded and stored with evict-last priority and stay L2-resident from
+//   step to step, the other slots stream through with evict-first.
 //
 // Per micro-step (both variants), with a split-phase grid barrier:
 //   history sum of step g      (overlaps the barrier wait)
@@ -89,6 +94,9 @@ struct KP {
     // opens micro-step hold_b (-1: none), so every wait on it runs out
     int hold_cta;
     long long hold_b;
+    // variant 1: ring slots [0, l2_pin) are read and written with L2
+    // evict-last priority, the other slots with evict-first (0: no hints)
+    int l2_pin;
     // variant 1: 2-D tiled map of the ring [L rows][rs columns] of doubles,
     // box = BW columns x R rows
     alignas(64) CUtensorMap tmap;
@@ -147,6 +155,32 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
+}
+// L2 eviction-priority policies for the cache-hinted ring loads and stores:
+// evict-last for the slots kept resident, evict-first for the streamed ones
+__device__ __forceinline__ unsigned long long l2_policy(bool keep)
+{
+    unsigned long long pol;
+    if (keep)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void tma_load_2d_hint(void *dst, const CUtensorMap *map, int x, int y,
+                                                 unsigned long long *bar, unsigned long long pol)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        ".L2::cache_hint [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar)),
+        "l"(pol)
+        : "memory");
+}
+__device__ __forceinline__ void st_hint_f64(double *ptr, double v, unsigned long long pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(ptr), "d"(v), "l"(pol)
+                 : "memory");
 }
 __device__ __forceinline__ void st_release_cta(volatile int *ptr, int v)
 {
@@ -473,6 +507,9 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
         bool ok = true;
         const int S_act = p.bal ? p.n / p.G + (blockIdx.x < p.n % p.G ? 1 : 0) : S_b;
         const int nbox = (S_act + p.BW - 1) / p.BW;
+        // slots [0, l2_pin) stay L2-resident, the others stream through
+        const unsigned long long pol_in = l2_policy(true);
+        const unsigned long long pol_out = l2_policy(false);
         for (long long b = 0; b < B && ok; ++b) {
             const long long g = p.step0 + b;
             const int lim = (int)(g < L ? g : L - 1);
@@ -519,9 +556,16 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 }
                 mbar_expect_tx(&full[st], (unsigned)(nbox * p.RB * p.BW * 8));
                 double *dst = s_stage + (size_t)st * STAGE;
-                for (int c = 0; c < nbox; ++c)
-                    tma_load_2d(dst + (size_t)c * p.R * p.BW, &p.tmap, lo + c * p.BW, y0,
-                                &full[st]);
+                if (p.l2_pin > 0) {
+                    const unsigned long long pol = y0 < p.l2_pin ? pol_in : pol_out;
+                    for (int c = 0; c < nbox; ++c)
+                        tma_load_2d_hint(dst + (size_t)c * p.R * p.BW, &p.tmap, lo + c * p.BW,
+                                         y0, &full[st], pol);
+                } else {
+                    for (int c = 0; c < nbox; ++c)
+                        tma_load_2d(dst + (size_t)c * p.R * p.BW, &p.tmap, lo + c * p.BW, y0,
+                                    &full[st]);
+                }
                 ++q;
                 if (++st == p.NST) {
                     st = 0;
@@ -550,6 +594,8 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     const bool wact = gw < wb1;
     const int i = gw * 32 + lane;
     const bool act = wact && __ldg(p.nid_of + i) >= 0;
+    const unsigned long long c_pol_in = VAR == 1 ? l2_policy(true) : 0;
+    const unsigned long long c_pol_out = VAR == 1 ? l2_policy(false) : 0;
 
     double V = act ? p.V[i] : 0.0;
     double tprev = 0.0, vlast = 0.0;
@@ -902,7 +948,11 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 } else {
                     V = p.b;
                 }
-                p.ring[(size_t)head * p.rs + i] = V;
+                if (VAR == 1 && p.l2_pin > 0)
+                    st_hint_f64(p.ring + (size_t)head * p.rs + i, V,
+                                head < p.l2_pin ? c_pol_in : c_pol_out);
+                else
+                    p.ring[(size_t)head * p.rs + i] = V;
                 if (RL > 0) {
 #pragma unroll
                     for (int j = (RL > 0 ? RL : 1) - 1; j > 0; --j)
