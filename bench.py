@@ -122,17 +122,24 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+def profile_traffic(shape=None):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary,
+    when it was captured with the launch shape `shape` (a
+    ctas:warps:variant:stages:rows:l2_pin_rows string); None otherwise."""
     path = os.path.join(ROOT, "profiles", "flif_gl_step_n20000_l1024.md")
+    traffic, captured = None, None
     try:
         with open(path) as f:
             for line in f:
                 if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":")[1])
+                    traffic = float(line.split(":", 1)[1])
+                elif line.startswith("traffic_launch_shape:"):
+                    captured = line.split(":", 1)[1].strip()
     except Exception:
-        pass
-    return None
+        return None
+    if shape is not None and captured != shape:
+        return None
+    return traffic
 
 
 # --------------------------------------------------------------- CPU arms --
@@ -308,7 +315,8 @@ def run_gpu_arm(args, rank, world):
     avg_ms = sum(per) / len(per)
     achieved = bpl / (avg_ms * 1e-3) / 1e9
     peak, kind = peaks()
-    traffic = profile_traffic()
+    traffic = profile_traffic(f"{lau.ctas}:{lau.warps_max}:{lau.variant}:{lau.stages}:"
+                              f"{lau.rows}:{pin_rows}")
 
     # end to end through spires_run with host buffers
     e2e = None
@@ -338,7 +346,14 @@ def run_gpu_arm(args, rank, world):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
                      "algorithmic_bytes_per_launch": bpl, "avg_launch_ms": avg_ms,
-                     "spike_rate": rate},
+                     "spike_rate": rate,
+                     # the ring slots kept L2-resident are algorithmic bytes
+                     # served by the L2: the DRAM side of the same launch
+                     "l2_resident_ring_slots": pin_rows,
+                     "dram_achieved": (traffic / (avg_ms * 1e-3) / 1e9
+                                       if traffic and pin_rows > 0 else None),
+                     "dram_frac": (traffic / (avg_ms * 1e-3) / 1e9 / peak
+                                   if traffic and pin_rows > 0 else None)},
         "clocks": clocks, "gpu_launches": int(launches), "e2e": e2e,
         "launch": {"ctas": lau.ctas, "warps": lau.warps_max, "variant": lau.variant,
                    "stages": lau.stages, "rows": lau.rows,
