@@ -276,6 +276,14 @@ __device__ __forceinline__ int spike_list(const unsigned *s_spk, int nw, int *s_
 // is that of the single-reservoir kernel for LIF_DISCRETE / FLIF_GL with
 // SIMPLE synapses (src/neurons/lif_discrete.c:22-34, src/neurons/flif_gl.c:50-100,
 // src/synapses/simple.c:59-64, src/reservoir.c:113-165).
+#ifdef SP_PHASE_STAMPS
+// Debug builds only: per job slot of the work table, the global timer when the
+// group's first CTA started and finished it, the group, its width and the
+// instance (spires_dbg_batch_job_stamps copies them out).
+constexpr int kJobStampCap = 4096;
+__device__ unsigned long long g_sp_jobstamps[kJobStampCap * 5];
+#endif
+
 __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -341,6 +349,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
         const long long B = I.T * I.micro;
         if (B == 0)
             continue;  // no steps: no arrival either, the counts stay matched
+#ifdef SP_PHASE_STAMPS
+        if (rank == 0 && tid == 0 && j < kJobStampCap) {
+            g_sp_jobstamps[j * 5 + 0] = globaltimer_ns();
+            g_sp_jobstamps[j * 5 + 2] = (unsigned long long)grp;
+            g_sp_jobstamps[j * 5 + 3] = (unsigned long long)gsize;
+            g_sp_jobstamps[j * 5 + 4] = (unsigned long long)p.jobs[j];
+        }
+#endif
         const int nw = I.nw, rs = I.rs, L = I.L;
         const bool gl = I.ntype == SP_FLIF_GL;
         const int wb0 = (int)((long long)rank * nw / gsize);
@@ -451,6 +467,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch(BParams p)
             if (gl)
                 I.tprev[i] = tprev;
         }
+#ifdef SP_PHASE_STAMPS
+        if (rank == 0 && tid == 0 && j < kJobStampCap)
+            g_sp_jobstamps[j * 5 + 1] = globaltimer_ns();
+#endif
     }
 }
 
@@ -922,9 +942,7 @@ extern "C" int sp_batch_create(sp_host_model *models, size_t count, sp_batch **o
     int per_sm = 0;
     if (b->smem > 200 * 1024)
         rc = SP_EINVAL;
-    if (!rc && b->smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)b->smem) != cudaSuccess)
+    if (!rc && b->smem > 48 * 1024 && set_max_dynamic_smem((const void *)k_batch) != cudaSuccess)
         rc = SP_EINVAL;
     if (!rc) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads, b->smem);
@@ -1495,6 +1513,9 @@ extern "C" int sp_batch_fit_predict(sp_batch *b, const double *const *u, const d
             rc = SP_EINTERNAL;
         if (!rc && cudaStreamSynchronize(b->stream) != cudaSuccess)
             rc = SP_EINTERNAL;
+        if (rc && getenv("SPIRES_DEBUG"))
+            fprintf(stderr, "spires: batch fit of instance %zu (n %d, rows %zu, washout %zu) failed: %d\n",
+                    k, I.n, T_fit[k], o->washout, rc);
     }
     cudaStreamSynchronize(b->stream);
     sp_ridge_ws_free(ws);
@@ -1569,3 +1590,22 @@ extern "C" int sp_batch_info(const sp_batch *b, int *ctas, int *groups, int *gra
         *graph = b->graph_ok;
     return SP_OK;
 }
+
+#ifdef SP_PHASE_STAMPS
+extern "C" __attribute__((visibility("default"))) int spires_dbg_batch_job_stamps(void *host,
+                                                                                 size_t bytes)
+{
+    if (bytes < sizeof(g_sp_jobstamps))
+        return -1;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpyFromSymbol(host, g_sp_jobstamps, sizeof(g_sp_jobstamps)) != cudaSuccess)
+        return -1;
+    // cleared after each read, so the next read holds only the runs since
+    void *sym = nullptr;
+    if (cudaGetSymbolAddress(&sym, g_sp_jobstamps) != cudaSuccess ||
+        cudaMemset(sym, 0, sizeof(g_sp_jobstamps)) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess)
+        return -1;
+    return 0;
+}
+#endif

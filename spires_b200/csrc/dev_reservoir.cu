@@ -874,8 +874,7 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     // variant 1: consumer warps, the producer warp and the gather warp
     dim3 grid(l.ctas), block(32 * (l.warps_max + (l.variant == 1 ? 2 : 0)));
     if (smem > 48 * 1024)
-        SP_CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
+        SP_CK(set_max_dynamic_smem((const void *)fn));
     if (l.ctas > 1) {
         SP_CK(cudaMemsetAsync(d->flags, 0,
                               (size_t)l.ctas * kFlagStride * sizeof(unsigned long long),
@@ -1133,8 +1132,7 @@ extern "C" int sp_dev_set_launch(sp_dev *d, const sp_launch *l)
         return SP_EINVAL;
     if (l->ctas > 1) {
         if (smem > 48 * 1024)
-            SP_CK(cudaFuncSetAttribute((const void *)fn,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            SP_CK(set_max_dynamic_smem((const void *)fn));
         int per_sm = 0;
         const int threads = 32 * (l->warps_max + (l->variant == 1 ? 2 : 0));
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, threads,

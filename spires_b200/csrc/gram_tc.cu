@@ -23,12 +23,18 @@
 //     (Cholesky-preconditioned CG in the ridge solver).
 //
 // Layout. Slices are written K-major (time innermost) as [slice][n_pad][T_pad]
-// by the split kernels; a CTA computes one 128 x 64 tile (rows I*128.., columns
-// J*64..) of the lower triangle at a time, persistent over the tile list. Per
-// K chunk of 64 bytes it stages, for every slice, the A rows (2 TMA boxes of
-// 64 rows x 64 B) and the B rows (1 box), 64-byte swizzled, and issues every
-// digit-pair product as two tcgen05.mma (K = 32 B each) into the accumulator
-// of its level (TMEM columns level*64 .. +63; 8 levels fill all 512 columns).
+// by the split kernels; a CTA computes one 128 x 256 tile (rows I*128..,
+// columns J*256..) of the lower triangle at a time, persistent over the tile
+// list (N = 256: at N = 64 an MMA costs about as long as at N = 256, so the
+// wider tile moves four times the work per instruction). Levels are taken one
+// at a time, from the largest: per K chunk of 64 bytes a stage holds the A
+// rows (2 TMA boxes of 64 rows x 64 B) and the B rows (4 boxes) of one digit
+// pair, 64-byte swizzled, and two tcgen05.mma (K = 32 B each) add it into the
+// level's 256-column TMEM accumulator; two accumulators alternate, so the
+// epilogue drains one level while the next accumulates. The FP64 combination
+// runs through the output (or a scratch for later row segments) in memory:
+// the largest level written, each smaller one added, the last scaled by
+// 2^(e_i+e_j-12) (tests/_ozaki_model.py restates the order in numpy).
 // Warp 0 issues the TMA copies, warp 1 the MMAs (one thread), warps 2-5 drain
 // TMEM (tcgen05.ld) and write FP64 rows. No cluster multicast is used.
 //
@@ -45,33 +51,20 @@
 #include <cstring>
 #include <vector>
 #include "sp_alloc.h"
+#include "sp_kernels.cuh"
 #include "sp_gram.h"
 #include "sp_model.h"
 #include "sp_dev.h"
 
 namespace {
 
-constexpr int kTileM = 128, kTileN = 64;     // output tile
+constexpr int kTileM = 128;                  // output tile rows
 constexpr int kChunk = 64;                   // K bytes staged per chunk
 constexpr int kBox = 64 * 64;                // one TMA box: 64 rows x 64 bytes
 constexpr int kMaxSlices = 8, kMaxProd = 36;
 constexpr int kSegChunks = 1023;             // int8: 1023 * 64 = 65472 rows per segment
 constexpr int kThreads = 192;
 constexpr unsigned long long kWaitNs = 2000000000ull;
-
-struct GP {
-    int mode;                 // SP_GRAM_BF16X3, SP_GRAM_TF32X3, SP_GRAM_INT8
-    int ns, nprod, nlev, nst;
-    int n, n_pad, tiles_i, ntiles;
-    int chunks, seg_chunks;   // K chunks in all; per segment
-    unsigned idesc;
-    signed char pa[kMaxProd], pb[kMaxProd], pl[kMaxProd], pfirst[kMaxProd];
-    const int *exps;          // [n_pad] column exponents (INT8)
-    double *C;
-    int ldc;
-    int *err;                 // [0] code, [1] where
-    alignas(64) CUtensorMap map;  // slices {T_pad elements, ns * n_pad rows}, box {64 B, 64}
-};
 
 // ------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ unsigned smem_u32(const void *p)
@@ -203,225 +196,7 @@ __device__ __forceinline__ bool wait_bar(unsigned long long *b, unsigned parity,
     return true;
 }
 
-// tile t -> (I, J) over the lower triangle: row block I has 2I + 2 column
-// blocks of 64 (J <= 2I + 1), so tiles before row block I number I (I + 1)
-__device__ __forceinline__ void tile_ij(int t, int *I, int *J)
-{
-    int i = (int)((sqrtf(4.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
-    while ((i + 1) * (i + 2) <= t)
-        ++i;
-    while (i * (i + 1) > t)
-        --i;
-    *I = i;
-    *J = t - i * (i + 1);
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1) k_gram_tc(const __grid_constant__ GP p)
-{
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char *smem =
-        (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int stage_bytes = p.ns * 3 * kBox;
-    unsigned long long *full = (unsigned long long *)(smem + (size_t)p.nst * stage_bytes);
-    unsigned long long *empty = full + p.nst;
-    unsigned long long *tfull = empty + p.nst;
-    unsigned long long *tempty = tfull + 1;
-    unsigned long long *mdone = tempty + 1;
-    unsigned *tmem_slot = (unsigned *)(mdone + 1);
-    __shared__ volatile int s_abort;
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        s_abort = 0;
-        for (int s = 0; s < p.nst; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
-        }
-        mbar_init(tfull, 1);
-        mbar_init(tempty, 4);
-        mbar_init(mdone, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
-                         smem_u32(tmem_slot))
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const unsigned tmem = *tmem_slot;
-    const int segs = (p.chunks + p.seg_chunks - 1) / p.seg_chunks;
-
-    if (warp == 0) {
-        // ---------------------------------------------------------- producer
-        if (lane == 0) {
-            long long q = 0;
-            bool ok = true;
-            const int xstep = kChunk / (MODE == SP_GRAM_INT8 ? 1 : (MODE == SP_GRAM_BF16X3 ? 2 : 4));
-            for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-                int I, J;
-                tile_ij(t, &I, &J);
-                for (int c = 0; c < p.chunks && ok; ++c, ++q) {
-                    const int st = (int)(q % p.nst);
-                    const long long round = q / p.nst;
-                    if (round > 0 && !wait_bar(&empty[st], (unsigned)((round - 1) & 1), p.err,
-                                               &s_abort, 1)) {
-                        ok = false;
-                        break;
-                    }
-                    unsigned char *A = smem + (size_t)st * stage_bytes;
-                    unsigned char *Bm = A + (size_t)p.ns * 2 * kBox;
-                    mbar_expect_tx(&full[st], (unsigned)(p.ns * 3 * kBox));
-                    for (int s = 0; s < p.ns; ++s) {
-                        const int rowA = s * p.n_pad + I * kTileM;
-                        tma_load_2d(A + (size_t)s * 2 * kBox, &p.map, c * xstep, rowA, &full[st]);
-                        tma_load_2d(A + (size_t)s * 2 * kBox + kBox, &p.map, c * xstep, rowA + 64,
-                                    &full[st]);
-                        tma_load_2d(Bm + (size_t)s * kBox, &p.map, c * xstep,
-                                    s * p.n_pad + J * kTileN, &full[st]);
-                    }
-                }
-            }
-            // every issued copy lands before the CTA may exit
-            const unsigned long long t0 = gtimer();
-            for (long long qq = (q > p.nst ? q - p.nst : 0); qq < q; ++qq) {
-                const int st = (int)(qq % p.nst);
-                while (!mbar_try(&full[st], (unsigned)((qq / p.nst) & 1)))
-                    if (gtimer() - t0 > kWaitNs)
-                        break;
-            }
-        }
-    } else if (warp == 1) {
-        // -------------------------------------------------------------- MMA
-        if (lane == 0) {
-            long long q = 0, sc = 0;
-            bool ok = true;
-            for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-                for (int sg = 0; sg < segs && ok; ++sg, ++sc) {
-                    if (sc > 0 && !wait_bar(tempty, (unsigned)((sc - 1) & 1), p.err, &s_abort, 2)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const int c0 = sg * p.seg_chunks;
-                    const int c1 = (c0 + p.seg_chunks < p.chunks) ? c0 + p.seg_chunks : p.chunks;
-                    for (int c = c0; c < c1; ++c, ++q) {
-                        const int st = (int)(q % p.nst);
-                        if (!wait_bar(&full[st], (unsigned)((q / p.nst) & 1), p.err, &s_abort, 3)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        const unsigned aB = smem_u32(smem + (size_t)st * stage_bytes);
-                        const unsigned bB = aB + (unsigned)(p.ns * 2 * kBox);
-                        for (int k = 0; k < p.nprod; ++k) {
-                            const unsigned da = aB + (unsigned)(p.pa[k] * 2 * kBox);
-                            const unsigned db = bB + (unsigned)(p.pb[k] * kBox);
-                            const unsigned td = tmem + (unsigned)(p.pl[k] * kTileN);
-#pragma unroll
-                            for (int kk = 0; kk < 2; ++kk)
-                                mma<MODE>(td, sdesc(da + kk * 32), sdesc(db + kk * 32), p.idesc,
-                                          !(c == c0 && p.pfirst[k] && kk == 0));
-                        }
-                        tc_commit(&empty[st]);  // stage reusable once these MMAs are done
-                    }
-                    if (ok)
-                        tc_commit(tfull);  // accumulators of this segment complete
-                }
-            }
-            // wait for every MMA issued before the accumulators are read or freed
-            tc_commit(mdone);
-            const unsigned long long t0 = gtimer();
-            while (!mbar_try(mdone, 0))
-                if (gtimer() - t0 > kWaitNs)
-                    break;
-        }
-        __syncwarp();
-    } else {
-        // --------------------------------------------------------- epilogue
-        const int qd = warp & 3;  // TMEM lane quarter this warp may access
-        const int r = qd * 32 + lane;
-        long long sc = 0;
-        bool ok = true;
-        for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-            int I, J;
-            tile_ij(t, &I, &J);
-            const int i = I * kTileM + r;
-            const int ei = (MODE == SP_GRAM_INT8 && i < p.n_pad) ? __ldg(p.exps + i) : 0;
-            for (int sg = 0; sg < segs && ok; ++sg, ++sc) {
-                // one lane polls; the warp then reads TMEM together (.sync.aligned)
-                int okw = 1;
-                if (lane == 0)
-                    okw = wait_bar(tfull, (unsigned)(sc & 1), p.err, &s_abort, 4) ? 1 : 0;
-                okw = __shfl_sync(0xffffffffu, okw, 0);
-                if (!okw) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                for (int cc = 0; cc < kTileN / 16; ++cc) {
-                    double v[16];
-#pragma unroll
-                    for (int c = 0; c < 16; ++c)
-                        v[c] = 0.0;
-                    for (int lv = p.nlev - 1; lv >= 0; --lv) {
-                        unsigned a[16];
-                        tmem_ld16(tmem + ((unsigned)(qd * 32) << 16) +
-                                      (unsigned)(lv * kTileN + cc * 16),
-                                  a);
-                        if (MODE == SP_GRAM_INT8) {
-                            const double sl = ldexp(1.0, -7 * lv);
-#pragma unroll
-                            for (int c = 0; c < 16; ++c)
-                                v[c] = __dadd_rn(v[c], __dmul_rn((double)(int)a[c], sl));
-                        } else {
-#pragma unroll
-                            for (int c = 0; c < 16; ++c)
-                                v[c] = __dadd_rn(v[c], (double)__uint_as_float(a[c]));
-                        }
-                    }
-                    if (i < p.n) {
-                        double *row = p.C + (size_t)i * p.ldc;
-#pragma unroll
-                        for (int c = 0; c < 16; ++c) {
-                            const int j = J * kTileN + cc * 16 + c;
-                            if (j >= p.n)
-                                continue;
-                            double val = v[c];
-                            if (MODE == SP_GRAM_INT8)
-                                val = ldexp(val, ei + __ldg(p.exps + j) - 12);
-                            row[j] = sg == 0 ? val : __dadd_rn(row[j], val);
-                        }
-                    }
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0)
-                    mbar_arrive(tempty);
-            }
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 1) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem)
-                     : "memory");
-    }
-}
-
-// ------------------------------------------------ level-by-level variant
-// 128 x 256 output tiles (N = 256: the shape at which a tcgen05.mma keeps the
-// tensor pipe full) and one level at a time: the MMA warp accumulates every
-// digit pair of level lv over the rows into one of two 256-column TMEM
-// buffers, then the next level into the other while the epilogue drains the
-// first. The FP64 combination of the levels runs through the output (or a
-// scratch for later row segments) in memory: the first level written, each
-// smaller one added, the last scaled by 2^(e_i+e_j-12) -- the same operations
-// in the same order as the all-levels kernel, so the two give the same bits.
+// ------------------------------------------------------- the Gram kernel
 constexpr int kTileNL = 256;
 
 struct GPL {
@@ -829,26 +604,10 @@ int device_ok()
 }
 
 template <int MODE>
-int launch_gram(cudaStream_t s, GP &p, size_t smem)
-{
-    auto fn = k_gram_tc<MODE>;
-    if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return SP_EINTERNAL;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = p.ntiles < sms ? p.ntiles : sms;
-    fn<<<grid, kThreads, smem, s>>>(p);
-    return cudaGetLastError() == cudaSuccess ? SP_OK : SP_EINTERNAL;
-}
-
-template <int MODE>
 int launch_gram_lv(cudaStream_t s, GPL &q, size_t smem)
 {
     auto fn = k_gram_lv<MODE>;
-    if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
+    if (smem > 48 * 1024 && sp::set_max_dynamic_smem((const void *)fn) != cudaSuccess)
         return SP_EINTERNAL;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -881,95 +640,67 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
     const size_t T_pad = ((tw ? tw : 1) + 127) / 128 * 128;
     if (T_pad * esz / kChunk > (size_t)INT_MAX)
         return SP_EINVAL;
-    // the level-by-level kernel (128 x 256 tiles) unless the all-levels one
-    // (128 x 64 tiles) is asked for
-    const char *kv = getenv("SPIRES_GRAM_KERNEL");
-    const bool lvk = !(kv && !strcmp(kv, "wide"));
-    const int n_pad = lvk ? (n + kTileNL - 1) / kTileNL * kTileNL
-                          : (n + kTileM - 1) / kTileM * kTileM;
+    const int n_pad = (n + kTileNL - 1) / kTileNL * kTileNL;
     const int ns = mode == SP_GRAM_INT8 ? slices : 2;
+    const int chunks = (int)(T_pad * esz / kChunk);
 
-    GP p;
-    memset(&p, 0, sizeof(p));
-    p.mode = mode;
-    p.ns = ns;
-    p.n = n;
-    p.n_pad = n_pad;
-    p.tiles_i = n_pad / kTileM;
-    p.ntiles = p.tiles_i * (p.tiles_i + 1);
-    p.chunks = (int)(T_pad * esz / kChunk);
-    // int8 level sums: at most `slices` products of |d| <= 64 digits per row
-    p.seg_chunks = mode == SP_GRAM_INT8 ? kSegChunks : p.chunks;
-    p.C = C;
-    p.ldc = ldc;
-    // products: INT8 digit pairs (a, b) with a + b <= k - 1, level a + b,
-    // grouped by level; split modes hi.hi, hi.lo, lo.hi into one level
-    int np = 0;
-    if (mode == SP_GRAM_INT8) {
-        for (int lv = 0; lv < slices; ++lv)
-            for (int a = 0; a <= lv; ++a) {
-                p.pa[np] = (signed char)a;
-                p.pb[np] = (signed char)(lv - a);
-                p.pl[np] = (signed char)lv;
-                p.pfirst[np] = (signed char)(a == 0);
-                ++np;
-            }
-        p.nlev = slices;
-    } else {
-        const int A[3] = {0, 0, 1}, B[3] = {0, 1, 0};
-        for (int k = 0; k < 3; ++k) {
-            p.pa[k] = (signed char)A[k];
-            p.pb[k] = (signed char)B[k];
-            p.pl[k] = 0;
-            p.pfirst[k] = (signed char)(k == 0);
-        }
-        np = 3;
-        p.nlev = 1;
-    }
-    p.nprod = np;
-    // instruction descriptor: D format (F32 = 1, S32 = 2), A/B formats
-    // (S8 = 1 for kind::i8, BF16 = 1 for kind::f16, TF32 = 2 for kind::tf32),
-    // K-major A and B, N >> 3, M >> 4
-    const unsigned cfmt = mode == SP_GRAM_INT8 ? 2u : 1u;
-    const unsigned abfmt = mode == SP_GRAM_TF32X3 ? 2u : 1u;
-    p.idesc = (cfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((unsigned)(kTileN >> 3) << 17) |
-              ((unsigned)(kTileM >> 4) << 24);
-
-    // the level kernel's parameters: the same products, by level
     GPL q;
     memset(&q, 0, sizeof(q));
     q.mode = mode;
-    q.nlev = p.nlev;
     q.n = n;
     q.n_pad = n_pad;
     q.tiles_i = n_pad / kTileM;
     for (int I = 0; I < q.tiles_i; ++I)
         q.ntiles += I / 2 + 1;
-    q.chunks = p.chunks;
-    q.seg_chunks = p.seg_chunks;
-    for (int k = 0; k < np; ++k) {
-        q.pa[k] = p.pa[k];
-        q.pb[k] = p.pb[k];
-    }
-    for (int lv = 0; lv <= p.nlev; ++lv)
-        q.lv_first[lv] = mode == SP_GRAM_INT8 ? lv * (lv + 1) / 2 : (lv == 0 ? 0 : 3);
-    q.idesc = (cfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((unsigned)(kTileNL >> 3) << 17) |
-              ((unsigned)(kTileM >> 4) << 24);
+    q.chunks = chunks;
+    // int8 level sums: at most `slices` products of |d| <= 64 digits per row
+    q.seg_chunks = mode == SP_GRAM_INT8 ? kSegChunks : chunks;
     q.C = C;
     q.ldc = ldc;
-    const int segs = (p.chunks + p.seg_chunks - 1) / p.seg_chunks;
+    // products: INT8 digit pairs (a, b) with a + b <= k - 1, level a + b,
+    // grouped by level; split modes hi.hi, hi.lo, lo.hi into one level
+    int np = 0;
+    if (mode == SP_GRAM_INT8) {
+        for (int lv = 0; lv < slices; ++lv) {
+            q.lv_first[lv] = np;
+            for (int a = 0; a <= lv; ++a) {
+                q.pa[np] = (signed char)a;
+                q.pb[np] = (signed char)(lv - a);
+                ++np;
+            }
+        }
+        q.nlev = slices;
+    } else {
+        const int A[3] = {0, 0, 1}, B[3] = {0, 1, 0};
+        for (int k = 0; k < 3; ++k) {
+            q.pa[k] = (signed char)A[k];
+            q.pb[k] = (signed char)B[k];
+        }
+        np = 3;
+        q.lv_first[0] = 0;
+        q.nlev = 1;
+    }
+    q.lv_first[q.nlev] = np;
+    // instruction descriptor: D format (F32 = 1, S32 = 2), A/B formats
+    // (S8 = 1 for kind::i8, BF16 = 1 for kind::f16, TF32 = 2 for kind::tf32),
+    // K-major A and B, N >> 3, M >> 4
+    const unsigned cfmt = mode == SP_GRAM_INT8 ? 2u : 1u;
+    const unsigned abfmt = mode == SP_GRAM_TF32X3 ? 2u : 1u;
+    q.idesc = (cfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((unsigned)(kTileNL >> 3) << 17) |
+              ((unsigned)(kTileM >> 4) << 24);
+    const int segs = (q.chunks + q.seg_chunks - 1) / q.seg_chunks;
 
-    const size_t stage_bytes = lvk ? (size_t)6 * kBox : (size_t)ns * 3 * kBox;
+    // a stage: A 128 rows (2 boxes) and B 256 rows (4 boxes) of one K chunk
+    const size_t stage_bytes = (size_t)6 * kBox;
     int dev = 0, smem_max = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t fixed = 1024 + 256;
     long long nst = ((long long)smem_max - (long long)fixed) / (long long)stage_bytes;
-    if (nst > (lvk ? 8 : 6))
-        nst = lvk ? 8 : 6;
+    if (nst > 8)
+        nst = 8;
     if (nst < 2)
         return SP_EINVAL;
-    p.nst = (int)nst;
     q.nst = (int)nst;
     const size_t smem = fixed + (size_t)nst * stage_bytes;
 
@@ -977,7 +708,7 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
     int *ex = nullptr, *flags = nullptr;
     double *V = nullptr;
     int rc = SP_OK;
-    if (lvk && segs > 1 &&
+    if (segs > 1 &&
         sp_cuda_malloc_async(&V, (size_t)n * ldc * sizeof(double), s) != cudaSuccess) {
         cudaGetLastError();
         return SP_EALLOC;
@@ -1022,13 +753,12 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
         cuuint64_t strides[1] = {(cuuint64_t)T_pad * esz};
         cuuint32_t box[2] = {(cuuint32_t)(kChunk / esz), 64};
         cuuint32_t estr[2] = {1, 1};
-        if (encoder()(&p.map, dt, 2, S, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        if (encoder()(&q.map, dt, 2, S, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                       CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             rc = SP_EINTERNAL;
-        q.map = p.map;
     }
-    if (!rc && lvk) {
+    if (!rc) {
         q.exps = ex;
         q.err = flags;
         q.V = V;
@@ -1038,15 +768,6 @@ extern "C" int sp_gram_tc(cudaStream_t s, int mode, int slices, const double *X,
             rc = launch_gram_lv<SP_GRAM_BF16X3>(s, q, smem);
         else
             rc = launch_gram_lv<SP_GRAM_TF32X3>(s, q, smem);
-    } else if (!rc) {
-        p.exps = ex;
-        p.err = flags;
-        if (mode == SP_GRAM_INT8)
-            rc = launch_gram<SP_GRAM_INT8>(s, p, smem);
-        else if (mode == SP_GRAM_BF16X3)
-            rc = launch_gram<SP_GRAM_BF16X3>(s, p, smem);
-        else
-            rc = launch_gram<SP_GRAM_TF32X3>(s, p, smem);
     }
     if (!rc) {
         k_mirror<<<1024, 256, 0, s>>>(C, n, ldc);

@@ -13,6 +13,23 @@ namespace sp {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// A kernel's dynamic shared-memory limit is one attribute per function for
+// the whole process: reservoirs and batches built on other host threads share
+// it, so a caller that set it to its own size could lower it under another
+// caller's pending launch ("invalid argument"). Every caller therefore sets
+// the same value, the device's opt-in maximum; occupancy and launches still
+// use each launch's own size.
+inline cudaError_t set_max_dynamic_smem(const void *fn)
+{
+    int dev = 0, v = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    return e;
+}
+
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }

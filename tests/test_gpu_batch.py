@@ -187,3 +187,33 @@ def test_autotuned_schedule_keeps_results():
         Rs, Vs = solo(cfgs[k], seeds[k], us[k])
         assert np.array_equal(R[k], Rs), k
         assert same_bits(V[k], Vs), k
+
+
+def test_batch_runs_after_a_smaller_batch_was_built():
+    """The batch kernel's shared-memory limit is one attribute for the whole
+    process. A batch with long rings (large shared memory) must still launch
+    after a second batch with short rings (less shared memory, still above the
+    48 KB default) was built, and re-plan for new
+    series lengths (a search builds the next chunk's batch on another thread
+    while the current one runs)."""
+    big_cfg = sp.make_config(1500, 1, 1, rho=0.9, ei=0.5, gamma=1.0, conn=0.05,
+                             topo=sp.CONN_RANDOM, neuron=sp.FLIF_GL,
+                             nparams=gl_params(0.6, 1024))
+    small_cfg = sp.make_config(300, 1, 1, rho=0.9, ei=0.5, gamma=1.0, conn=0.05,
+                               topo=sp.CONN_RANDOM, neuron=sp.FLIF_GL,
+                               nparams=gl_params(0.6, 128))
+    rng = np.random.default_rng(5)
+    big = sp.Batch([big_cfg, big_cfg], [11, 12])
+    small = sp.Batch([small_cfg], [13])
+    try:
+        for T in (60, 140):
+            us = [rng.uniform(-1.0, 1.5, size=(T, 1)) for _ in range(2)]
+            R, V, _ = big.run(us)
+            for k, seed in enumerate((11, 12)):
+                Rs, Vs = solo(big_cfg, seed, us[k])
+                assert np.array_equal(R[k], Rs)
+                assert same_bits(V[k], Vs)
+        small.run([rng.uniform(-1.0, 1.5, size=(50, 1))])
+    finally:
+        big.close()
+        small.close()
