@@ -502,7 +502,11 @@ def run_search_workload(args):
         space, task = S.Space(), S.Task(length=8000, val=1000, washout=200)
         rungs, points, chains = (500, 2000, 8000), 1024, 32
     out = {}
-    arms = [a for a in ("plain", "surrogate", "no_surrogate") if a in args.search_arms.split(",")]
+    # surrogate: the headline arm (with --search-prescreen); surrogate_full:
+    # the same without the pre-screen; no_surrogate: the schedule without
+    # the networks (ranked by the low-fidelity loss)
+    names = ("plain", "surrogate", "surrogate_full", "no_surrogate")
+    arms = [a for a in names if a in args.search_arms.split(",")]
     assert "plain" in arms and "surrogate" in arms, "plain and surrogate arms are required"
     for name in arms:
         ev = S.Evaluator(space, task, seed=1)
@@ -510,7 +514,8 @@ def run_search_workload(args):
             r = S.plain_agile(ev, chains=chains, T=rungs[-1], seed=0, max_points=points)
         else:
             r = S.surrogate_agile(ev, chains=chains, rungs=rungs, max_points=points, waves=8,
-                                  seed=0, use_surrogate=(name == "surrogate"))
+                                  prescreen=args.search_prescreen if name == "surrogate" else 0.0,
+                                  seed=0, use_surrogate=(name != "no_surrogate"))
         out[name] = (r, ev.stats)
     plain = out["plain"][0]
     target = plain.best_loss + math.log(1.02)
@@ -520,13 +525,14 @@ def run_search_workload(args):
             "ratio_to_plain_wall": (tt / plain.wall_s) if tt is not None else None,
             "plain_wall_s": plain.wall_s, "plain_best_nrmse": plain.best_nrmse,
             "plain_time_to_best_s": plain.time_to(plain.best_loss)}
-    for name in [a for a in ("surrogate", "no_surrogate") if a in out]:
+    for name in [a for a in names[1:] if a in out]:
         r, st = out[name]
         line[name] = {"best_nrmse": r.best_nrmse, "wall_s": r.wall_s,
                       "time_to_target_s": r.time_to(target), "evals": r.evals,
                       "neuron_steps": st.neuron_steps, "build_s": st.build_s,
                       "build_wait_s": st.build_wait_s,
                       "construct_s": st.construct_s, "setup_s": st.setup_s,
+                      "screened_out": r.extra.get("screened_out"),
                       "surrogate_rmse_logNRMSE": r.extra.get("surrogate_rmse"),
                       "low_fidelity_rmse_logNRMSE": r.extra.get("low_fidelity_rmse")}
     line["plain_neuron_steps"] = out["plain"][1].neuron_steps
@@ -534,7 +540,8 @@ def run_search_workload(args):
     line["plain_build_wait_s"] = out["plain"][1].build_wait_s
     line["plain_construct_s"] = out["plain"][1].construct_s
     line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
-                      "rungs": list(rungs), "points": points, "chains": chains, "waves": 8}
+                      "rungs": list(rungs), "points": points, "chains": chains, "waves": 8,
+                      "prescreen": args.search_prescreen}
     line["data"] = "synthetic (seeded Mackey-Glass)"
     print(json.dumps(line))
 
@@ -837,6 +844,8 @@ def main():
     ap.add_argument("--sweep-tmax", type=int, default=10000,
                     help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
+    ap.add_argument("--search-prescreen", type=float, default=0.0,
+                    help="surrogate arm: fraction of asked points simulated once trained")
     ap.add_argument("--search-arms", default="plain,surrogate,no_surrogate",
                     help="comma list of plain, surrogate, no_surrogate")
     args = ap.parse_args()

@@ -77,7 +77,10 @@ struct BParams {
 constexpr int kHistChunk = 32;  // ring values in flight per thread (cost model)
 
 constexpr int kHistC = 8;  // ring values per cp.async group and thread
-constexpr int kHistS = 4;  // groups in flight per thread
+#ifndef SP_BATCH_HIST_S
+#define SP_BATCH_HIST_S 4
+#endif
+constexpr int kHistS = SP_BATCH_HIST_S;  // groups in flight per thread
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 {

@@ -17,16 +17,20 @@ constexpr unsigned kFull = 0xffffffffu;
 // the whole process: reservoirs and batches built on other host threads share
 // it, so a caller that set it to its own size could lower it under another
 // caller's pending launch ("invalid argument"). Every caller therefore sets
-// the same value, the device's opt-in maximum; occupancy and launches still
-// use each launch's own size.
+// the same value, the device's opt-in maximum less the kernel's static shared
+// memory; occupancy and launches still use each launch's own size.
 inline cudaError_t set_max_dynamic_smem(const void *fn)
 {
     int dev = 0, v = 0;
+    cudaFuncAttributes fa;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        e = cudaFuncGetAttributes(&fa, fn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 v - (int)fa.sharedSizeBytes);
     return e;
 }
 

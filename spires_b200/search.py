@@ -277,7 +277,8 @@ def plain_agile(ev: Evaluator, chains: int = 16, T: int = 16000, seed: int = 0,
 def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), keep: float = 0.1,
                     max_points: int = 4096, waves: int = 8, seed: int = 0,
                     opts: AgileOpts | None = None, use_surrogate: bool = True, epochs: int = 200,
-                    calibration: int = 8, kappa: float = 1.0) -> SearchResult:
+                    calibration: int = 8, kappa: float = 1.0,
+                    prescreen: float = 0.0) -> SearchResult:
     """Surrogate-guided multi-fidelity AGILE (see module doc). The chains start
     from the same points with the same seeds as :func:`plain_agile`.
 
@@ -289,10 +290,21 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
     them; the networks train on them before the first wave), and every wave
     carries `calibration` further seeded random points through every rung.
     Cuts rank by the optimistic score mean - kappa * std, so that points the
-    network is unsure about still get simulated."""
+    network is unsure about still get simulated.
+
+    prescreen > 0 adds a cut before any simulation: once the networks have
+    trained, a further network maps the 9 hyper-parameter features alone to
+    the full-fidelity loss, and of each round's asked points only the best
+    fraction `prescreen` by its optimistic score (plus `calibration` random
+    ones) is built and simulated at the lowest fidelity; the chains are told
+    that network's prediction for the others, which are neither built nor
+    pooled."""
     lib, h = _agile_start(chains, seed, opts)
     ncut = len(rungs) - 1
     nets = [Surrogate(seed=seed + r) for r in range(ncut)] if use_surrogate else None
+    pre_net = Surrogate(seed=seed + 97) if (use_surrogate and prescreen > 0.0) else None
+    X_pre = []
+    screened = 0
     trained = False
     rng = np.random.default_rng(seed + 7)
     pts = np.empty((2 * chains, DIM))
@@ -303,6 +315,7 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
     best, best_th, hist, evals, asked = math.inf, None, [], 0, 0
     pred_rmse, low_rmse = [], []
     wave_size = max(1, max_points // max(1, waves))
+    wave_asked = 0
     t0 = time.perf_counter()
 
     def net_input(th, low):
@@ -354,6 +367,10 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
             X_tr[r].extend(list(new_X[r]))
             nets[r].train(np.asarray(X_tr[r], np.float32), ya, epochs=epochs,
                           batch=min(256, len(ya)), lr=1e-3, seed=seed + 31 * len(hist) + r)
+        if pre_net is not None:
+            X_pre.extend(list(net_input(th[sel], np.zeros(len(sel)))))
+            pre_net.train(np.asarray(X_pre, np.float32), ya, epochs=epochs,
+                          batch=min(256, len(ya)), lr=1e-3, seed=seed + 31 * len(hist) + 17)
         trained = True
 
     try:
@@ -375,6 +392,11 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
                     nets[r].train(np.asarray(X_tr[r], np.float32), np.asarray(y_tr, np.float32),
                                   epochs=epochs, batch=min(256, len(y_tr)), lr=1e-3,
                                   seed=seed + r)
+                if pre_net is not None:
+                    X_pre.extend(list(net_input(th, np.zeros(n))))
+                    pre_net.train(np.asarray(X_pre, np.float32), np.asarray(y_tr, np.float32),
+                                  epochs=epochs, batch=min(256, len(y_tr)), lr=1e-3,
+                                  seed=seed + 97)
                 trained = True
             lib.spires_ext_agile_batch_tell(h, dptr(np.ascontiguousarray(full)))
         while asked < max_points:
@@ -382,18 +404,33 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
             if n <= 0:
                 break
             th = pts[:n].copy()
-            l0 = ev.evaluate(th, rungs[0], np.arange(asked, asked + n))
-            evals += n
+            ids = np.arange(asked, asked + n)
             asked += n
-            est = predict(0, th, l0)
+            est = np.empty(n)
+            run = np.arange(n)
+            if pre_net is not None and trained:
+                m, v = pre_net.predict(net_input(th, np.zeros(n)), bf16=True)
+                score = m.astype(np.float64) - kappa * np.exp(
+                    0.5 * np.clip(v.astype(np.float64), -20.0, 20.0))
+                nk = max(1, int(math.ceil(prescreen * n)))
+                cal = rng.choice(n, size=min(calibration, n), replace=False)
+                run = np.union1d(np.argsort(score, kind="stable")[:nk], cal)
+                rest = np.setdiff1d(np.arange(n), run)
+                est[rest] = m.astype(np.float64)[rest]
+                screened += len(rest)
+            l0 = ev.evaluate(th[run], rungs[0], ids[run])
+            evals += len(run)
+            est[run] = predict(0, th[run], l0)
             lib.spires_ext_agile_batch_tell(h, dptr(np.ascontiguousarray(est)))
-            pool_th.append(th)
+            pool_th.append(th[run])
             pool_l0.append(l0)
-            pool_id.append(np.arange(asked - n, asked))
-            if sum(len(p) for p in pool_th) >= wave_size:
+            pool_id.append(ids[run])
+            wave_asked += n  # waves are counted in asked points, pooled or screened
+            if wave_asked >= wave_size:
                 cut_wave(np.concatenate(pool_th), np.concatenate(pool_l0),
                          np.concatenate(pool_id))
                 pool_th, pool_l0, pool_id = [], [], []
+                wave_asked = 0
         if pool_th:
             cut_wave(np.concatenate(pool_th), np.concatenate(pool_l0), np.concatenate(pool_id))
     finally:
@@ -401,6 +438,8 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
         if nets is not None:
             for net in nets:
                 net.close()
+        if pre_net is not None:
+            pre_net.close()
     extra = {"surrogate_rmse": pred_rmse, "low_fidelity_rmse": low_rmse, "tuples": len(y_tr),
-             "points": asked}
+             "points": asked, "screened_out": screened}
     return SearchResult(best, best_th, time.perf_counter() - t0, evals, hist, extra)

@@ -67,3 +67,19 @@ def test_searches_run_and_surrogate_helps(task):
     # same schedule ranked by the low-fidelity loss alone
     assert with_net.best_loss <= without.best_loss + 1e-12
     assert with_net.extra["tuples"] > 0 and without.extra["tuples"] == 0
+
+
+def test_prescreen_skips_points_and_still_searches(task):
+    """With the hyper-parameter pre-screen, part of each round's asked points
+    is told the network's prediction without being built or simulated; the
+    search still ends with a scored best point, and the low-fidelity
+    simulations are fewer than without the pre-screen."""
+    kw = dict(chains=8, rungs=RUNGS, max_points=256, waves=4, seed=0)
+    ev1 = S.Evaluator(SPACE, task, seed=1)
+    pre = S.surrogate_agile(ev1, prescreen=0.4, **kw)
+    ev2 = S.Evaluator(SPACE, task, seed=1)
+    full = S.surrogate_agile(ev2, **kw)
+    assert math.isfinite(pre.best_loss) and pre.best_theta is not None
+    assert pre.extra["screened_out"] > 0 and full.extra["screened_out"] == 0
+    assert pre.extra["points"] == full.extra["points"]
+    assert ev1.stats.neuron_steps < ev2.stats.neuron_steps
