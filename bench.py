@@ -515,6 +515,7 @@ def run_search_workload(args):
         else:
             r = S.surrogate_agile(ev, chains=chains, rungs=rungs, max_points=points, waves=8,
                                   prescreen=args.search_prescreen if name == "surrogate" else 0.0,
+                                  keep=args.search_keep,
                                   seed=0, use_surrogate=(name != "no_surrogate"))
         out[name] = (r, ev.stats)
     plain = out["plain"][0]
@@ -541,7 +542,7 @@ def run_search_workload(args):
     line["plain_construct_s"] = out["plain"][1].construct_s
     line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
                       "rungs": list(rungs), "points": points, "chains": chains, "waves": 8,
-                      "prescreen": args.search_prescreen}
+                      "prescreen": args.search_prescreen, "keep": args.search_keep}
     line["data"] = "synthetic (seeded Mackey-Glass)"
     print(json.dumps(line))
 
@@ -844,6 +845,8 @@ def main():
     ap.add_argument("--sweep-tmax", type=int, default=10000,
                     help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
+    ap.add_argument("--search-keep", type=float, default=0.1,
+                    help="surrogate arms: fraction surviving each rung (the configuration's 10 %%)")
     ap.add_argument("--search-prescreen", type=float, default=0.0,
                     help="surrogate arm: fraction of asked points simulated once trained")
     ap.add_argument("--search-arms", default="plain,surrogate,no_surrogate",

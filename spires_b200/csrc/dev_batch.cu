@@ -77,10 +77,9 @@ struct BParams {
 constexpr int kHistChunk = 32;  // ring values in flight per thread (cost model)
 
 constexpr int kHistC = 8;  // ring values per cp.async group and thread
-#ifndef SP_BATCH_HIST_S
-#define SP_BATCH_HIST_S 4
-#endif
-constexpr int kHistS = SP_BATCH_HIST_S;  // groups in flight per thread
+// groups in flight per thread (6 or 8 need more shared memory than two CTAs
+// per SM allow, and one CTA per SM halved the sweep's throughput)
+constexpr int kHistS = 4;
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 {
