@@ -347,9 +347,9 @@ def run_gpu_arm(args, rank, world):
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
                      "algorithmic_bytes_per_launch": bpl, "avg_launch_ms": avg_ms,
                      "spike_rate": rate,
-                     # the ring slots kept L2-resident are algorithmic bytes
+                     # the ring lags kept L2-resident are algorithmic bytes
                      # served by the L2: the DRAM side of the same launch
-                     "l2_resident_ring_slots": pin_rows,
+                     "l2_resident_ring_lags": pin_rows,
                      "dram_achieved": (traffic / (avg_ms * 1e-3) / 1e9
                                        if traffic and pin_rows > 0 else None),
                      "dram_frac": (traffic / (avg_ms * 1e-3) / 1e9 / peak
@@ -826,7 +826,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="force step-kernel variant")
     ap.add_argument("--l2-pin", type=int, default=-1,
-                    help="ring slots kept L2-resident (-1: the library's automatic choice)")
+                    help="oldest ring lags kept L2-resident (-1: the library's automatic choice)")
     ap.add_argument("--profile-case", action="store_true",
                     help="fill the ring, then one launch of --chunk steps (for ncu -s 1 -c 1)")
     ap.add_argument("--profile-gram", action="store_true",

@@ -86,16 +86,17 @@ typedef struct {
     int rows;         /* ring rows per stage (variant 1) */
     int csr_global;   /* 1: walk the recurrent CSR rows in global memory even
                          when the CTA's slice fits in shared memory (0 default) */
-    int l2_pin;       /* variant 1: ring slots [0, l2_pin) are loaded and stored
-                         with L2 evict-last priority and the other slots with
-                         evict-first, so that part of a ring larger than the L2
-                         stays resident from step to step; 0 = no cache hints,
-                         -1 = automatic (default: half of the L2 when the ring
-                         is larger than three quarters of it, else 0) */
+    int l2_pin;       /* variant 1: the oldest l2_pin lags of every step are
+                         loaded with L2 evict-last priority and younger lags
+                         and the ring writes with evict-first, so that part of
+                         a ring larger than the L2 stays resident from step to
+                         step; 0 = no cache hints, -1 = automatic (default: 70 %
+                         of the L2 when the ring is larger than three quarters
+                         of it, else 0) */
 } spires_ext_launch;
 
 spires_status spires_ext_get_launch(const spires_reservoir *r, spires_ext_launch *l);
-/* Ring slots the current launch keeps L2-resident (l2_pin with -1 resolved;
+/* Ring lags the current launch keeps L2-resident (l2_pin with -1 resolved;
  * 0 for variant 0 or without cache hints). */
 int           spires_ext_l2_pin_rows(const spires_reservoir *r);
 spires_status spires_ext_set_launch(spires_reservoir *r, const spires_ext_launch *l);

@@ -373,21 +373,23 @@ static int max_smem(const sp_dev *d)
     return v > 0 ? v : 48 * 1024;
 }
 
-// Ring slots kept L2-resident by the variant-1 cache hints when the launch
-// asks for the automatic choice: a ring that does not fit in the L2 would miss
-// on every row under plain replacement (each row is read once per step, in a
-// cycle longer than the cache), so half of the L2 holds a fixed set of slots
-// with evict-last priority while the other slots stream through with
-// evict-first. (N=20000, L=1024 on one B200: 391 of 1024 slots, about 25.5 us
-// per step against 30.1 without hints; pinning 640 or 768 slots was slower,
-// the streamed rows then evicting pinned ones.)
+// Lags kept L2-resident by the variant-1 cache hints when the launch asks for
+// the automatic choice. A ring that does not fit in the L2 would miss on every
+// row under plain replacement (each row is read once per step, in a cycle
+// longer than the cache), so the oldest lags of every step -- 70 % of the L2
+// -- are read with evict-last priority and stay resident, while younger rows
+// stream through with evict-first. (N=20000, L=1024 on one B200: 490 lags,
+// 24.6-24.9 us per step against 29.3 without hints; 600 lags 25.1, 700 lags
+// 27.7 -- the streamed rows then evict resident ones -- and the earlier
+// choice of a fixed set of ring slots at half the L2, 26.0 with a wide
+// spread from launch to launch.)
 static int auto_l2_pin(const sp_dev *d)
 {
     const double row = (double)d->rs * sizeof(double);
     const double ring = row * d->nc.L;
     if (d->l2_bytes <= 0 || ring <= 0.75 * d->l2_bytes)
         return 0;
-    const int rows = (int)(0.5 * d->l2_bytes / row);
+    const int rows = (int)(0.7 * d->l2_bytes / row);
     return rows < d->nc.L ? rows : d->nc.L;
 }
 

@@ -29,9 +29,10 @@ typedef struct {
     int rows;        /* ring rows per stage of variant 1 */
     int csr_global;  /* 1: SIMPLE synapse rows walked in global memory even when
                         the CTA's CSR slice fits in shared memory */
-    int l2_pin;      /* variant 1: ring slots [0, l2_pin) read and written with
-                        L2 evict-last priority, the others evict-first; 0 = no
-                        cache hints, -1 = automatic (sp_dev_l2_pin_rows) */
+    int l2_pin;      /* variant 1: the oldest l2_pin lags of a step read with L2
+                        evict-last priority, younger lags and ring writes
+                        evict-first; 0 = no cache hints, -1 = automatic
+                        (sp_dev_l2_pin_rows) */
 } sp_launch;
 
 int  sp_dev_create(const sp_host_model *m, sp_dev **out);
@@ -70,7 +71,7 @@ int  sp_dev_upload_w_out(sp_dev *d, const double *h_W_out);
 int  sp_dev_download_w_out(sp_dev *d, double *h_W_out);
 void *sp_dev_stream(sp_dev *d);
 int  sp_dev_get_launch(sp_dev *d, sp_launch *l);
-/* Ring slots the launch keeps L2-resident (its l2_pin with -1 resolved). */
+/* Ring lags the launch keeps L2-resident (its l2_pin with -1 resolved). */
 int  sp_dev_l2_pin_rows(const sp_dev *d);
 int  sp_dev_set_launch(sp_dev *d, const sp_launch *l);
 int  sp_dev_set_seed(sp_dev *d, uint64_t seed);

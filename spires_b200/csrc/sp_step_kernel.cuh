@@ -22,9 +22,11 @@
 //   reads no global memory but the spike words. A gather warp watches the
 //   other CTAs' arrival flags and copies their spike words into a
 //   double-buffered shared array while the consumers are still summing.
-//   A ring larger than the L2 is read with cache hints: slots [0, l2_pin)
-//   are loaded and stored with evict-last priority and stay L2-resident from
-//   step to step, the other slots stream through with evict-first.
+//   A ring larger than the L2 is read with cache hints: the oldest l2_pin
+//   lags of a step are loaded with evict-last priority and stay L2-resident
+//   from step to step (each row joins them once, when it reaches lag
+//   L - l2_pin), the younger lags stream through with evict-first, so the
+//   DRAM reads come first in every step and run on through the serial phase.
 //
 // Per micro-step (both variants), with a split-phase grid barrier:
 //   history sum of step g      (overlaps the barrier wait)
@@ -94,8 +96,9 @@ struct KP {
     // opens micro-step hold_b (-1: none), so every wait on it runs out
     int hold_cta;
     long long hold_b;
-    // variant 1: ring slots [0, l2_pin) are read and written with L2
-    // evict-last priority, the other slots with evict-first (0: no hints)
+    // variant 1: the oldest l2_pin lags of every step are read with L2
+    // evict-last priority, younger ones and the ring writes with evict-first
+    // (0: no hints)
     int l2_pin;
     // variant 1: 2-D tiled map of the ring [L rows][rs columns] of doubles,
     // box = BW columns x R rows
@@ -557,7 +560,11 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 mbar_expect_tx(&full[st], (unsigned)(nbox * p.RB * p.BW * 8));
                 double *dst = s_stage + (size_t)st * STAGE;
                 if (p.l2_pin > 0) {
-                    const unsigned long long pol = y0 < p.l2_pin ? pol_in : pol_out;
+                    // the oldest l2_pin lags stay resident: a row is read
+                    // evict-first while young and turns evict-last when it
+                    // reaches lag L - l2_pin (one row per step comes back
+                    // from DRAM for that)
+                    const unsigned long long pol = k + cnt > L - p.l2_pin ? pol_in : pol_out;
                     for (int c = 0; c < nbox; ++c)
                         tma_load_2d_hint(dst + (size_t)c * p.R * p.BW, &p.tmap, lo + c * p.BW,
                                          y0, &full[st], pol);
@@ -594,7 +601,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
     const bool wact = gw < wb1;
     const int i = gw * 32 + lane;
     const bool act = wact && __ldg(p.nid_of + i) >= 0;
-    const unsigned long long c_pol_in = VAR == 1 ? l2_policy(true) : 0;
+    // ring writes: evict-first (a row is lag 34 when it is first read back)
     const unsigned long long c_pol_out = VAR == 1 ? l2_policy(false) : 0;
 
     double V = act ? p.V[i] : 0.0;
@@ -950,7 +957,7 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 }
                 if (VAR == 1 && p.l2_pin > 0)
                     st_hint_f64(p.ring + (size_t)head * p.rs + i, V,
-                                head < p.l2_pin ? c_pol_in : c_pol_out);
+                                c_pol_out);
                 else
                     p.ring[(size_t)head * p.rs + i] = V;
                 if (RL > 0) {
