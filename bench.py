@@ -675,6 +675,84 @@ def run_small_lif_workload(args):
     print(json.dumps(line))
 
 
+def run_models_workload(args):
+    """Every neuron model (SIMPLE synapses) and every synapse model (FLIF_GL
+    neurons) on the bench's graph (N=20000, Barabasi-Albert m=5, Din=13):
+    neuron-steps/s of the step kernel in steady state (history full), and for
+    the models that stream a history, its bytes per neuron-step and rate.
+    History lengths: FLIF_GL 1024, FLIF_CAPUTO 512, fractional synapse 512."""
+    import numpy as np
+    import torch
+
+    import spires_b200 as sp
+
+    lib = sp.load()
+    S, reps = 128, 3
+    neuron_params = {
+        sp.LIF_DISCRETE: (0.0, 1.0, 0.3, 0.05),
+        sp.LIF_BIO: (0.0, 1.0, 5.0, 0.85),
+        sp.FLIF_CAPUTO: (1.0, 0.2, 0.0, 1.0, 0.0, 1.5, 0.7, 2.0, 512.0),
+        sp.FLIF_GL: GL_PARAMS,
+        sp.FLIF_DIFFUSIVE: (1.0, 0.0, 0.0, 5.0, 1.0, 3.0, 0.85),
+    }
+    syn_params = {sp.SYN_SIMPLE: None, sp.SYN_PSC_HOM: (3.0,), sp.SYN_PSC_HET: (1.0, 10.0),
+                  sp.SYN_FRAC: (0.6, 4.0, 512.0), sp.SYN_FRAC_MEXP: (0.5, 4.0, 1.0, 40.0, 5)}
+    nnames = {sp.LIF_DISCRETE: "LIF_DISCRETE", sp.LIF_BIO: "LIF_BIO", sp.FLIF_CAPUTO: "FLIF_CAPUTO",
+              sp.FLIF_GL: "FLIF_GL", sp.FLIF_DIFFUSIVE: "FLIF_DIFFUSIVE"}
+    snames = {sp.SYN_SIMPLE: "SIMPLE", sp.SYN_PSC_HOM: "PSC_HOMOGENEOUS",
+              sp.SYN_PSC_HET: "PSC_HETEROGENEOUS", sp.SYN_FRAC: "FRACTIONAL",
+              sp.SYN_FRAC_MEXP: "FRACTIONAL_MULTIEXP"}
+    # history bytes per neuron-step (steady state): ring lags read
+    hist_bytes = {sp.FLIF_GL: 8 * 1023, sp.FLIF_CAPUTO: 8 * 510}
+    combos = [(nt, sp.SYN_SIMPLE) for nt in neuron_params] + \
+             [(sp.FLIF_GL, st) for st in (sp.SYN_PSC_HOM, sp.SYN_PSC_HET, sp.SYN_FRAC,
+                                          sp.SYN_FRAC_MEXP)]
+    rows = []
+    for nt, st in combos:
+        cfg = sp.make_config(N_NEURONS, DIN, DOUT, rho=0.9, ei=0.5, gamma=0.5,
+                             conn=5.0 / (N_NEURONS - 1), dt=1.0, topo=sp.CONN_SCALE_FREE,
+                             neuron=nt, nparams=neuron_params[nt], synapse=st,
+                             sparams=syn_params[st])
+        r = sp.Reservoir(cfg, seed=SEED)
+        lau = r.launch()
+        fill = L_HIST + 8
+        u = torch.from_numpy(input_stream(fill + S * (reps + 1))).cuda()
+        torch.cuda.synchronize()
+
+        def launch(pos, steps):
+            assert lib.spires_ext_run_device(r.h, C.c_void_p(u.data_ptr() + pos * DIN * 8),
+                                             steps, None, None, None) == sp.SPIRES_OK
+
+        launch(0, fill)
+        stream = torch.cuda.ExternalStream(lib.spires_ext_stream(r.h))
+        pos, times = fill, []
+        for k in range(reps + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            launch(pos, S)
+            e1.record(stream)
+            pos += S
+            assert lib.spires_ext_sync(r.h) == sp.SPIRES_OK
+            times.append(e0.elapsed_time(e1))
+        r.close()
+        ms = float(np.median(times[1:]))
+        us_step = ms * 1e3 / S
+        row = {"neuron": nnames[nt], "synapse": snames[st], "us_per_step": us_step,
+               "neuron_steps_per_s": N_NEURONS * S / (ms * 1e-3),
+               "launch": {"ctas": lau.ctas, "warps": lau.warps_max, "variant": lau.variant}}
+        hb = hist_bytes.get(nt, 0) + (8 * 512 if st == sp.SYN_FRAC else 0)
+        if hb:
+            row["history_bytes_per_neuron_step"] = hb
+            row["history_GBps"] = hb * N_NEURONS / (us_step * 1e-6) / 1e9
+        rows.append(row)
+    peak, kind = peaks()
+    print(json.dumps({"metric": "step throughput per model", "unit": "neuron-steps/s",
+                      "models": rows, "peak_GBps": peak, "peak_kind": kind, "dtype": "f64",
+                      "data": "synthetic", "config": {"workload": "FLIF_GL bench graph, every model",
+                                                      "neurons": N_NEURONS, "steps_per_launch": S}}))
+
+
 def run_ridge_workload(args):
     """FLIF_GL N=4000 L=512 Watts-Strogatz k=10, Mackey-Glass T=20000,
     washout 1000, lambda 1e-6: the Gram X^T X of the 19000 fitted states in
@@ -836,7 +914,8 @@ def main():
     ap.add_argument("--cpu-fill", type=int, default=L_HIST + 8)
     ap.add_argument("--cpu-timed", type=int, default=100)
     ap.add_argument("--workload", default="step",
-                    choices=["step", "sweep", "search", "classify", "ridge", "small", "construct"],
+                    choices=["step", "sweep", "search", "classify", "ridge", "small", "construct",
+                             "models"],
                     help="step (default, the headline line) or an additional workload")
     ap.add_argument("--sweep-count", type=int, default=256)
     ap.add_argument("--construct-count", type=int, default=300)
@@ -855,7 +934,8 @@ def main():
     if args.workload != "step":
         {"sweep": run_sweep_workload, "search": run_search_workload,
          "classify": run_classify_workload, "ridge": run_ridge_workload,
-         "small": run_small_lif_workload, "construct": run_construct_workload}[args.workload](args)
+         "small": run_small_lif_workload, "construct": run_construct_workload,
+         "models": run_models_workload}[args.workload](args)
         return
 
     rank = int(os.environ.get("RANK", "0"))

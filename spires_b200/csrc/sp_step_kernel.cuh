@@ -34,7 +34,8 @@
 //   recurrent input            SIMPLE: warp-cooperative walk over the warp's
 //                              CSR edges, ballot of spiking presynaptic bits,
 //                              owner lane adds the weights in ascending edge
-//                              order; others: per-row walk over eff[]
+//                              order; others: warp-cooperative walk, one
+//                              term per edge, owner lane adds in edge order
 //   neuron update, ring write, ballot -> spike word of step g
 //   synapse prepare for g+1 (own spike), publish, arrive barrier g+1
 #pragma once
@@ -304,6 +305,48 @@ __device__ unsigned long long g_sp_stamps[kSpStampCtas * kSpStampSteps * kSpStam
     do {                         \
     } while (0)
 #endif
+
+// Synapses whose drive is not a spike bit (PSC and fractional: every edge
+// carries a term), one warp: rows [row0, row0 + 32), lane r owns row row0 + r.
+// The warp's contiguous edge range is taken 32 edges at a time, each lane
+// forming one edge's term in parallel -- w_k * eff[col_k], or for
+// PSC_HETEROGENEOUS the updated edge trace times w_k -- and the owner lane
+// of each edge's row adds the terms in ascending edge order, the order of the
+// reference's per-row loop (src/synapses/psc_heterogeneous.c:124-139,
+// src/synapse.c:90-105), so the sums are the same bits as a per-row walk.
+template <int ST>
+__device__ __forceinline__ double rowpass_terms_warp(const KP &p, const double *ef,
+                                                     const unsigned *s_spk, int row0, int lane)
+{
+    const long long e0 = __ldg(p.row_ptr + row0), e1 = __ldg(p.row_ptr + row0 + 32);
+    const long long my_start = __ldg(p.row_ptr + row0 + lane);
+    const long long my_end = __ldg(p.row_ptr + row0 + lane + 1);
+    double acc = 0.0;
+    for (long long base = e0; base < e1; base += 32) {
+        const long long k = base + lane;
+        double term = 0.0;
+        if (k < e1) {
+            const int c = __ldg(p.col + k);
+            if (ST == SP_SYN_PSC_HET) {
+                const double sv = ((s_spk[c >> 5] >> (c & 31)) & 1u) ? 1.0 : 0.0;
+                const double tr = add(mul(p.edge_trace[k], __ldg(p.edge_decay + k)),
+                                      mul(__ldg(p.edge_omd + k), sv));
+                p.edge_trace[k] = tr;
+                term = mul(__ldg(p.w + k), tr);
+            } else {
+                term = mul(__ldg(p.w + k), __ldcg(ef + c));
+            }
+        }
+        const int cnt = e1 - base < 32 ? (int)(e1 - base) : 32;
+        for (int j = 0; j < cnt; ++j) {
+            const double t = __shfl_sync(kFull, term, j);
+            const long long eb = base + j;
+            if (eb >= my_start && eb < my_end)
+                acc = add(acc, t);
+        }
+    }
+    return acc;
+}
 
 // The same walk over the CTA's CSR slice in shared memory: rp = row offsets
 // relative to the slice (rows of the CTA in position order), col = column
@@ -905,24 +948,9 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 else
                     rec = rowpass_simple_warp(p.row_ptr, p.col, p.w, s_spk, gw * 32, 32, lane);
             }
-        } else if (act) {
-            const long long k0 = __ldg(p.row_ptr + i), k1 = __ldg(p.row_ptr + i + 1);
-            if (ST == SP_SYN_PSC_HET) {
-                for (long long k = k0; k < k1; ++k) {
-                    const int c = __ldg(p.col + k);
-                    const double sv = ((s_spk[c >> 5] >> (c & 31)) & 1u) ? 1.0 : 0.0;
-                    const double tr = add(mul(p.edge_trace[k], __ldg(p.edge_decay + k)),
-                                          mul(__ldg(p.edge_omd + k), sv));
-                    p.edge_trace[k] = tr;
-                    rec = add(rec, mul(__ldg(p.w + k), tr));
-                }
-            } else {
-                const double *ef = p.eff + (size_t)cur * p.rs;
-                for (long long k = k0; k < k1; ++k) {
-                    const int c = __ldg(p.col + k);
-                    rec = add(rec, mul(__ldg(p.w + k), __ldcg(ef + c)));
-                }
-            }
+        } else if (wact) {
+            // whole warps (holes are empty rows): every edge carries a term
+            rec = rowpass_terms_warp<ST>(p, p.eff + (size_t)cur * p.rs, s_spk, gw * 32, lane);
         }
 
         SP_STAMP(tid == 0, b, B, 4);
