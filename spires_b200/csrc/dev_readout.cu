@@ -187,8 +187,11 @@ __global__ void k_add_diag(double *A, int n, int lda, double lam)
 // ------------------------------------------------------- blocked Cholesky
 // A (n x n, row-major, lower triangle used) -> L in place.
 // Diagonal block of panel [k0, k0 + kb), one CTA of 256 threads: thread t
-// owns row t % 64 and the 16 columns t / 64 + 4 m of the trailing update, so
-// each column step is 16 predicated FMAs per thread between two barriers.
+// owns row t % 64 and the 16 columns t / 64 + 4 m of the trailing update.
+// For column j every thread derives the factor itself from the current
+// values (d = sqrt(a_jj), l_rj = a_rj / d as a_rj * (1 / d)) and updates its
+// entries right of column j; the scaled column is written after the one
+// barrier of the column, when nobody reads it any more.
 __global__ void __launch_bounds__(256) k_potrf_diag(double *A, int n, int lda, int k0, int kb,
                                                     int *info)
 {
@@ -198,38 +201,38 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double *A, int n, int lda, i
         return;
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
         const int r = q / kb, c = q % kb;
-        s[r][c] = A[(size_t)(k0 + r) * lda + k0 + c];
+        if (c <= r)
+            s[r][c] = A[(size_t)(k0 + r) * lda + k0 + c];
     }
     if (threadIdx.x == 0)
         bad = 0;
     __syncthreads();
     const int r = threadIdx.x & (NB - 1), c0 = threadIdx.x >> 6;
     for (int j = 0; j < kb; ++j) {
-        if (threadIdx.x == 0) {
-            const double d = s[j][j];
-            if (!(d > 0.0) || !isfinite(d)) {
-                if (!bad)
-                    bad = k0 + j + 1;
-                s[j][j] = 1.0;
-            } else {
-                s[j][j] = sqrt(d);
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x < NB && r > j && r < kb)
-            s[r][j] /= s[j][j];
-        __syncthreads();
+        const double a = s[j][j];
+        const bool okd = a > 0.0 && isfinite(a);
+        const double d = okd ? sqrt(a) : 1.0;
+        const double inv = 1.0 / d;
+        double lrj = 0.0;
         if (r > j && r < kb) {
-            const double lrj = s[r][j];
+            lrj = s[r][j] * inv;
 #pragma unroll
             for (int m = 0; m < NB / 4; ++m) {
                 const int c = c0 + 4 * m;
                 if (c > j && c <= r)
-                    s[r][c] -= lrj * s[c][j];
+                    s[r][c] = fma(-lrj, s[c][j] * inv, s[r][c]);
             }
         }
-        __syncthreads();
+        __syncthreads();  // every read of column j is done
+        if (c0 == 0 && r > j && r < kb)
+            s[r][j] = lrj;
+        if (threadIdx.x == 0) {
+            s[j][j] = d;
+            if (!okd && !bad)
+                bad = k0 + j + 1;
+        }
     }
+    __syncthreads();
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
         const int rr = q / kb, cc = q % kb;
         if (cc <= rr)
@@ -239,13 +242,15 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double *A, int n, int lda, i
         atomicCAS(info, 0, bad);
 }
 
-// Rows r >= k0 + kb: L[r][k0:k0+kb] = A[r][k0:k0+kb] L_kk^-T. One warp per
-// row, lane l holding columns l and l + 32; columns are eliminated in order
-// (x_c = a_c / L_cc, then a_q -= x_c L_qc for q > c). 32 rows per CTA.
+// Rows r >= k0 + kb: L[r][k0:k0+kb] = A[r][k0:k0+kb] L_kk^-T. A warp solves 4
+// rows side by side (independent chains), lane l holding columns l and l + 32
+// of each; columns are eliminated in order (x_c = a_c * (1 / L_cc), then
+// a_q -= x_c L_qc for q > c). 32 rows per CTA.
 __global__ void __launch_bounds__(256) k_trsm_panel(double *A, int n, int lda, int k0, int kb,
                                                     const int *info)
 {
     __shared__ double sL[NB][NB + 1];
+    __shared__ double sInv[NB];
     if (*info)
         return;
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
@@ -253,32 +258,49 @@ __global__ void __launch_bounds__(256) k_trsm_panel(double *A, int n, int lda, i
         sL[r][c] = (c <= r) ? A[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
     }
     __syncthreads();
+    if (threadIdx.x < kb)
+        sInv[threadIdx.x] = 1.0 / sL[threadIdx.x][threadIdx.x];
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = 0; k < 4; ++k) {
-        const int r = k0 + kb + blockIdx.x * 32 + k * 8 + warp;
-        if (r >= n)
-            return;
-        double *row = A + (size_t)r * lda + k0;
-        double a0 = lane < kb ? row[lane] : 0.0;
-        double a1 = lane + 32 < kb ? row[lane + 32] : 0.0;
-        for (int c = 0; c < kb; ++c) {
-            const double ac = __shfl_sync(kFull, c < 32 ? a0 : a1, c & 31);
-            const double xc = ac / sL[c][c];
+    const int r0 = k0 + kb + blockIdx.x * 32 + warp * 4;
+    if (r0 >= n)
+        return;
+    double a0[4], a1[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool ok = r0 + q < n;
+        const double *row = A + (size_t)(r0 + q) * lda + k0;
+        a0[q] = ok && lane < kb ? row[lane] : 0.0;
+        a1[q] = ok && lane + 32 < kb ? row[lane + 32] : 0.0;
+    }
+    for (int c = 0; c < kb; ++c) {
+        const double ic = sInv[c];
+        const double l0 = (lane > c && lane < kb) ? sL[lane][c] : 0.0;
+        const double l1 = (lane + 32 > c && lane + 32 < kb) ? sL[lane + 32][c] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double xc = __shfl_sync(kFull, c < 32 ? a0[q] : a1[q], c & 31) * ic;
             if (lane == (c & 31)) {
                 if (c < 32)
-                    a0 = xc;
+                    a0[q] = xc;
                 else
-                    a1 = xc;
+                    a1[q] = xc;
             }
             if (lane > c && lane < kb)
-                a0 = fma(-xc, sL[lane][c], a0);
+                a0[q] = fma(-xc, l0, a0[q]);
             if (lane + 32 > c && lane + 32 < kb)
-                a1 = fma(-xc, sL[lane + 32][c], a1);
+                a1[q] = fma(-xc, l1, a1[q]);
         }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (r0 + q >= n)
+            break;
+        double *row = A + (size_t)(r0 + q) * lda + k0;
         if (lane < kb)
-            row[lane] = a0;
+            row[lane] = a0[q];
         if (lane + 32 < kb)
-            row[lane + 32] = a1;
+            row[lane + 32] = a1[q];
     }
 }
 
@@ -335,22 +357,27 @@ __global__ void __launch_bounds__(256) k_syrk_update(double *A, int n, int lda, 
 // ----------------------------------------------------- triangular solves
 // Forward L Z = B in place on Z (n x dout), panel by panel: the diagonal
 // block by one CTA (warp w takes outputs w, w + 8, ...; lane l holds rows l
-// and l + 32; columns eliminated in order), then the rows below it.
+// and l + 32; columns eliminated in order, dividing by the diagonal as a
+// product with its reciprocal), then the rows below it.
 __global__ void __launch_bounds__(256) k_fwd_diag(const double *L, int lda, int k0, int kb,
                                                   double *Z, int dout)
 {
     __shared__ double sL[NB][NB + 1];
+    __shared__ double sInv[NB];
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
         const int r = q / kb, c = q % kb;
         sL[r][c] = (c <= r) ? L[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
     }
+    __syncthreads();
+    if (threadIdx.x < kb)
+        sInv[threadIdx.x] = 1.0 / sL[threadIdx.x][threadIdx.x];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int o = warp; o < dout; o += 8) {
         double z0 = lane < kb ? Z[(size_t)(k0 + lane) * dout + o] : 0.0;
         double z1 = lane + 32 < kb ? Z[(size_t)(k0 + lane + 32) * dout + o] : 0.0;
         for (int j = 0; j < kb; ++j) {
-            const double zj = __shfl_sync(kFull, j < 32 ? z0 : z1, j & 31) / sL[j][j];
+            const double zj = __shfl_sync(kFull, j < 32 ? z0 : z1, j & 31) * sInv[j];
             if (lane == (j & 31)) {
                 if (j < 32)
                     z0 = zj;
@@ -400,17 +427,21 @@ __global__ void __launch_bounds__(256) k_bwd_diag(const double *L, int lda, int 
                                                   double *Z, int dout)
 {
     __shared__ double sL[NB][NB + 1];
+    __shared__ double sInv[NB];
     for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
         const int r = q / kb, c = q % kb;
         sL[r][c] = (c <= r) ? L[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
     }
+    __syncthreads();
+    if (threadIdx.x < kb)
+        sInv[threadIdx.x] = 1.0 / sL[threadIdx.x][threadIdx.x];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int o = warp; o < dout; o += 8) {
         double z0 = lane < kb ? Z[(size_t)(k0 + lane) * dout + o] : 0.0;
         double z1 = lane + 32 < kb ? Z[(size_t)(k0 + lane + 32) * dout + o] : 0.0;
         for (int j = kb - 1; j >= 0; --j) {
-            const double xj = __shfl_sync(kFull, j < 32 ? z0 : z1, j & 31) / sL[j][j];
+            const double xj = __shfl_sync(kFull, j < 32 ? z0 : z1, j & 31) * sInv[j];
             if (lane == (j & 31)) {
                 if (j < 32)
                     z0 = xj;
