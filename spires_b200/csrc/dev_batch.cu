@@ -101,17 +101,39 @@ __device__ __forceinline__ double batch_history_async(double hist, const double 
 {
     if (lim < 2)
         return hist;
-    int r = head - 2;
+    int r = head - 2;  // ring row of the next lag to issue
     if (r < 0)
         r += L;
+    const double *gp = ci + (size_t)r * rs;   // its element of this column
+    const double *gtop = ci + (size_t)(L - 1) * rs;
     int kiss = 2;  // next lag to issue
     auto issue = [&](int stg) {
+        double *dst = s_h + (size_t)stg * kHistC * kBatchThreads + tid;
+        if (kiss + kHistC - 1 <= lim && r >= kHistC - 1) {
+            // a whole group before the ring's wrap: fixed offsets, no tests
 #pragma unroll
-        for (int j = 0; j < kHistC; ++j) {
-            if (kiss + j <= lim) {
-                cp_async8(s_h + (size_t)(stg * kHistC + j) * kBatchThreads + tid,
-                          ci + (size_t)r * rs);
-                r = (r == 0) ? L - 1 : r - 1;
+            for (int j = 0; j < kHistC; ++j) {
+                cp_async8(dst + (size_t)j * kBatchThreads, gp);
+                gp -= rs;
+            }
+            r -= kHistC;
+            if (r < 0) {
+                r += L;
+                gp = gtop;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kHistC; ++j) {
+                if (kiss + j <= lim) {
+                    cp_async8(dst + (size_t)j * kBatchThreads, gp);
+                    if (r == 0) {
+                        r = L - 1;
+                        gp = gtop;
+                    } else {
+                        --r;
+                        gp -= rs;
+                    }
+                }
             }
         }
         kiss += kHistC;
@@ -125,10 +147,16 @@ __device__ __forceinline__ double batch_history_async(double hist, const double 
         issue((stg + kHistS - 1) % kHistS);  // possibly an empty group
         cp_async_wait<kHistS - 1>();          // the group of lags k.. has landed
         const double *src = s_h + (size_t)stg * kHistC * kBatchThreads + tid;
+        if (k + kHistC - 1 <= lim) {
 #pragma unroll
-        for (int j = 0; j < kHistC; ++j)
-            if (k + j <= lim)
+            for (int j = 0; j < kHistC; ++j)
                 hist = add(hist, mul(s_coef[k + j], src[(size_t)j * kBatchThreads]));
+        } else {
+#pragma unroll
+            for (int j = 0; j < kHistC; ++j)
+                if (k + j <= lim)
+                    hist = add(hist, mul(s_coef[k + j], src[(size_t)j * kBatchThreads]));
+        }
         stg = (stg + 1 == kHistS) ? 0 : stg + 1;
     }
     cp_async_wait<0>();
