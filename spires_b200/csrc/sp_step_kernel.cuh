@@ -1055,8 +1055,12 @@ __global__ void __launch_bounds__(Bounds<VAR>::threads, 1) k_run(const __grid_co
                 }
             }
         }
-        if (VAR == 1)
-            fence_proxy_async();  // ring row of step g is read by bulk copies later
+        // the ring row of step g is first read by a bulk copy as lag RL + 2,
+        // RL + 2 steps later: with the register lags one proxy fence per 16
+        // steps orders every row before that read (kernel boundaries order
+        // the rest)
+        if (VAR == 1 && (RL < 32 || (g & 15) == 15))
+            fence_proxy_async();
 
         // ---- spike word of step g
         const unsigned word = __ballot_sync(kFull, fired);
