@@ -321,28 +321,39 @@ __device__ __forceinline__ double rowpass_terms_warp(const KP &p, const double *
     const long long e0 = __ldg(p.row_ptr + row0), e1 = __ldg(p.row_ptr + row0 + 32);
     const long long my_start = __ldg(p.row_ptr + row0 + lane);
     const long long my_end = __ldg(p.row_ptr + row0 + lane + 1);
-    double acc = 0.0;
-    for (long long base = e0; base < e1; base += 32) {
-        const long long k = base + lane;
-        double term = 0.0;
-        if (k < e1) {
-            const int c = __ldg(p.col + k);
-            if (ST == SP_SYN_PSC_HET) {
-                const double sv = ((s_spk[c >> 5] >> (c & 31)) & 1u) ? 1.0 : 0.0;
-                const double tr = add(mul(p.edge_trace[k], __ldg(p.edge_decay + k)),
-                                      mul(__ldg(p.edge_omd + k), sv));
-                p.edge_trace[k] = tr;
-                term = mul(__ldg(p.w + k), tr);
-            } else {
-                term = mul(__ldg(p.w + k), __ldcg(ef + c));
-            }
+    auto term_of = [&](long long k) -> double {
+        if (k >= e1)
+            return 0.0;
+        const int c = __ldg(p.col + k);
+        if (ST == SP_SYN_PSC_HET) {
+            const double sv = ((s_spk[c >> 5] >> (c & 31)) & 1u) ? 1.0 : 0.0;
+            const double tr = add(mul(p.edge_trace[k], __ldg(p.edge_decay + k)),
+                                  mul(__ldg(p.edge_omd + k), sv));
+            p.edge_trace[k] = tr;
+            return mul(__ldg(p.w + k), tr);
         }
-        const int cnt = e1 - base < 32 ? (int)(e1 - base) : 32;
-        for (int j = 0; j < cnt; ++j) {
-            const double t = __shfl_sync(kFull, term, j);
-            const long long eb = base + j;
-            if (eb >= my_start && eb < my_end)
-                acc = add(acc, t);
+        return mul(__ldg(p.w + k), __ldcg(ef + c));
+    };
+    double acc = 0.0;
+    // 4 chunks of 32 edges at a time: their loads in flight together, then
+    // each chunk's terms added by the owner lanes in ascending edge order
+    for (long long base = e0; base < e1; base += 4 * 32) {
+        double t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            t[u] = term_of(base + 32 * u + lane);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long cb = base + 32 * u;
+            if (cb >= e1)
+                break;
+            const int cnt = e1 - cb < 32 ? (int)(e1 - cb) : 32;
+            for (int j = 0; j < cnt; ++j) {
+                const double v = __shfl_sync(kFull, t[u], j);
+                const long long eb = cb + j;
+                if (eb >= my_start && eb < my_end)
+                    acc = add(acc, v);
+            }
         }
     }
     return acc;
