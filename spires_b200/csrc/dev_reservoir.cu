@@ -698,10 +698,30 @@ fail:
 #undef TRY
 }
 
+// Give every 128-byte line of [base, base + bytes) normal L2 eviction
+// priority (base 128-byte aligned, bytes a multiple of 128).
+__global__ void k_l2_demote(const char *base, size_t bytes)
+{
+    const size_t stride = (size_t)gridDim.x * blockDim.x * 128;
+    for (size_t off = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 128; off < bytes;
+         off += stride)
+        asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(base + off)
+                     : "memory");
+}
+
 extern "C" void sp_dev_destroy(sp_dev *d)
 {
     if (!d)
         return;
+    if (d->stream && d->ring && d->l2_hinted) {
+        // ring lines the step kernel left with evict-last priority would
+        // otherwise outrank every later normal line in the L2 for the rest
+        // of the process: give them normal priority before the ring is freed
+        const size_t bytes = d->ring_elems * sizeof(double);
+        k_l2_demote<<<(unsigned)(d->num_sms > 0 ? 4 * d->num_sms : 512), 256, 0, d->stream>>>(
+            (const char *)d->ring, bytes);
+        cudaGetLastError();
+    }
     if (d->stream)
         cudaStreamSynchronize(d->stream);
     void *bufs[] = {d->V, d->tprev, d->ring, d->cap_pos, d->refr_until, d->rng, d->spk,
@@ -858,6 +878,8 @@ extern "C" int sp_dev_launch_chunk(sp_dev *d, const double *u, size_t T, double 
     p.bar = d->bar; p.err = d->err; p.flags = d->flags;
     p.tmo = d->wait_ns ? d->wait_ns : kBarrierTimeoutNs;
     p.l2_pin = sp_dev_l2_pin_rows(d);
+    if (p.l2_pin > 0)
+        d->l2_hinted = 1;
     p.hold_cta = -1;
     p.hold_b = -1;
     if (d->hold_cta >= 0 && d->hold_b >= 1 && d->hold_b < (long long)T * d->micro) {

@@ -19,6 +19,7 @@
 struct sp_dev {
     int device, num_sms, coop;
     int l2_bytes;  // device L2 cache size
+    int l2_hinted; // a launch read the ring with evict-last hints (demoted at destroy)
     cudaStream_t stream;
     int n, din, dout, micro;
     int nw;              // warps of positions (= spike words in position space)
