@@ -278,7 +278,7 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
                     max_points: int = 4096, waves: int = 8, seed: int = 0,
                     opts: AgileOpts | None = None, use_surrogate: bool = True, epochs: int = 200,
                     calibration: int = 8, kappa: float = 1.0,
-                    prescreen: float = 0.0) -> SearchResult:
+                    prescreen: float = 0.0, tell_optimistic: bool = False) -> SearchResult:
     """Surrogate-guided multi-fidelity AGILE (see module doc). The chains start
     from the same points with the same seeds as :func:`plain_agile`.
 
@@ -298,7 +298,11 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
     fraction `prescreen` by its optimistic score (plus `calibration` random
     ones) is built and simulated at the lowest fidelity; the chains are told
     that network's prediction for the others, which are neither built nor
-    pooled."""
+    pooled.
+
+    tell_optimistic tells the chains the optimistic score mean - kappa * std
+    instead of the predicted mean, so that regions the network is unsure
+    about attract them."""
     lib, h = _agile_start(chains, seed, opts)
     ncut = len(rungs) - 1
     nets = [Surrogate(seed=seed + r) for r in range(ncut)] if use_surrogate else None
@@ -416,11 +420,11 @@ def surrogate_agile(ev: Evaluator, chains: int = 16, rungs=(1000, 4000, 16000), 
                 cal = rng.choice(n, size=min(calibration, n), replace=False)
                 run = np.union1d(np.argsort(score, kind="stable")[:nk], cal)
                 rest = np.setdiff1d(np.arange(n), run)
-                est[rest] = m.astype(np.float64)[rest]
+                est[rest] = (score if tell_optimistic else m.astype(np.float64))[rest]
                 screened += len(rest)
             l0 = ev.evaluate(th[run], rungs[0], ids[run])
             evals += len(run)
-            est[run] = predict(0, th[run], l0)
+            est[run] = predict(0, th[run], l0, optimistic=tell_optimistic)
             lib.spires_ext_agile_batch_tell(h, dptr(np.ascontiguousarray(est)))
             pool_th.append(th[run])
             pool_l0.append(l0)
