@@ -516,6 +516,7 @@ def run_search_workload(args):
             r = S.surrogate_agile(ev, chains=chains, rungs=rungs, max_points=points, waves=8,
                                   prescreen=args.search_prescreen if name == "surrogate" else 0.0,
                                   keep=args.search_keep,
+                                  tell_optimistic=args.search_tell_optimistic,
                                   seed=0, use_surrogate=(name != "no_surrogate"))
         out[name] = (r, ev.stats)
     plain = out["plain"][0]
@@ -542,7 +543,8 @@ def run_search_workload(args):
     line["plain_construct_s"] = out["plain"][1].construct_s
     line["config"] = {"workload": "surrogate-guided AGILE", "scale": args.search_scale,
                       "rungs": list(rungs), "points": points, "chains": chains, "waves": 8,
-                      "prescreen": args.search_prescreen, "keep": args.search_keep}
+                      "prescreen": args.search_prescreen, "keep": args.search_keep,
+                      "tell_optimistic": args.search_tell_optimistic}
     line["data"] = "synthetic (seeded Mackey-Glass)"
     print(json.dumps(line))
 
@@ -924,6 +926,8 @@ def main():
     ap.add_argument("--sweep-tmax", type=int, default=10000,
                     help="longest series of the sweep (smaller for profiling)")
     ap.add_argument("--search-scale", default="medium", choices=["medium", "full"])
+    ap.add_argument("--search-tell-optimistic", action="store_true",
+                    help="surrogate arms: tell the chains mean - std instead of the mean")
     ap.add_argument("--search-keep", type=float, default=0.1,
                     help="surrogate arms: fraction surviving each rung (the configuration's 10 %%)")
     ap.add_argument("--search-prescreen", type=float, default=0.0,
