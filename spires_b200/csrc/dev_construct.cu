@@ -60,12 +60,22 @@ __global__ void __launch_bounds__(256) k_power_iter(PIArgs a)
     for (; it < a.max_iter; ++it) {
         const int slot = it & 1;
         double lm = 0.0;
-        for (long long i = g0; i < a.n; i += stride) {
+        // one warp per row: the lanes load 32 edges' terms at once, and every
+        // lane adds them in ascending edge order from +0 (the same sum as a
+        // sequential walk of the row), so long rows do not serialise loads
+        const int lane = threadIdx.x & 31;
+        for (long long i = g0 >> 5; i < a.n; i += stride >> 5) {
             double s = 0.0;
-            const long long k1 = __ldg(a.row_ptr + i + 1);
-            for (long long k = __ldg(a.row_ptr + i); k < k1; ++k)
-                s = add(s, mul(__ldg(a.w + k), __ldcg(a.x + __ldg(a.col + k))));
-            a.y[i] = s;
+            const long long k0 = __ldg(a.row_ptr + i), k1 = __ldg(a.row_ptr + i + 1);
+            for (long long base = k0; base < k1; base += 32) {
+                const long long k = base + lane;
+                const double t = k < k1 ? mul(__ldg(a.w + k), __ldcg(a.x + __ldg(a.col + k))) : 0.0;
+                const int cnt = k1 - base < 32 ? (int)(k1 - base) : 32;
+                for (int j = 0; j < cnt; ++j)
+                    s = add(s, __shfl_sync(kFull, t, j));
+            }
+            if (lane == 0)
+                a.y[i] = s;
             const double v = fabs(s);
             if (v > lm)  // NaN never wins, as in the host comparison
                 lm = v;
@@ -128,7 +138,11 @@ extern "C" int sp_dev_spectral_radius(size_t n, const int64_t *row_ptr, const in
     if (!coop || per_sm < 1)
         return SP_EINTERNAL;
     per_sm = per_sm > 2 ? 2 : per_sm;
+    // a warp per row: enough CTAs for the rows' edges, at most a full grid
     long long blocks = ((long long)n + 255) / 256;
+    const long long by_edges = ((long long)row_ptr[n] + 16383) / 16384;
+    if (blocks < by_edges)
+        blocks = by_edges;
     if (blocks > (long long)per_sm * sms)
         blocks = (long long)per_sm * sms;
     if (blocks < 1)
